@@ -1,0 +1,241 @@
+// chns_fft.cuh -- register/shared-memory FFT building blocks for sm_100a.
+//
+// Replaces the reference's FFTW-MPI transforms (fft.c:11-31, plans main.c:193-194).
+// A length-N transform (N = 2^p, 32 <= N <= 4096) is done by a "group" of
+// NT = N/16 threads; thread t of the group holds the 16 elements
+// x[t + NT*m], m = 0..15, in registers.  Stages follow Stockham's autosorting
+// decimation-in-time scheme with radix 16 (a radix-2/4/8 stage first when
+// log2(N) is not a multiple of 4): every stage reads the pattern x[t + NT*m]
+// from shared memory, multiplies by twiddles from a table in global memory,
+// does an in-register DFT, and scatters; the last radix-16 stage leaves the
+// output in registers, again as X[t + NT*m] (natural order).  One shared-memory
+// round trip per stage after the first; the shared array is padded by one
+// element every 16 so that all stage patterns are bank-conflict free.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace chns {
+
+template <class R> struct __align__(2 * sizeof(R)) cx {
+  R x, y;
+};
+using cxf = cx<float>;
+using cxd = cx<double>;
+
+template <class R> __device__ __forceinline__ cx<R> mk(R a, R b) { cx<R> r; r.x = a; r.y = b; return r; }
+template <class R> __device__ __forceinline__ cx<R> operator+(cx<R> a, cx<R> b) { return mk<R>(a.x + b.x, a.y + b.y); }
+template <class R> __device__ __forceinline__ cx<R> operator-(cx<R> a, cx<R> b) { return mk<R>(a.x - b.x, a.y - b.y); }
+template <class R> __device__ __forceinline__ cx<R> cmul(cx<R> a, cx<R> b) {
+  return mk<R>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+template <class R> __device__ __forceinline__ cx<R> cmulc(cx<R> a, cx<R> b) {
+  return mk<R>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// Rounded arithmetic without contraction: used wherever the reference's
+// expression order must be kept (the FFT butterflies are free to use FMA).
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// multiply by DIR*i: forward transforms use DIR = -1 (kernel exp(-2 pi i jk/N))
+template <int DIR, class R> __device__ __forceinline__ cx<R> mul_i(cx<R> a) {
+  return DIR < 0 ? mk<R>(a.y, -a.x) : mk<R>(-a.y, a.x);
+}
+
+template <int DIR, class R> __device__ __forceinline__ void dft2(cx<R>& a0, cx<R>& a1) {
+  cx<R> t = a0 - a1;
+  a0 = a0 + a1;
+  a1 = t;
+}
+
+template <int DIR, class R> __device__ __forceinline__ void dft4(cx<R>& a0, cx<R>& a1, cx<R>& a2, cx<R>& a3) {
+  cx<R> t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = mul_i<DIR>(a1 - a3);
+  a0 = t0 + t2;
+  a2 = t0 - t2;
+  a1 = t1 + t3;
+  a3 = t1 - t3;
+}
+
+// constants of the 16th roots of unity
+#define CHNS_C8 0.92387953251128675612818318939678828682241662586364
+#define CHNS_S8 0.38268343236508977172845998403039886676134456248563
+#define CHNS_R2 0.70710678118654752440084436210484903928483593768847
+
+// v *= W16^(DIR... e), W16 = exp(DIR * 2 pi i / 16) with DIR = -1 forward
+template <int DIR, int E, class R> __device__ __forceinline__ cx<R> tw16(cx<R> v) {
+  constexpr int e = E & 15;
+  const R c8 = (R)CHNS_C8, s8 = (R)CHNS_S8, r2 = (R)CHNS_R2;
+  // w = cos(2 pi e/16) + DIR * i sin(2 pi e/16)
+  if (e == 0) return v;
+  if (e == 4) return mul_i<DIR>(v);
+  if (e == 8) return mk<R>(-v.x, -v.y);
+  if (e == 12) return mul_i<-DIR>(v);
+  R wc, ws;  // cos, sin of 2 pi e / 16
+  switch (e) {
+    case 1: wc = c8; ws = s8; break;
+    case 2: wc = r2; ws = r2; break;
+    case 3: wc = s8; ws = c8; break;
+    case 5: wc = -s8; ws = c8; break;
+    case 6: wc = -r2; ws = r2; break;
+    case 7: wc = -c8; ws = s8; break;
+    case 9: wc = -c8; ws = -s8; break;
+    case 10: wc = -r2; ws = -r2; break;
+    case 11: wc = -s8; ws = -c8; break;
+    case 13: wc = s8; ws = -c8; break;
+    case 14: wc = r2; ws = -r2; break;
+    default: wc = c8; ws = -s8; break;  // 15
+  }
+  ws = DIR < 0 ? -ws : ws;
+  return mk<R>(v.x * wc - v.y * ws, v.x * ws + v.y * wc);
+}
+
+// In-register DFT of size R_ on v[off + stride*r], r = 0..R_-1; outputs in
+// natural order at the same slots.
+template <int DIR, int RADIX, int STRIDE, class R> __device__ __forceinline__ void dft(cx<R>* v) {
+  if constexpr (RADIX == 2) {
+    dft2<DIR>(v[0], v[STRIDE]);
+  } else if constexpr (RADIX == 4) {
+    dft4<DIR>(v[0], v[STRIDE], v[2 * STRIDE], v[3 * STRIDE]);
+  } else if constexpr (RADIX == 8) {
+    // 8 = 2 x 4: r = r1 + 2 r2; X[k2 + 4 k1] lands in slot k1 + 2 k2
+    cx<R> y[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) y[r] = v[r * STRIDE];
+    dft4<DIR>(y[0], y[2], y[4], y[6]);
+    dft4<DIR>(y[1], y[3], y[5], y[7]);
+    y[3] = tw16<DIR, 2>(y[3]);
+    y[5] = tw16<DIR, 4>(y[5]);
+    y[7] = tw16<DIR, 6>(y[7]);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; k2++) dft2<DIR>(y[2 * k2], y[2 * k2 + 1]);
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k * STRIDE] = y[(k / 4) + 2 * (k % 4)];
+  } else {
+    static_assert(RADIX == 16, "radix");
+    // 16 = 4 x 4: r = r1 + 4 r2; X[k2 + 4 k1] lands in slot k1 + 4 k2
+    cx<R> y[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++) y[r] = v[r * STRIDE];
+#pragma unroll
+    for (int r1 = 0; r1 < 4; r1++) dft4<DIR>(y[r1], y[r1 + 4], y[r1 + 8], y[r1 + 12]);
+    y[5] = tw16<DIR, 1>(y[5]);
+    y[9] = tw16<DIR, 2>(y[9]);
+    y[13] = tw16<DIR, 3>(y[13]);
+    y[6] = tw16<DIR, 2>(y[6]);
+    y[10] = tw16<DIR, 4>(y[10]);
+    y[14] = tw16<DIR, 6>(y[14]);
+    y[7] = tw16<DIR, 3>(y[7]);
+    y[11] = tw16<DIR, 6>(y[11]);
+    y[15] = tw16<DIR, 9>(y[15]);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; k2++) dft4<DIR>(y[4 * k2], y[4 * k2 + 1], y[4 * k2 + 2], y[4 * k2 + 3]);
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k * STRIDE] = y[(k / 4) + 4 * (k % 4)];
+  }
+}
+
+__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
+
+// shared-memory slot of element q of one group's buffer (one pad per 16)
+__device__ __forceinline__ int spad(int q) { return q + (q >> 4); }
+
+template <int N> struct FftShape {
+  static constexpr int NT = N / 16;                   // threads per transform
+  static constexpr int LOGN = ilog2c(N);
+  static constexpr int R0 = 1 << (LOGN % 4);         // leading small radix (1 = none)
+  static constexpr int N16 = LOGN / 4;               // number of radix-16 stages
+  static constexpr int SMEM = N + N / 16;            // complex slots per group
+};
+
+// One Stockham stage: radix RADIX, span NS (product of the earlier radices).
+// v holds x[t + NT*m]; writes the stage output to sh (padded).
+template <int N, int DIR, int RADIX, int NS, class R>
+__device__ __forceinline__ void fft_stage_to_smem(cx<R>* v, cx<R>* sh, int t, const cx<R>* __restrict__ tw) {
+  constexpr int NT = N / 16;
+  constexpr int B = 16 / RADIX;  // butterflies per thread
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int j = t + NT * b;
+    const int k = j % NS;
+    cx<R> u[RADIX];
+#pragma unroll
+    for (int r = 0; r < RADIX; r++) u[r] = v[b + r * B];
+    if (NS > 1) {
+      // twiddle W_{NS*RADIX}^{k r} = tw[k r N/(NS RADIX)], conjugated for the inverse
+#pragma unroll
+      for (int r = 1; r < RADIX; r++) {
+        cx<R> w = tw[(k * r * (N / (NS * RADIX))) & (N - 1)];
+        u[r] = DIR < 0 ? cmul(u[r], w) : cmulc(u[r], w);
+      }
+    }
+    dft<DIR, RADIX, 1>(u);
+    const int base = (j / NS) * NS * RADIX + k;
+#pragma unroll
+    for (int q = 0; q < RADIX; q++) sh[spad(base + q * NS)] = u[q];
+  }
+}
+
+template <int N, class R>
+__device__ __forceinline__ void fft_load_smem(cx<R>* v, const cx<R>* sh, int t) {
+  constexpr int NT = N / 16;
+#pragma unroll
+  for (int m = 0; m < 16; m++) v[m] = sh[spad(t + NT * m)];
+}
+
+// Last radix-16 stage (NS = N/16): result stays in registers in natural order.
+template <int N, int DIR, class R>
+__device__ __forceinline__ void fft_last_stage(cx<R>* v, int t, const cx<R>* __restrict__ tw) {
+  constexpr int NS = N / 16;
+  if (NS > 1) {
+    const int k = t;  // j = t < NS
+#pragma unroll
+    for (int r = 1; r < 16; r++) {
+      cx<R> w = tw[(k * r) & (N - 1)];
+      v[r] = DIR < 0 ? cmul(v[r], w) : cmulc(v[r], w);
+    }
+  }
+  dft<DIR, 16, 1>(v);
+}
+
+// Full transform of one group.  All threads of the CTA must call it together
+// (it uses __syncthreads); sh is this group's padded buffer of FftShape<N>::SMEM.
+// The leading barrier protects the buffer from the previous transform's readers.
+template <int N, int DIR, class R>
+__device__ __forceinline__ void fft(cx<R>* v, cx<R>* sh, int t, const cx<R>* __restrict__ tw) {
+  using S = FftShape<N>;
+  if constexpr (S::N16 == 1 && S::R0 == 1) {
+    fft_last_stage<N, DIR>(v, t, tw);  // N = 16: single stage
+  } else {
+    if constexpr (S::R0 > 1) {
+      __syncthreads();
+      fft_stage_to_smem<N, DIR, S::R0, 1>(v, sh, t, tw);
+      __syncthreads();
+      fft_load_smem<N>(v, sh, t);
+    }
+    if constexpr (S::N16 >= 2) {
+      __syncthreads();
+      fft_stage_to_smem<N, DIR, 16, S::R0>(v, sh, t, tw);
+      __syncthreads();
+      fft_load_smem<N>(v, sh, t);
+    }
+    if constexpr (S::N16 >= 3) {
+      __syncthreads();
+      fft_stage_to_smem<N, DIR, 16, S::R0 * 16>(v, sh, t, tw);
+      __syncthreads();
+      fft_load_smem<N>(v, sh, t);
+    }
+    static_assert(S::N16 <= 3, "N <= 4096");
+    fft_last_stage<N, DIR>(v, t, tw);
+  }
+}
+
+}  // namespace chns

@@ -1,0 +1,157 @@
+#!/usr/bin/env python3
+"""Generates the golden fixtures in tests/golden/ by running the REFERENCE's own
+compiled sources (oracle/_ref/<config>/libref.so, built by oracle/build_ref.py).
+
+The reference ships no tests, fixtures or golden vectors of its own, so these
+vectors are the reference run here: its etd2rk.c / nonlin.c / ... code, with the
+oracle's FP64 FFT behind its FFTW calls.  They pin both the C restatement
+(oracle/chns_oracle.c) and, through it, the GPU path.
+
+Small grids store full spectral states; the two full-size configurations
+(binary 256^2 x 1000 steps, ternary 512^2 x 2000 steps) store a fingerprint of
+the final state (see fingerprint()).
+
+Usage:  python tests/golden/make_golden.py [--full]
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "ternary-chns_b200"))
+
+from chns_b200 import fields  # noqa: E402
+
+# scenario: (config, steps, phase seed, vorticity seed or None, vorticity kmax, rms)
+SMALL = [
+    ("ns32", 20, None, 3, 6.0, 1.0),
+    ("bin32", 20, 1, 5, 6.0, 0.5),
+    ("bin64", 20, 1, 5, 6.0, 0.5),
+    ("ter32", 20, 2, 5, 6.0, 0.5),
+    ("ter64", 20, 2, 5, 6.0, 0.5),
+    ("bindef64", 20, 4, 6, 3.0, 0.5),
+    ("terdef64", 20, 4, 6, 3.0, 0.5),
+]
+FULL = [
+    # binary 256^2, omega = 0, spinodal c, 1000 steps
+    ("bin256", 1000, 100, None, 0.0, 0.0),
+    # ternary 512^2, omega = 0, c_i = 1/3 + U(+-0.02), 2000 steps
+    ("ter512", 2000, 101, None, 0.0, 0.0),
+]
+
+NPROJ = 8
+KLOW = 16
+
+
+def initial_state(model: int, n: int, lx: float, phase_seed, w_seed, kmax, rms):
+    """Returns (real phase fields, omega_hat) of a scenario."""
+    p1 = p2 = None
+    if model == 1:
+        p1 = fields.spinodal_binary(n, phase_seed)
+    elif model == 2:
+        p1, p2 = fields.spinodal_ternary(n, phase_seed)
+    w = None
+    if w_seed is not None:
+        w = fields.random_vorticity_hat(n, w_seed, kmax=kmax, rms=rms, lx=lx)
+    return p1, p2, w
+
+
+def apply_initial(sim, model, p1, p2, w):
+    """init.c INIT_READ_DATA order: phase fields via dfft + truncation, omega_hat set after."""
+    if model >= 1:
+        sim.set_phase_real(p1, p2)
+    if w is not None:
+        st = sim.get_state()
+        st[0] = w
+        sim.set_state(*st)
+
+
+def fingerprint(spec: np.ndarray, seed: int = 1000) -> dict:
+    """Size-independent summary of a spectral field (n x (n/2+1) complex):
+    the block |m| <= KLOW, j <= KLOW; NPROJ random projections over all modes;
+    the L2 norm; the k = 0 mode."""
+    n = spec.shape[0]
+    rows = list(range(0, KLOW + 1)) + list(range(n - KLOW, n))
+    low = spec[rows, : KLOW + 1]
+    flat = spec.reshape(-1)
+    proj = []
+    for r in range(NPROJ):
+        u = fields.uniform(seed + r, 2 * flat.size)
+        wgt = (2 * u[: flat.size] - 1) + 1j * (2 * u[flat.size:] - 1)
+        proj.append(np.sum(wgt * flat))
+    return dict(low=low, proj=np.array(proj), norm=float(np.sqrt(np.sum(np.abs(flat) ** 2))),
+                k0=complex(spec[0, 0]))
+
+
+def fingerprint_rel_err(fp_ref: dict, fp: dict) -> float:
+    """max over the parts of ||part - ref|| / ||field||-scaled reference."""
+    e_low = np.linalg.norm(fp["low"] - fp_ref["low"]) / max(np.linalg.norm(fp_ref["low"]), 1e-300)
+    e_proj = np.linalg.norm(fp["proj"] - fp_ref["proj"]) / max(np.linalg.norm(fp_ref["proj"]), 1e-300)
+    e_norm = abs(fp["norm"] - fp_ref["norm"]) / max(fp_ref["norm"], 1e-300)
+    return float(max(e_low, e_proj, e_norm))
+
+
+def make_small(O):
+    for name, steps, ps, ws, kmax, rms in SMALL:
+        p = O.ref_config_params(name)
+        R = O.RefLib(name)
+        n = p["nx"]
+        p1, p2, w = initial_state(p["model"], n, p["lx"], ps, ws, kmax, rms)
+        apply_initial(R, p["model"], p1, p2, w)
+        s0 = R.get_state()
+        r0 = R.rhs()
+        R.set_state(*s0)
+        fe0 = R.free_energy() if p["model"] >= 1 else (0.0, 0.0)
+        ke0 = R.kinetic_energy()
+        R.step(steps)
+        s1 = R.get_state()
+        out = dict(params=json.dumps(p), steps=steps)
+        for k, a in enumerate(s0):
+            out[f"init{k}"] = a
+        for k, a in enumerate(r0):
+            out[f"rhs{k}"] = a
+        for k, a in enumerate(s1):
+            out[f"final{k}"] = a
+        out["fe0"] = np.array(fe0)
+        out["ke0"] = np.array(ke0)
+        # FFT pair of the reference's fft.c on a seeded field
+        x = fields.uniform(77, n * n).reshape(n, n) - 0.5
+        out["fft_in"] = x
+        out["fft_dfft"] = R.dfft(x)
+        out["fft_ifft"] = R.ifft(out["fft_dfft"])
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print("wrote", name)
+
+
+def make_full(O):
+    for name, steps, ps, ws, kmax, rms in FULL:
+        p = O.ref_config_params(name)
+        R = O.RefLib(name, nthreads=min(8, os.cpu_count() or 1))
+        n = p["nx"]
+        p1, p2, w = initial_state(p["model"], n, p["lx"], ps, ws, kmax, rms)
+        apply_initial(R, p["model"], p1, p2, w)
+        s0 = R.get_state()
+        R.step(steps)
+        s1 = R.get_state()
+        out = dict(params=json.dumps(p), steps=steps)
+        for k, a in enumerate(s1):
+            fp = fingerprint(a)
+            for key, v in fp.items():
+                out[f"final{k}_{key}"] = np.asarray(v)
+            out[f"init{k}_k0"] = np.asarray(complex(s0[k][0, 0]))
+        np.savez_compressed(os.path.join(HERE, f"{name}_fp.npz"), **out)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    import oracle as O
+    O.build_ref.build_all()
+    make_small(O)
+    if "--full" in sys.argv:
+        make_full(O)

@@ -1,0 +1,151 @@
+"""CPU tests of the oracle: the FFT, the C restatement against the reference's
+own compiled code (golden fixtures made by tests/golden/make_golden.py, and live
+when oracle/_ref is built), and analytic known answers."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import make_golden as MG
+from _golden import SMALL_CONFIGS, load_small, load_full, rel_l2
+from chns_b200 import fields
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    O.build_oracle_lib()
+
+
+@pytest.mark.parametrize("n", [32, 64, 256, 512])
+def test_fft_matches_numpy(n):
+    p = dict(model=0, nx=n, ny=n, lx=2 * math.pi, ly=2 * math.pi, dt=1e-3, nu=0.01)
+    o = O.Oracle(p)
+    x = fields.uniform(5, n * n).reshape(n, n) - 0.5
+    X = o.dfft(x)
+    ref = np.fft.rfft2(x)
+    assert np.abs(X - ref).max() <= 1e-13 * np.abs(ref).max()
+    y = o.ifft(X)
+    assert np.abs(y - x).max() <= 1e-14
+    # c2r of a non-Hermitian half spectrum follows numpy/FFTW: Im of the j=0, n/2 bins ignored
+    rng = np.random.default_rng(0)
+    Z = rng.standard_normal(X.shape) + 1j * rng.standard_normal(X.shape)
+    assert np.abs(o.ifft(Z) - np.fft.irfft2(Z, s=(n, n))).max() <= 1e-13
+
+
+@pytest.mark.parametrize("name", SMALL_CONFIGS)
+def test_restatement_matches_reference_golden(name):
+    g = load_small(name)
+    p = g["params"]
+    o = O.Oracle(p)
+    o.set_state(*g["init"])
+    for a, b in zip(o.rhs(), g["rhs"]):
+        assert rel_l2(a, b) <= 1e-14, name
+    o.set_state(*g["init"])
+    if p["model"] >= 1:
+        fe = o.free_energy()
+        assert abs(fe[0] - g["fe0"][0]) <= 1e-11 and abs(fe[1] - g["fe0"][1]) <= 1e-11
+    ke = o.kinetic_energy()
+    assert np.allclose(ke, g["ke0"][: len(ke)], atol=1e-11, rtol=0)
+    o.step(g["steps"])
+    for a, b in zip(o.get_state(), g["final"]):
+        assert rel_l2(a, b) <= 1e-13, name
+    # the FFT behind the reference's fft.c
+    assert rel_l2(o.dfft(g["fft_in"]), g["fft_dfft"]) <= 1e-14
+    assert rel_l2(o.ifft(g["fft_dfft"]), g["fft_ifft"]) <= 1e-14
+
+
+@pytest.mark.parametrize("name", ["bin32", "ter32", "bindef64", "ns32"])
+def test_restatement_bitwise_vs_live_reference(name):
+    if not os.path.isfile(O.build_ref.lib_path(name)):
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    p = O.ref_config_params(name)
+    R = O.RefLib(name)
+    for k in ("dt", "nu", "epsilon", "lambda", "sigma", "sigma12", "sigma13", "sigma23", "xlambda"):
+        if k in p:
+            assert R.param(k) == p[k]
+    o = O.Oracle(p)
+    n = p["nx"]
+    seed = 1234
+    p1, p2, w = MG.initial_state(p["model"], n, p["lx"], seed, seed + 1, 5.0, 0.7)
+    MG.apply_initial(R, p["model"], p1, p2, w)
+    MG.apply_initial(o, p["model"], p1, p2, w)
+    R.step(7)
+    o.step(7)
+    for a, b in zip(o.get_state(), R.get_state()):
+        assert np.array_equal(a, b), name
+
+
+def test_restatement_cfg0_full_fingerprint():
+    """BASELINE configuration 0 (binary 256^2, 1000 steps) against the reference run."""
+    g = load_full("bin256")
+    p = g["params"]
+    o = O.Oracle(p, nthreads=1)
+    p1, p2, w = MG.initial_state(p["model"], p["nx"], p["lx"], 100, None, 0, 0)
+    MG.apply_initial(o, p["model"], p1, p2, w)
+    o.step(g["steps"])
+    for k, a in enumerate(o.get_state()):
+        fp = MG.fingerprint(a)
+        ref = {key: g[f"final{k}_{key}"] for key in ("low", "proj", "norm")}
+        assert MG.fingerprint_rel_err(ref, fp) <= 1e-12
+
+
+@pytest.mark.slow
+def test_restatement_cfg1_full_fingerprint():
+    g = load_full("ter512")
+    p = g["params"]
+    o = O.Oracle(p, nthreads=8)
+    p1, p2, w = MG.initial_state(p["model"], p["nx"], p["lx"], 101, None, 0, 0)
+    MG.apply_initial(o, p["model"], p1, p2, w)
+    o.step(g["steps"])
+    for k, a in enumerate(o.get_state()):
+        fp = MG.fingerprint(a)
+        ref = {key: g[f"final{k}_{key}"] for key in ("low", "proj", "norm")}
+        assert MG.fingerprint_rel_err(ref, fp) <= 1e-12
+
+
+def test_taylor_green_decays_exactly():
+    """u.grad w = 0 for the Taylor-Green vortex w = 2 sin x sin y: ETD2RK gives exp(-2 nu t)."""
+    n = 32
+    p = dict(model=0, nx=n, ny=n, lx=2 * math.pi, ly=2 * math.pi, dt=1e-2, nu=0.05)
+    o = O.Oracle(p)
+    x = np.arange(n) * (2 * math.pi / n)
+    w0 = 2 * np.sin(x)[:, None] * np.sin(x)[None, :]
+    o.set_state(o.dfft(w0))
+    o.step(50)
+    w = o.ifft(o.get_state()[0])
+    assert np.abs(w - w0 * math.exp(-2 * p["nu"] * 0.5)).max() <= 1e-12
+
+
+def test_mean_concentration_conserved():
+    for name in ("bin32", "ter32"):
+        g = load_small(name)
+        o = O.Oracle(g["params"])
+        o.set_state(*g["init"])
+        m0 = [s[0, 0] for s in o.get_state()[1:]]
+        o.step(50)
+        m1 = [s[0, 0] for s in o.get_state()[1:]]
+        for a, b in zip(m0, m1):
+            assert abs(a - b) <= 1e-12 * abs(a)
+
+
+def test_linear_ch_growth_rate():
+    """A small single mode about c0 grows at -lambda k^2 (A f'(c0) + kappa k^2) (binary,
+    A = 24 sigma/eps, kappa = 1.5 sigma eps, f' = 1 - 6c + 6c^2), with omega = 0."""
+    n = 64
+    p = O.ref_config_params("bin64")
+    o = O.Oracle(p)
+    x = np.arange(n) * (p["lx"] / n)
+    kk, c0, amp = 5, 0.5, 1e-7
+    c = c0 + amp * np.cos(kk * x)[:, None] * np.ones(n)[None, :]
+    o.set_phase_real(c)
+    steps = 20
+    o.step(steps)
+    ch = o.get_state()[1]
+    ratio = abs(ch[kk, 0]) / (amp * n * n / 2)
+    A = 24 * p["sigma"] / p["epsilon"]
+    kap = 1.5 * p["sigma"] * p["epsilon"]
+    fp = 1 - 6 * c0 + 6 * c0 ** 2
+    rate = -p["lambda"] * kk ** 2 * (A * fp + kap * kk ** 2)
+    assert abs(ratio - math.exp(rate * steps * p["dt"])) <= 1e-6 * math.exp(rate * steps * p["dt"])
