@@ -1,0 +1,440 @@
+#!/usr/bin/env python3
+"""Benchmark of the ETD2RK CHNS step on B200 (one JSON line on rank 0).
+
+Workload: binary CHNS on a 4096^2 grid (the configuration the metric is quoted
+on): Kolmogorov forcing F0 sin(4y) x-hat, F0 = 1, nu = M = 1e-3, sigma = 0.1,
+eps = 2 dx, 64 tanh drops of radius 0.3 on c = 0 and random vorticity modes
+|k| <= 8 at rms 0.1, all seeded synthetic inputs.  FP32 transforms and
+pointwise arithmetic, ETD coefficients from FP64 (series for small |c h|),
+k = 0 modes in FP64.  A "step" is one full ETD2RK step (both stages).
+
+  value    : steps/s of the whole job (all ranks), state resident in HBM
+  e2e      : steps/s through the reference-facing call with HOST buffers: every
+             step uploads the FFTW-layout state from pinned memory, steps once and
+             reads it back (the contract of the drop-in etd2rk())
+  roofline : the dominant kernel's algorithmic bytes / its CUDA-event time
+  cpu_baseline : the reference's own etd2rk() (compiled here, oracle/_ref)
+             timed on the host cores on a sample of the same workload
+
+--impl reference times the reference's CPU implementation (oracle/_ref) on the
+same metric; multi-GPU runs are independent replicas (the step does not shard;
+one all-to-all per transform would be the only way to split a field).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ternary-chns_b200"))
+
+N_DEFAULT = 4096
+METRIC = "steps/s @4096^2 binary CHNS ETD2RK (FP32, FP64 coefficients)"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload_params(n: int, precision: int, coef_mode: int = 1, dt: float = 2e-4) -> dict:
+    lx = 2 * math.pi
+    p = dict(model=1, precision=precision, nx=n, ny=n, lx=lx, ly=lx, dt=dt, nu=1e-3, sigma=0.1,
+             epsilon=2.0 * (lx / n), coef_mode=coef_mode, force_amp=1.0, force_k=4.0)
+    p["lambda"] = 1e-3
+    return p
+
+
+def initial_fields(n: int):
+    from chns_b200 import fields
+
+    lx = 2 * math.pi
+    c0 = fields.drops_binary(n, 42, ndrops=64, radius=0.3, lx=lx, epsilon=2.0 * (lx / n))
+    w0 = fields.random_vorticity_hat(n, 43, kmax=8.0, rms=0.1, lx=lx)
+    return c0, w0
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[3 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def kernel_bytes(n: int, jt: int, rsz: int) -> dict:
+    """Algorithmic bytes per launch of the binary stage kernels:
+    complex fields of the S/H layouts hold (n/2+1) x n values, G fields (jt+1) x n;
+    P1 loads only the modes inside the truncation disc."""
+    cx = 2 * rsz
+    S = (n // 2 + 1) * n * cx
+    G = (jt + 1) * n * cx
+    disc = 0
+    for j in range(jt + 1):
+        pass
+    return {
+        "spec_inv": None,  # filled by caller with the exact disc size
+        "row_adv": 7 * G + 3 * S,
+        "spec_fwd_c": 3 * S + S + G + S + S + S,   # HA,HF,HB + c, -> nw, G_mu, c, saved
+        "row_force": 3 * G + 2 * S,
+        "spec_curl_w": 2 * S + S + S + S + S,      # HFX,HFY,nw,w -> w, saved
+    }
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import chns_b200 as C
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    n = args.n
+    c0, w0 = initial_fields(n)
+    L = C.load_library()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---------------- device-resident throughput (FP32) ----------------
+    ctx = C.Context(workload_params(n, C.FP32))
+    ctx.set_phase_real(c0)
+    st = ctx.get_state()
+    st[0] = w0
+    ctx.set_state(*st)
+    stream = torch.cuda.Stream()
+    L.chns_set_stream(ctx.handle, ctypes_stream(stream))
+    ctx.step(args.warmup)
+    ctx.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        ctx.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    t_max = ms
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    ms_per_step = t_max / args.steps
+    value = world * args.steps / (t_max / 1e3)
+    launches = ctx.launches_per_step() * args.steps
+    fe, ke, rc = ctx.diagnostics()
+    finite = rc == 0
+
+    # ---------------- per-kernel times of one step (events between launches) ----------------
+    prof = profile_kernels(ctx, L, stream, reps=max(3, min(10, args.steps)))
+
+    # ---------------- FP64 plain step on the same workload ----------------
+    ctx64 = C.Context(workload_params(n, C.FP64, coef_mode=0))
+    ctx64.set_state(*ctx.get_state()) if False else None
+    ctx64.set_phase_real(c0)
+    s64 = ctx64.get_state()
+    s64[0] = w0
+    ctx64.set_state(*s64)
+    L.chns_set_stream(ctx64.handle, ctypes_stream(stream))
+    ctx64.step(2)
+    ctx64.synchronize()
+    k64 = max(3, args.steps // 4)
+    ev0.record(stream)
+    ctx64.step(k64)
+    ev1.record(stream)
+    ev1.synchronize()
+    fp64_sps = k64 / (ev0.elapsed_time(ev1) / 1e3)
+    ctx64.close()
+
+    # ---------------- end to end through the host-buffer call ----------------
+    e2e = e2e_host_loop(ctx, stream, max(3, min(args.steps, 10)))
+
+    rsz = 4
+    jt = n // 4
+    out = None
+    if rank == 0:
+        hbm, src = peaks()
+        dom = max(prof["per_kernel_ms"].items(), key=lambda kv: kv[1]) if prof["per_kernel_ms"] else (None, None)
+        kb = prof["bytes"]
+        roof = None
+        if dom[0]:
+            ach = kb[dom[0]] / (dom[1] / 1e3) / 1e9
+            roof = {"kernel": dom[0], "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "peak_source": src,
+                    "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": None,
+                    "algorithmic_bytes_per_launch": kb[dom[0]], "ms_per_launch": round(dom[1], 4)}
+        model_bytes = 120 * n * n * rsz
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"binary CHNS {n}^2, Kolmogorov forcing, 64 drops, dt 2e-4",
+                       "grid": n, "model": "binary", "precision": "fp32+fp64 coefficients",
+                       "l2": "inputs larger than L2 (state and intermediates ~1 GB)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": e2e,
+            "roofline": roof,
+            "step_model": {"bytes_per_step": model_bytes, "achieved_gbs": round(model_bytes * value / world / 1e9, 1),
+                           "frac_of_peak": round(model_bytes * value / world / 1e9 / hbm, 4),
+                           "note": "whole step against the 120 N^2 s bytes/step model"},
+            "fp64_steps_per_s": round(fp64_sps, 3),
+            "fp32_over_fp64": round((value / world) / fp64_sps, 3),
+            "per_kernel_ms": prof["per_kernel_ms"],
+            "gpu_launches": launches,
+            "state_finite": bool(finite),
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(n, args.cpu_steps)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if out:
+        print(json.dumps(out))
+
+
+def ctypes_stream(stream):
+    import ctypes
+
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def profile_kernels(ctx, L, stream, reps: int):
+    """Times every kernel of one step with CUDA events recorded between launches
+    on the context's stream (outside the graph; same kernels, same arguments)."""
+    import ctypes
+
+    import torch
+
+    maxk = 64
+    arr = (ctypes.c_float * maxk)()
+    names = (ctypes.c_int * maxk)()
+    L.chns_profile_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    L.chns_profile_step.restype = ctypes.c_int
+    nk = L.chns_profile_step(ctx.handle, reps, arr, names, maxk)
+    kinds = {0: "spec_inv", 1: "row_adv", 2: "spec_fwd_c", 3: "row_force", 4: "spec_curl_w", 5: "row_adv_b"}
+    per = {}
+    cnt = {}
+    for k in range(max(nk, 0)):
+        nm = kinds.get(names[k], str(names[k]))
+        per[nm] = per.get(nm, 0.0) + arr[k]
+        cnt[nm] = cnt.get(nm, 0) + 1
+    per_launch = {k: per[k] / cnt[k] for k in per}
+    n = ctx.nx
+    jt = n // 4
+    cx = 8 if ctx.params.get("precision", 0) == 1 else 16
+    S = (n // 2 + 1) * n * cx
+    G = (jt + 1) * n * cx
+    disc = disc_modes(n) * cx
+    bytes_ = {
+        "spec_inv": 2 * disc + 7 * G,
+        "row_adv": 7 * G + 3 * S,
+        "spec_fwd_c": 3 * S + S + S + G + S + S,
+        "row_force": 3 * G + 2 * S,
+        "spec_curl_w": 2 * S + S + S + S + S,
+    }
+    return {"per_kernel_ms": {k: round(v, 4) for k, v in per_launch.items()}, "bytes": bytes_}
+
+
+def disc_modes(n: int) -> int:
+    fx = 1.0
+    dax = (n / 4.0) * fx
+    lim2 = dax * dax
+    cnt = 0
+    for j in range(n // 2 + 1):
+        ky = fx * j
+        for m in range(n // 2 + 1):
+            kx = fx * m
+            if kx * kx + ky * ky > lim2:
+                break
+            cnt += 1 if m == 0 else 2
+    return cnt
+
+
+def e2e_host_loop(ctx, stream, steps: int):
+    """The drop-in contract: host FFTW-layout state in, one step, state out."""
+    import numpy as np
+    import torch
+
+    n = ctx.nx
+    shape = (n, n // 2 + 1)
+    pin = [torch.empty(shape[0] * shape[1] * 2, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    st = ctx.get_state()
+    for a, s in zip(pin, st):
+        a.numpy()[:] = s.view(np.float64).ravel()
+    L = ctx.L
+    ptrs = [a.data_ptr() for a in pin]
+    import ctypes
+
+    def one():
+        rc = L.chns_set_state(ctx.handle, ctypes.c_void_p(ptrs[0]), ctypes.c_void_p(ptrs[1]), None, 0)
+        assert rc == 0
+        rc = L.chns_step(ctx.handle, 1)
+        assert rc == 0
+        rc = L.chns_get_state(ctx.handle, ctypes.c_void_p(ptrs[0]), ctypes.c_void_p(ptrs[1]), None, 0)
+        assert rc == 0
+
+    one()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    ev1.record(stream)
+    ev1.synchronize()
+    wall = time.perf_counter() - t0
+    bytes_ = 2 * shape[0] * shape[1] * 16
+    return {"value": round(steps / wall, 3), "unit": "steps/s", "h2d_bytes_per_step": bytes_,
+            "d2h_bytes_per_step": bytes_, "note": "chns_set_state(host) + chns_step(1) + chns_get_state(host)"}
+
+
+def cpu_baseline(n: int, steps: int, threads: int | None = None):
+    """The reference's own etd2rk() (oracle/_ref/bin<n>) on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    name = f"bin{n}"
+    if not os.path.isfile(O.build_ref.lib_path(name)):
+        return {"value": None, "unit": "steps/s", "kind": "reference", "cores": 0,
+                "sample": f"oracle/_ref/{name} not built"}
+    thr = threads or os.cpu_count() or 1
+    R = O.RefLib(name, nthreads=thr)
+    c0, _ = initial_fields(n) if n >= 256 else (None, None)
+    R.set_phase_real(c0)
+    R.step(1)
+    t0 = time.perf_counter()
+    R.step(steps)
+    el = time.perf_counter() - t0
+    return {"value": round(steps / el, 5), "unit": "steps/s", "kind": "reference", "cores": thr,
+            "sample": f"{steps} reference etd2rk() steps at {n}^2 binary (unforced: the reference has no working "
+                      f"forcing), FFTW replaced by the oracle FFT on {thr} threads, reference loops single-threaded, "
+                      f"-O2"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    n = args.n
+    name = f"bin{n}"
+    if not os.path.isfile(O.build_ref.lib_path(name)):
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/{name}/libref.so not built"}))
+        return
+    thr = os.cpu_count() or 1
+    R = O.RefLib(name, nthreads=thr)
+    c0, _ = initial_fields(n)
+    R.set_phase_real(c0)
+    R.step(args.warmup)
+    t0 = time.perf_counter()
+    R.step(args.steps)
+    el = time.perf_counter() - t0
+    v = args.steps / el
+    sample = (f"{args.steps} reference etd2rk() steps at {n}^2 binary (unforced), FFTW replaced by the oracle FFT on "
+              f"{thr} threads, reference loops single-threaded")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 / v, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"binary CHNS {n}^2 (reference etd2rk, CPU)", "grid": n},
+        "cpu_baseline": {"value": round(v, 5), "unit": "steps/s", "kind": "reference", "cores": thr, "sample": sample},
+        "e2e": {"value": round(v, 5), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="chns", choices=["chns", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        if args.n == N_DEFAULT and args.steps > 10:
+            args.steps = 10  # one reference step at 4096^2 takes seconds
+            args.warmup = 1
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,130 @@
+/*
+ * chns.h -- C ABI of the B200-native ETD2RK step for 2D pseudospectral
+ * Cahn-Hilliard-Navier-Stokes (binary and ternary phase-field flows).
+ *
+ * Drop-in boundary for phynadia/Ternary-CHNS's time step.  The reference's
+ * step is   void etd2rk(fftw_complex *cwz [, *cphi | , *cphi1, *cphi2])
+ * (etd2rk.c:14-20, declared unprototyped at global.h:94), which updates the
+ * state in place in FFTW's spectral layout and takes every parameter from
+ * compile-time #defines (global.h:19-45,102-143) and process globals.  This ABI
+ * keeps the fields, the layout and the arithmetic of that step, with explicit
+ * parameters and context instead of globals:
+ *
+ *   state arrays : nx x (ny/2+1) complex, interleaved doubles, row i = kx[i]
+ *                  (IDXC(i,j) = j + Ny2*i, global.h:13), i.e. the arrays
+ *                  cwz, cphi / cphi1, cphi2 of the reference.
+ *   real arrays  : nx x ny doubles, row-major, row i = x (the layout of the
+ *                  reference's read_array_real / write_array_real files,
+ *                  read_array.c:20-29, write_array.c:29-38).
+ *
+ * All functions return CHNS_OK (0) or a negative status; none aborts.  A context
+ * owns its device memory, tables and CUDA stream; calls on one context are
+ * stream-ordered and must not be made concurrently from several threads.  The
+ * literal drop-in etd2rk() with the reference's own signature is in
+ * ternary-chns_b200/csrc/etd2rk_dropin.c (it is compiled against the reference's
+ * global.h so that it sees the configuration macros).
+ */
+#ifndef CHNS_H
+#define CHNS_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHNS_OK 0
+#define CHNS_ERR_ARG (-1)         /* bad argument or parameter */
+#define CHNS_ERR_CUDA (-2)        /* a CUDA call failed */
+#define CHNS_ERR_NONFINITE (-3)   /* the state holds NaN/Inf or blew up */
+#define CHNS_ERR_TIMEOUT (-4)     /* a bounded device wait ran out */
+#define CHNS_ERR_UNSUPPORTED (-5) /* size or option not supported */
+#define CHNS_ERR_NOMEM (-6)       /* device or host allocation failed */
+
+enum { CHNS_MODEL_NS = 0, CHNS_MODEL_BINARY = 1, CHNS_MODEL_TERNARY = 2 };
+enum { CHNS_FP64 = 0, CHNS_FP32 = 1 };
+/* ETD phi-function coefficients: REFERENCE evaluates etd2rk.c's direct formulas
+ * (etd2rk.c:88-206, with its small-|c| branches) on the host in double, so
+ * the FP64 step reproduces the reference; ACCURATE uses expm1 and a series for
+ * small |c h| (more accurate than the reference for small |c h|). */
+enum { CHNS_COEF_REFERENCE = 0, CHNS_COEF_ACCURATE = 1 };
+enum { CHNS_HOST = 0, CHNS_DEVICE = 1 };
+
+typedef struct chns_params {
+    int model;          /* CHNS_MODEL_*: none / BINARY / TERNARY (macro.h) */
+    int precision;      /* CHNS_FP64 or CHNS_FP32 */
+    int nx, ny;         /* Nx, Ny (global.h:23-24); nx == ny, power of two, 32..4096 */
+    double lx, ly;      /* box (global.h:20-21) */
+    double dt, nu;      /* dt, nu (global.h:30-31) */
+    double lambda;      /* mobility (global.h:104,132) */
+    double sigma;       /* binary surface tension (global.h:102) */
+    double epsilon;     /* interface width (global.h:103,131) */
+    double sigma12, sigma13, sigma23; /* ternary sigma_ij (global.h:127-129) */
+    double xlambda;     /* ternary Xlambda (global.h:133) */
+    double dealias_div; /* truncation radius (nx/dealias_div)*2pi/lx; the reference's is 4 (functions.c:56) */
+    int coef_mode;      /* CHNS_COEF_* */
+    double force_amp;   /* Kolmogorov forcing F0 sin(kf y) x-hat on the flow; 0 = off.  Not in the reference */
+    double force_k;     /* kf; kf*ly/(2 pi) must be an integer <= ny/2 */
+} chns_params;
+
+typedef struct chns_ctx chns_ctx;
+
+/* Fills p with the reference's defaults (global.h:19-45 and the BINARY /
+ * TERNARY blocks :102-143) for the given model and grid n. */
+void chns_default_params(chns_params *p, int model, int n);
+
+/* Creates a context: device buffers, truncation table, ETD coefficient tables,
+ * twiddles, stream.  Replaces the allocation/plan/kxky set-up of main.c:43-211. */
+int chns_create(const chns_params *p, chns_ctx **out);
+int chns_destroy(chns_ctx *ctx);
+
+/* Uses `stream` (a cudaStream_t) for all later work instead of the context's own. */
+int chns_set_stream(chns_ctx *ctx, void *stream);
+int chns_synchronize(chns_ctx *ctx);
+
+/* State in FFTW layout (w = cwz, c1 = cphi or cphi1, c2 = cphi2); pointers on
+ * the host or the device (where = CHNS_HOST / CHNS_DEVICE).  Unused fields may
+ * be NULL. */
+int chns_set_state(chns_ctx *ctx, const double *w, const double *c1, const double *c2, int where);
+int chns_get_state(chns_ctx *ctx, double *w, double *c1, double *c2, int where);
+
+/* Initial phase field(s) from real nx x ny arrays: dfft + truncation, omega = 0
+ * (init.c:78-87,221-225,253-262 with INIT_READ_DATA). */
+int chns_set_phase_real(chns_ctx *ctx, const double *p1, const double *p2, int where);
+
+/* nsteps ETD2RK steps on the resident state (etd2rk.c:14-224 each), replayed
+ * from a CUDA graph.  Asynchronous: returns after enqueueing. */
+int chns_step(chns_ctx *ctx, int nsteps);
+
+/* Right-hand side N(u) of the current state: the output of potential() +
+ * nonlin() (etd2rk.c:28 / 40-51), in FFTW layout.  The state is unchanged. */
+int chns_rhs(chns_ctx *ctx, double *nw, double *nc1, double *nc2, int where);
+
+/* fft.c on the device: dfft = unnormalised 2D r2c of a real nx x ny array into
+ * FFTW layout; ifft = c2r then x 1/(nx ny) (fft.c:11-31). */
+int chns_dfft(chns_ctx *ctx, const double *real, double *spec, int where);
+int chns_ifft(chns_ctx *ctx, const double *spec, double *real, int where);
+
+/* Free energy (free_energy.c:3-157) and kinetic energy (kinetic_energy.c:3-144)
+ * of the current state: out_fe[2] = {bulk, gradient}; out_ke[3] = {<|u|^2/2>,
+ * phase-1 mean, phase-2 mean}. */
+int chns_diagnostics(chns_ctx *ctx, double *out_fe, double *out_ke);
+
+/* Kernel launches of one step (known after the first chns_step). */
+int chns_launches_per_step(const chns_ctx *ctx);
+
+/* Tracing: runs `reps` steps launching the kernels one by one (not from the
+ * graph) with a CUDA event recorded after each launch on the context's stream;
+ * writes the mean duration of every launch of one step to ms[] and its kind to
+ * kind[] (0 spectral inverse pass, 1 row advection pass, 2 spectral forward pass
+ * of c, 3 row force pass, 4 spectral curl/ETD pass of w, 5 second row advection
+ * pass).  Returns the number of launches per step, or a negative status.
+ * The state advances by `reps` steps. */
+int chns_profile_step(chns_ctx *ctx, int reps, float *ms, int *kind, int maxk);
+
+const char *chns_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,220 @@
+"""Host-side mirror of the reference's step interface over the C ABI (include/chns.h).
+
+The reference advances the state with etd2rk(cwz, cphi[, cphi2]) in FFTW's
+spectral layout (etd2rk.c:14-20); ``Context.step`` is that call on the GPU, with
+the parameters of global.h passed explicitly (``params``) instead of compiled in.
+
+Arrays are numpy: spectral fields (nx, ny//2+1) complex128 in FFTW layout,
+real fields (nx, ny) float64.  There is no CPU fallback: without the built
+library (ternary-chns_b200/lib/libchns_b200.so) or without a GPU every call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "lib", "libchns_b200.so")
+
+MODEL_NS, MODEL_BINARY, MODEL_TERNARY = 0, 1, 2
+FP64, FP32 = 0, 1
+COEF_REFERENCE, COEF_ACCURATE = 0, 1
+HOST, DEVICE = 0, 1
+
+STATUS = {0: "ok", -1: "bad argument", -2: "CUDA error", -3: "non-finite or blown-up state",
+          -4: "device wait timed out", -5: "unsupported size or option", -6: "out of memory"}
+
+
+class ChnsError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({status})")
+        self.status = status
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("model", ctypes.c_int), ("precision", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("dt", ctypes.c_double), ("nu", ctypes.c_double),
+        ("lam", ctypes.c_double), ("sigma", ctypes.c_double), ("epsilon", ctypes.c_double),
+        ("sigma12", ctypes.c_double), ("sigma13", ctypes.c_double), ("sigma23", ctypes.c_double),
+        ("xlambda", ctypes.c_double), ("dealias_div", ctypes.c_double), ("coef_mode", ctypes.c_int),
+        ("force_amp", ctypes.c_double), ("force_k", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libchns_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.isfile(path):
+        raise FileNotFoundError(f"{path} is missing: run __graft_entry__.build() (no CPU fallback exists)")
+    L = ctypes.CDLL(path)
+    vp, dp, ip = ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int
+    L.chns_default_params.argtypes = [ctypes.POINTER(Params), ip, ip]
+    L.chns_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(vp)]
+    L.chns_destroy.argtypes = [vp]
+    L.chns_set_stream.argtypes = [vp, vp]
+    L.chns_synchronize.argtypes = [vp]
+    L.chns_set_state.argtypes = [vp, dp, dp, dp, ip]
+    L.chns_get_state.argtypes = [vp, dp, dp, dp, ip]
+    L.chns_set_phase_real.argtypes = [vp, dp, dp, ip]
+    L.chns_step.argtypes = [vp, ip]
+    L.chns_rhs.argtypes = [vp, dp, dp, dp, ip]
+    L.chns_dfft.argtypes = [vp, dp, dp, ip]
+    L.chns_ifft.argtypes = [vp, dp, dp, ip]
+    L.chns_diagnostics.argtypes = [vp, dp, dp]
+    L.chns_launches_per_step.argtypes = [vp]
+    L.chns_status_string.restype = ctypes.c_char_p
+    L.chns_status_string.argtypes = [ip]
+    _lib = L
+    return L
+
+
+def default_params(model: int, n: int) -> dict:
+    """The reference's global.h defaults for `model` on an n x n grid."""
+    L = load_library()
+    s = Params()
+    L.chns_default_params(ctypes.byref(s), model, n)
+    return params_to_dict(s)
+
+
+def params_to_dict(s: Params) -> dict:
+    d = {k: getattr(s, k) for k, _ in Params._fields_}
+    d["lambda"] = d.pop("lam")
+    return d
+
+
+def make_params(p: dict) -> Params:
+    s = Params()
+    s.model = int(p["model"])
+    s.precision = int(p.get("precision", FP64))
+    s.nx = int(p["nx"])
+    s.ny = int(p.get("ny", p["nx"]))
+    s.lx = float(p.get("lx", 2 * math.pi))
+    s.ly = float(p.get("ly", s.lx))
+    s.dt = float(p["dt"])
+    s.nu = float(p.get("nu", 0.0))
+    s.lam = float(p.get("lambda", 0.0))
+    s.sigma = float(p.get("sigma", 0.0))
+    s.epsilon = float(p.get("epsilon", 0.0))
+    s.sigma12 = float(p.get("sigma12", 0.0))
+    s.sigma13 = float(p.get("sigma13", 0.0))
+    s.sigma23 = float(p.get("sigma23", 0.0))
+    s.xlambda = float(p.get("xlambda", 2.0))
+    s.dealias_div = float(p.get("dealias_div", 4.0))
+    s.coef_mode = int(p.get("coef_mode", COEF_REFERENCE))
+    s.force_amp = float(p.get("force_amp", 0.0))
+    s.force_k = float(p.get("force_k", 0.0))
+    return s
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise ChnsError(rc, what)
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """One simulation on one GPU: the reference's state (cwz, cphi / cphi1, cphi2)
+    and its ETD2RK step."""
+
+    def __init__(self, params: dict):
+        self.L = load_library()
+        self.params = dict(params)
+        self._p = make_params(params)
+        h = ctypes.c_void_p()
+        _check(self.L.chns_create(ctypes.byref(self._p), ctypes.byref(h)), "chns_create")
+        self._h = h
+        self.model = self._p.model
+        self.nx, self.ny = self._p.nx, self._p.ny
+        self.shape = (self.nx, self.ny // 2 + 1)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.L.chns_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _spec(self, a):
+        a = np.ascontiguousarray(a, np.complex128)
+        if a.shape != self.shape:
+            raise ValueError(f"expected spectral shape {self.shape}, got {a.shape}")
+        return a
+
+    def set_state(self, w, c1=None, c2=None):
+        arrs = [self._spec(a) if a is not None else None for a in (w, c1, c2)]
+        _check(self.L.chns_set_state(self._h, *[_ptr(a) for a in arrs], HOST), "chns_set_state")
+
+    def get_state(self):
+        out = [np.empty(self.shape, np.complex128) for _ in range(self.model + 1)]
+        ptrs = [_ptr(a) for a in out] + [None] * (3 - len(out))
+        _check(self.L.chns_get_state(self._h, *ptrs, HOST), "chns_get_state")
+        return out
+
+    def set_phase_real(self, p1, p2=None):
+        a = np.ascontiguousarray(p1, np.float64)
+        b = np.ascontiguousarray(p2, np.float64) if p2 is not None else None
+        _check(self.L.chns_set_phase_real(self._h, _ptr(a), _ptr(b), HOST), "chns_set_phase_real")
+
+    def step(self, n: int = 1):
+        _check(self.L.chns_step(self._h, int(n)), "chns_step")
+
+    def synchronize(self):
+        _check(self.L.chns_synchronize(self._h), "chns_synchronize")
+
+    def rhs(self):
+        out = [np.empty(self.shape, np.complex128) for _ in range(self.model + 1)]
+        ptrs = [_ptr(a) for a in out] + [None] * (3 - len(out))
+        _check(self.L.chns_rhs(self._h, *ptrs, HOST), "chns_rhs")
+        return out
+
+    def dfft(self, real):
+        x = np.ascontiguousarray(real, np.float64)
+        out = np.empty(self.shape, np.complex128)
+        _check(self.L.chns_dfft(self._h, _ptr(x), _ptr(out), HOST), "chns_dfft")
+        return out
+
+    def ifft(self, spec):
+        s = self._spec(spec)
+        out = np.empty((self.nx, self.ny), np.float64)
+        _check(self.L.chns_ifft(self._h, _ptr(s), _ptr(out), HOST), "chns_ifft")
+        return out
+
+    def diagnostics(self):
+        """((bulk, gradient) free energy, (<|u|^2/2>, phase-1 mean, phase-2 mean)) of the state."""
+        fe = np.zeros(2)
+        ke = np.zeros(3)
+        rc = self.L.chns_diagnostics(self._h, _ptr(fe), _ptr(ke))
+        if rc not in (0, -3):
+            _check(rc, "chns_diagnostics")
+        return fe, ke, rc
+
+    def launches_per_step(self) -> int:
+        return self.L.chns_launches_per_step(self._h)

@@ -1,0 +1,655 @@
+// chns_api.cu -- the C ABI (include/chns.h): context, tables, state I/O, steps.
+//
+// Replaces the set-up of the reference's main.c:43-211 (allocation, plans,
+// wavenumbers, gamma_i/Delta) and its time-step entry etd2rk() (etd2rk.c:14-224)
+// for one GPU.  All tables are computed here on the host in double with the
+// reference's operand order (this file is compiled with -ffp-contract=off on
+// the host side), then uploaded once.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "chns_internal.h"
+
+namespace chns {
+#define CHNS_DECL(NN)                  \
+  const Launchers* launchers_f64_##NN(); \
+  const Launchers* launchers_f32_##NN();
+CHNS_DECL(32)
+CHNS_DECL(64)
+CHNS_DECL(128)
+CHNS_DECL(256)
+CHNS_DECL(512)
+CHNS_DECL(1024)
+CHNS_DECL(2048)
+CHNS_DECL(4096)
+
+const Launchers* launchers_f64(int logn) {
+  switch (logn) {
+    case 5: return launchers_f64_32();
+    case 6: return launchers_f64_64();
+    case 7: return launchers_f64_128();
+    case 8: return launchers_f64_256();
+    case 9: return launchers_f64_512();
+    case 10: return launchers_f64_1024();
+    case 11: return launchers_f64_2048();
+    case 12: return launchers_f64_4096();
+  }
+  return nullptr;
+}
+const Launchers* launchers_f32(int logn) {
+  switch (logn) {
+    case 5: return launchers_f32_32();
+    case 6: return launchers_f32_64();
+    case 7: return launchers_f32_128();
+    case 8: return launchers_f32_256();
+    case 9: return launchers_f32_512();
+    case 10: return launchers_f32_1024();
+    case 11: return launchers_f32_2048();
+    case 12: return launchers_f32_4096();
+  }
+  return nullptr;
+}
+}  // namespace chns
+
+namespace {
+
+int ilog2_exact(int n) {
+  int l = 0;
+  while ((1 << l) < n) l++;
+  return (1 << l) == n ? l : -1;
+}
+
+#define CK(call)                                  \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return CHNS_ERR_CUDA;  \
+  } while (0)
+
+// (e^z - 1 - z) / z^2 for the ACCURATE coefficient mode
+double phi2_z(double z) {
+  if (fabs(z) < 0.5) {
+    double term = 0.5, sum = 0.5;
+    for (int n = 1; n < 20; n++) {
+      term *= z / (double)(n + 2);
+      sum += term;
+    }
+    return sum;
+  }
+  return (expm1(z) - z) / (z * z);
+}
+
+// ETD coefficients of one wavenumber, etd2rk.c:88-97,102-111,117-127 (stage 1)
+// and :162-172,177-186,191-203 (stage 2), in the reference's operand order.
+void etd_coefs(const chns_params& p, double ksqr, double* o) {
+  const double dt = p.dt, nu = p.nu;
+  double c = -nu * ksqr;
+  double eta = exp(-nu * dt * ksqr);
+  double z1, z2;
+  if (p.coef_mode == CHNS_COEF_REFERENCE) {
+    z1 = (fabs(c) > 1e-12) ? (eta - 1.0) / c : dt;
+    z2 = (fabs(c) > 1e-12) ? (eta - 1.0 - c * dt) / (dt * c * c) : 0.5 * dt;
+  } else {
+    double z = c * dt;
+    z1 = (z != 0.0) ? dt * (expm1(z) / z) : dt;
+    z2 = dt * phi2_z(z);
+  }
+  double beta = 1.0, z1c = dt, z2c = 0.5 * dt;
+  if (p.model == CHNS_MODEL_BINARY) {
+    c = -1.5 * p.lambda * p.sigma * p.epsilon * ksqr * ksqr;
+    beta = exp(dt * c);
+    if (p.coef_mode == CHNS_COEF_REFERENCE) {
+      z1c = (fabs(c) > 1e-12) ? (beta - 1.0) / c : dt;
+      z2c = (fabs(c) != 0.0) ? (beta - 1.0 - c * dt) / (dt * c * c) : 0.5 * dt;
+    }
+  } else if (p.model == CHNS_MODEL_TERNARY) {
+    c = -0.75 * p.lambda * p.epsilon;
+    c *= ksqr * ksqr;
+    beta = exp(dt * c);
+    if (p.coef_mode == CHNS_COEF_REFERENCE) {
+      if (fabs(c) > 1e-12) {
+        z1c = (beta - 1.0) / c;
+        z2c = (beta - 1.0 - c * dt);
+        z2c /= (dt * c * c);
+      } else {
+        z1c = dt;
+        z2c = 0.5 * dt;
+      }
+    }
+  }
+  if (p.model != CHNS_MODEL_NS && p.coef_mode != CHNS_COEF_REFERENCE) {
+    double z = dt * c;
+    z1c = (z != 0.0) ? dt * (expm1(z) / z) : dt;
+    z2c = dt * phi2_z(z);
+  }
+  o[0] = eta;
+  o[1] = z1;
+  o[2] = z2;
+  o[3] = beta;
+  o[4] = z1c;
+  o[5] = z2c;
+}
+
+int validate(const chns_params* p) {
+  if (!p) return CHNS_ERR_ARG;
+  if (p->model < 0 || p->model > 2) return CHNS_ERR_ARG;
+  if (p->precision != CHNS_FP64 && p->precision != CHNS_FP32) return CHNS_ERR_ARG;
+  if (p->nx != p->ny) return CHNS_ERR_UNSUPPORTED;
+  const int l = ilog2_exact(p->nx);
+  if (l < 5 || l > 12) return CHNS_ERR_UNSUPPORTED;
+  if (!(p->lx > 0) || !(p->ly > 0) || !(p->dt > 0) || !(p->nu >= 0)) return CHNS_ERR_ARG;
+  if (!(p->dealias_div > 2.0)) return CHNS_ERR_ARG;  // the truncated band must stay below the Nyquist row
+  if (p->model != CHNS_MODEL_NS && !(p->epsilon > 0)) return CHNS_ERR_ARG;
+  if (p->coef_mode != CHNS_COEF_REFERENCE && p->coef_mode != CHNS_COEF_ACCURATE) return CHNS_ERR_ARG;
+  if (p->force_amp != 0.0) {
+    const double q = p->force_k * p->ly / (2.0 * M_PI);
+    const double r = nearbyint(q);
+    if (fabs(q - r) > 1e-9 || r < 1 || r > p->ny / 2) return CHNS_ERR_ARG;
+  }
+  return CHNS_OK;
+}
+
+void free_all(chns_ctx* c) {
+  if (!c) return;
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  void* ptrs[] = {c->state[0], c->state[1], c->state[2], c->saved[0], c->saved[1], c->saved[2], c->nw,
+                  c->coef, c->mrow, c->tw, c->k0, c->stage, c->realbuf, c->realdbl, c->red, c->redscratch};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  for (void* q : c->g)
+    if (q) cudaFree(q);
+  for (void* q : c->h)
+    if (q) cudaFree(q);
+  if (c->hostpin) cudaFreeHost(c->hostpin);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  free(c);
+}
+
+int dmalloc(void** p, size_t bytes) {
+  if (cudaMalloc(p, bytes) != cudaSuccess) {
+    *p = nullptr;
+    return CHNS_ERR_NOMEM;
+  }
+  return cudaMemsetAsync(*p, 0, bytes) == cudaSuccess ? CHNS_OK : CHNS_ERR_CUDA;
+}
+
+// Copies `bytes` from a host or device pointer to device memory.
+int to_device(chns_ctx* c, void* dst, const void* src, size_t bytes, int where) {
+  CK(cudaMemcpyAsync(dst, src, bytes, where == CHNS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     c->stream));
+  return CHNS_OK;
+}
+int from_device(chns_ctx* c, void* dst, const void* src, size_t bytes, int where) {
+  CK(cudaMemcpyAsync(dst, src, bytes, where == CHNS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     c->stream));
+  if (where != CHNS_DEVICE) CK(cudaStreamSynchronize(c->stream));
+  return CHNS_OK;
+}
+
+__global__ void k_real_d2r_f32(const double* __restrict__ a, float* __restrict__ b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+__global__ void k_real_r2d_f32(const float* __restrict__ a, double* __restrict__ b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (double)a[i];
+}
+// FP32 contexts keep the k = 0 modes in double: copy (0,0) of FFTW staging <-> k0
+__global__ void k_k0_set(double* k0, const double* st, int slot) {
+  k0[2 * slot] = st[0];
+  k0[2 * slot + 1] = st[1];
+}
+__global__ void k_k0_get(const double* k0, double* st, int slot) {
+  st[0] = k0[2 * slot];
+  st[1] = k0[2 * slot + 1];
+}
+
+int enqueue_step(chns_ctx* c) {
+  int n1 = c->L->stage(c, 1);
+  int n2 = c->L->stage(c, 2);
+  c->launches_per_step = n1 + n2;
+  return CHNS_OK;
+}
+
+int build_graph(chns_ctx* c) {
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return CHNS_ERR_CUDA;
+  enqueue_step(c);
+  if (cudaStreamEndCapture(c->stream, &g) != cudaSuccess) return CHNS_ERR_CUDA;
+  cudaError_t e = cudaGraphInstantiate(&c->step_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    c->step_graph = nullptr;
+    return CHNS_ERR_CUDA;
+  }
+  c->graph_ok = true;
+  return CHNS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void chns_default_params(chns_params* p, int model, int n) {
+  memset(p, 0, sizeof(*p));
+  p->model = model;
+  p->precision = CHNS_FP64;
+  p->nx = p->ny = n;
+  p->lx = p->ly = 4.0 * M_PI;  // global.h:20-21
+  p->dt = 1e-4;                 // global.h:31
+  p->nu = 0.01;                 // global.h:30
+  const double dx = p->lx / n;
+  p->epsilon = 3.0 * dx;  // global.h:103,131
+  if (model == CHNS_MODEL_BINARY) {
+    p->sigma = 2.0;    // global.h:102
+    p->lambda = 1e-6;  // global.h:104
+  } else if (model == CHNS_MODEL_TERNARY) {
+    p->sigma12 = 0.2;   // global.h:127-129
+    p->sigma23 = 0.45;
+    p->sigma13 = 0.2;
+    p->lambda = 1e-4;   // global.h:132
+    p->xlambda = 2.0;   // global.h:133
+  }
+  p->dealias_div = 4.0;
+  p->coef_mode = CHNS_COEF_REFERENCE;
+}
+
+int chns_create(const chns_params* pin, chns_ctx** out) {
+  if (!out) return CHNS_ERR_ARG;
+  *out = nullptr;
+  int rc = validate(pin);
+  if (rc != CHNS_OK) return rc;
+  chns_ctx* c = (chns_ctx*)calloc(1, sizeof(chns_ctx));
+  if (!c) return CHNS_ERR_NOMEM;
+  c->p = *pin;
+  const chns_params& p = c->p;
+  c->n = p.nx;
+  c->nr = p.nx / 2 + 1;
+  c->f32 = p.precision == CHNS_FP32;
+  c->rsz = c->f32 ? 4 : 8;
+  const int logn = ilog2_exact(c->n);
+  c->L = c->f32 ? chns::launchers_f32(logn) : chns::launchers_f64(logn);
+  if (!c->L) {
+    free(c);
+    return CHNS_ERR_UNSUPPORTED;
+  }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    free(c);
+    return CHNS_ERR_CUDA;
+  }
+  c->own_stream = true;
+
+  // wavenumbers (main.c:54-55, functions.c:11-33) and the truncation table (functions.c:47-84)
+  const int n = c->n, nr = c->nr;
+  c->fx = (2 * M_PI) / p.lx;
+  c->fy = (2 * M_PI) / p.ly;
+  const double dax = (p.nx / p.dealias_div) * c->fx;
+  const double dealias = dax * dax;
+  std::vector<int> mrow(nr, -1);
+  c->jt = -1;
+  for (int j = 0; j < nr; j++) {
+    const double ky = c->fy * j;
+    int lim = -1;
+    for (int m = 0; m <= n / 2; m++) {
+      const double kx = c->fx * m;
+      const double ks = kx * kx + ky * ky;
+      if (ks > dealias) break;
+      lim = m;
+    }
+    mrow[j] = lim;
+    if (lim >= 0) c->jt = j;
+  }
+  if (c->jt < 0 || c->jt >= n / 2) {
+    free_all(c);
+    return CHNS_ERR_UNSUPPORTED;
+  }
+  // ternary surface-tension coefficients (main.c:166-170)
+  if (p.model == CHNS_MODEL_TERNARY) {
+    c->gamma[0] = (p.sigma12 - p.sigma23 + p.sigma13);
+    c->gamma[1] = (p.sigma12 - p.sigma13 + p.sigma23);
+    c->gamma[2] = (p.sigma23 - p.sigma12 + p.sigma13);
+    c->del = (6.0 * c->gamma[0] * c->gamma[1] * c->gamma[2]);
+    c->del /= (c->gamma[0] * c->gamma[1] + c->gamma[0] * c->gamma[2] + c->gamma[1] * c->gamma[2]);
+    if (!(c->gamma[0] != 0 && c->gamma[1] != 0 && c->gamma[2] != 0)) {
+      free_all(c);
+      return CHNS_ERR_ARG;
+    }
+  }
+  // Kolmogorov forcing: curl of F0 sin(kf y) x-hat = -F0 kf cos(kf y); its
+  // unnormalised transform is -F0 kf (nx ny / 2) at kx = 0, ky = kf
+  c->force_j = -1;
+  if (p.force_amp != 0.0) {
+    c->force_j = (int)nearbyint(p.force_k * p.ly / (2.0 * M_PI));
+    c->force_hat = -p.force_amp * p.force_k * ((double)p.nx * (double)p.ny / 2.0);
+  }
+
+  // ETD coefficient tables [6][nr rows][nr |m|]
+  const size_t tsz = (size_t)nr * nr;
+  std::vector<double> coef(6 * tsz);
+  for (int j = 0; j < nr; j++) {
+    const double ky = c->fy * j;
+    for (int m = 0; m < nr; m++) {
+      const double kx = c->fx * m;
+      const double ks = kx * kx + ky * ky;
+      double o[6];
+      etd_coefs(p, ks, o);
+      for (int q = 0; q < 6; q++) coef[q * tsz + (size_t)j * nr + m] = o[q];
+    }
+  }
+  for (int q = 0; q < 6; q++) c->k0coef[q] = coef[q * tsz];
+
+  // twiddles exp(-2 pi i q / n), long double then rounded
+  std::vector<double> twd(2 * (size_t)n);
+  for (int q = 0; q < n; q++) {
+    const long double a = 6.283185307179586476925286766559005768L * (long double)q / (long double)n;
+    twd[2 * q] = (double)cosl(a);
+    twd[2 * q + 1] = (double)-sinl(a);
+  }
+
+  const size_t ncx = (size_t)nr * n;           // complex per S/H field
+  const size_t ngx = (size_t)(c->jt + 1) * n;  // complex per G field
+  const size_t cxsz = 2 * c->rsz;
+  const int nfields = p.model + 1;
+  rc = CHNS_OK;
+  for (int f = 0; f < 3 && rc == CHNS_OK; f++) {
+    if (f < nfields) {
+      rc = dmalloc(&c->state[f], ncx * cxsz);
+      if (rc == CHNS_OK) rc = dmalloc(&c->saved[f], ncx * cxsz);
+    }
+  }
+  if (rc == CHNS_OK) rc = dmalloc(&c->nw, ncx * cxsz);
+  for (int k = 0; k < 12 && rc == CHNS_OK; k++) rc = dmalloc(&c->g[k], ngx * cxsz);
+  for (int k = 0; k < 7 && rc == CHNS_OK; k++) rc = dmalloc(&c->h[k], ncx * cxsz);
+  if (rc == CHNS_OK) rc = dmalloc(&c->coef, 6 * tsz * c->rsz);
+  if (rc == CHNS_OK) rc = dmalloc((void**)&c->mrow, nr * sizeof(int));
+  if (rc == CHNS_OK) rc = dmalloc(&c->tw, (size_t)n * cxsz);
+  if (rc == CHNS_OK) rc = dmalloc((void**)&c->k0, 16 * sizeof(double));
+  if (rc == CHNS_OK) rc = dmalloc((void**)&c->stage, 2 * ncx * sizeof(double));
+  if (rc == CHNS_OK) rc = dmalloc(&c->realbuf, (size_t)n * n * c->rsz);
+  if (rc == CHNS_OK) rc = dmalloc((void**)&c->realdbl, (size_t)n * n * sizeof(double));
+  if (rc == CHNS_OK) rc = dmalloc((void**)&c->red, 16 * sizeof(double));
+  if (rc == CHNS_OK) rc = dmalloc(&c->redscratch, (size_t)(n / 2 + 1) * 8 * sizeof(double));
+  if (rc != CHNS_OK) {
+    free_all(c);
+    return rc;
+  }
+  // uploads (tables converted to the context precision)
+  cudaError_t e = cudaSuccess;
+  if (c->f32) {
+    std::vector<float> cf(coef.begin(), coef.end());
+    std::vector<float> tf(twd.begin(), twd.end());
+    e = cudaMemcpy(c->coef, cf.data(), cf.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->tw, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice);
+  } else {
+    e = cudaMemcpy(c->coef, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->tw, twd.data(), twd.size() * 8, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(c->mrow, mrow.data(), nr * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    free_all(c);
+    return CHNS_ERR_CUDA;
+  }
+  *out = c;
+  return CHNS_OK;
+}
+
+int chns_destroy(chns_ctx* c) {
+  if (!c) return CHNS_ERR_ARG;
+  cudaStreamSynchronize(c->stream);
+  free_all(c);
+  return CHNS_OK;
+}
+
+int chns_set_stream(chns_ctx* c, void* stream) {
+  if (!c) return CHNS_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  c->stream = (cudaStream_t)stream;
+  c->own_stream = false;
+  if (c->step_graph) {
+    cudaGraphExecDestroy(c->step_graph);
+    c->step_graph = nullptr;
+    c->graph_ok = false;
+  }
+  return CHNS_OK;
+}
+
+int chns_synchronize(chns_ctx* c) {
+  if (!c) return CHNS_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  return CHNS_OK;
+}
+
+static int set_field(chns_ctx* c, int f, const double* src, int where) {
+  const size_t bytes = 2 * (size_t)c->n * c->nr * sizeof(double);
+  int rc = to_device(c, c->stage, src, bytes, where);
+  if (rc) return rc;
+  c->L->from_fftw(c, c->stage, c->state[f]);
+  if (c->f32) k_k0_set<<<1, 1, 0, c->stream>>>(c->k0, c->stage, f);
+  CK(cudaGetLastError());
+  return CHNS_OK;
+}
+
+static int get_field(chns_ctx* c, int f, const void* s, double* dst, int where, int k0slot) {
+  const size_t bytes = 2 * (size_t)c->n * c->nr * sizeof(double);
+  c->L->to_fftw(c, s, c->stage);
+  if (c->f32 && k0slot >= 0) k_k0_get<<<1, 1, 0, c->stream>>>(c->k0, c->stage, k0slot);
+  CK(cudaGetLastError());
+  return from_device(c, dst, c->stage, bytes, where);
+}
+
+int chns_set_state(chns_ctx* c, const double* w, const double* c1, const double* c2, int where) {
+  if (!c) return CHNS_ERR_ARG;
+  const double* src[3] = {w, c1, c2};
+  for (int f = 0; f <= c->p.model; f++) {
+    if (!src[f]) continue;
+    int rc = set_field(c, f, src[f], where);
+    if (rc) return rc;
+  }
+  return chns_synchronize(c);
+}
+
+int chns_get_state(chns_ctx* c, double* w, double* c1, double* c2, int where) {
+  if (!c) return CHNS_ERR_ARG;
+  double* dst[3] = {w, c1, c2};
+  for (int f = 0; f <= c->p.model; f++) {
+    if (!dst[f]) continue;
+    int rc = get_field(c, f, c->state[f], dst[f], where, f);
+    if (rc) return rc;
+  }
+  return CHNS_OK;
+}
+
+static int upload_real(chns_ctx* c, const double* real, int where) {
+  const size_t nn = (size_t)c->n * c->n;
+  int rc = to_device(c, c->realdbl, real, nn * sizeof(double), where);
+  if (rc) return rc;
+  if (c->f32) {
+    k_real_d2r_f32<<<1024, 256, 0, c->stream>>>(c->realdbl, (float*)c->realbuf, nn);
+  } else {
+    CK(cudaMemcpyAsync(c->realbuf, c->realdbl, nn * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  return CHNS_OK;
+}
+
+int chns_set_phase_real(chns_ctx* c, const double* p1, const double* p2, int where) {
+  if (!c || c->p.model == CHNS_MODEL_NS) return CHNS_ERR_ARG;
+  if (!p1 || (c->p.model == CHNS_MODEL_TERNARY && !p2)) return CHNS_ERR_ARG;
+  const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
+  CK(cudaMemsetAsync(c->state[0], 0, bytes, c->stream));  // init.c:78-87
+  if (c->f32) CK(cudaMemsetAsync(c->k0, 0, 2 * sizeof(double), c->stream));
+  const double* src[2] = {p1, p2};
+  for (int f = 0; f < c->p.model; f++) {
+    int rc = upload_real(c, src[f], where);
+    if (rc) return rc;
+    c->L->dfft(c, c->realbuf, c->state[1 + f]);
+    c->L->truncate(c, c->state[1 + f]);
+    if (c->f32) {
+      // the k = 0 mode in double comes from the same FP32 transform
+      c->L->to_fftw(c, c->state[1 + f], c->stage);
+      k_k0_set<<<1, 1, 0, c->stream>>>(c->k0, c->stage, 1 + f);
+    }
+  }
+  CK(cudaGetLastError());
+  return chns_synchronize(c);
+}
+
+int chns_step(chns_ctx* c, int nsteps) {
+  if (!c || nsteps < 0) return CHNS_ERR_ARG;
+  if (nsteps == 0) return CHNS_OK;
+  if (!c->graph_ok) {
+    if (build_graph(c) != CHNS_OK) {
+      cudaGetLastError();
+      c->graph_ok = false;
+    }
+  }
+  for (int s = 0; s < nsteps; s++) {
+    if (c->graph_ok) {
+      CK(cudaGraphLaunch(c->step_graph, c->stream));
+    } else {
+      enqueue_step(c);
+    }
+  }
+  CK(cudaGetLastError());
+  return CHNS_OK;
+}
+
+int chns_rhs(chns_ctx* c, double* nw, double* nc1, double* nc2, int where) {
+  if (!c) return CHNS_ERR_ARG;
+  // stage 1 stores N(u) of the current state in the `saved` buffers; run it on
+  // a copy of the state and restore the state afterwards
+  const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
+  void* keep[3] = {nullptr, nullptr, nullptr};
+  double k0keep[12];
+  int rc = CHNS_OK;
+  for (int f = 0; f <= c->p.model && rc == CHNS_OK; f++) {
+    if (cudaMalloc(&keep[f], bytes) != cudaSuccess) rc = CHNS_ERR_NOMEM;
+    else if (cudaMemcpyAsync(keep[f], c->state[f], bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+      rc = CHNS_ERR_CUDA;
+  }
+  if (rc == CHNS_OK && c->f32 && cudaMemcpy(k0keep, c->k0, sizeof(k0keep), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = CHNS_ERR_CUDA;
+  if (rc == CHNS_OK) c->L->stage(c, 1);
+  double* dst[3] = {nw, nc1, nc2};
+  for (int f = 0; f <= c->p.model && rc == CHNS_OK; f++)
+    if (dst[f]) rc = get_field(c, f, c->saved[f], dst[f], where, 3 + f);
+  for (int f = 0; f <= c->p.model; f++) {
+    if (keep[f]) {
+      cudaMemcpyAsync(c->state[f], keep[f], bytes, cudaMemcpyDeviceToDevice, c->stream);
+      cudaStreamSynchronize(c->stream);
+      cudaFree(keep[f]);
+    }
+  }
+  if (c->f32) cudaMemcpy(c->k0, k0keep, sizeof(k0keep), cudaMemcpyHostToDevice);
+  if (rc == CHNS_OK) rc = chns_synchronize(c);
+  return rc;
+}
+
+int chns_dfft(chns_ctx* c, const double* real, double* spec, int where) {
+  if (!c || !real || !spec) return CHNS_ERR_ARG;
+  int rc = upload_real(c, real, where);
+  if (rc) return rc;
+  c->L->dfft(c, c->realbuf, c->nw);
+  return get_field(c, 0, c->nw, spec, where, -1);
+}
+
+int chns_ifft(chns_ctx* c, const double* spec, double* real, int where) {
+  if (!c || !real || !spec) return CHNS_ERR_ARG;
+  const size_t nn = (size_t)c->n * c->n;
+  int rc = to_device(c, c->stage, spec, 2 * (size_t)c->n * c->nr * sizeof(double), where);
+  if (rc) return rc;
+  c->L->from_fftw(c, c->stage, c->nw);
+  c->L->ifft(c, c->nw, c->realbuf);
+  if (c->f32) {
+    k_real_r2d_f32<<<1024, 256, 0, c->stream>>>((const float*)c->realbuf, c->realdbl, nn);
+  } else {
+    CK(cudaMemcpyAsync(c->realdbl, c->realbuf, nn * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  CK(cudaGetLastError());
+  return from_device(c, real, c->realdbl, nn * sizeof(double), where);
+}
+
+int chns_diagnostics(chns_ctx* c, double* out_fe, double* out_ke) {
+  if (!c) return CHNS_ERR_ARG;
+  c->L->diag(c);
+  CK(cudaGetLastError());
+  double r[8];
+  CK(cudaMemcpyAsync(r, c->red, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const chns_params& p = c->p;
+  const double scale = 1.0 / ((double)p.nx * (double)p.ny);
+  double fe[2] = {0.0, 0.0};
+  if (p.model == CHNS_MODEL_BINARY) {
+    fe[0] = r[0] * (12.0 * (p.sigma / p.epsilon)) * scale;  // free_energy.c:39-42
+    fe[1] = r[1] * ((0.75 * p.sigma * p.epsilon) * scale);  // free_energy.c:96
+  } else if (p.model == CHNS_MODEL_TERNARY) {
+    fe[0] = r[0] * (6.0 / p.epsilon) * scale;  // free_energy.c:48-54
+    fe[1] = r[1] * (0.375 * p.epsilon * scale);  // free_energy.c:141
+  }
+  double ke[3];
+  ke[0] = r[2] * scale;                   // kinetic_energy.c:94
+  ke[1] = r[5] > 0 ? r[3] / r[5] : 0.0;   // kinetic_energy.c:103-106
+  ke[2] = r[6] > 0 ? r[4] / r[6] : 0.0;   // kinetic_energy.c:123-131
+  if (out_fe) memcpy(out_fe, fe, sizeof(fe));
+  if (out_ke) memcpy(out_ke, ke, sizeof(ke));
+  for (int k = 0; k < 7; k++)
+    if (!isfinite(r[k])) return CHNS_ERR_NONFINITE;
+  if (fe[0] >= 100.0) return CHNS_ERR_NONFINITE;  // the reference's blow-up guard (free_energy.c:151-154)
+  return CHNS_OK;
+}
+
+int chns_launches_per_step(const chns_ctx* c) { return c ? c->launches_per_step : 0; }
+
+int chns_profile_step(chns_ctx* c, int reps, float* ms, int* kind, int maxk) {
+  if (!c || reps < 1 || !ms || !kind || maxk < 1) return CHNS_ERR_ARG;
+  const int cap = 64;
+  cudaEvent_t ev[cap + 1];
+  int kinds[cap];
+  for (int k = 0; k <= cap; k++)
+    if (cudaEventCreate(&ev[k]) != cudaSuccess) return CHNS_ERR_CUDA;
+  for (int k = 0; k < maxk; k++) ms[k] = 0.0f;
+  int nk = 0;
+  int rc = CHNS_OK;
+  for (int r = 0; r < reps && rc == CHNS_OK; r++) {
+    c->prof_ev = ev + 1;
+    c->prof_kind = kinds;
+    c->prof_n = 0;
+    c->prof_max = cap;
+    cudaEventRecord(ev[0], c->stream);
+    enqueue_step(c);
+    nk = c->prof_n;
+    c->prof_ev = nullptr;
+    if (cudaEventSynchronize(ev[nk]) != cudaSuccess) rc = CHNS_ERR_CUDA;
+    for (int k = 0; k < nk && k < maxk && rc == CHNS_OK; k++) {
+      float t = 0.0f;
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      ms[k] += t / reps;
+      kind[k] = kinds[k];
+    }
+  }
+  c->prof_ev = nullptr;
+  for (int k = 0; k <= cap; k++) cudaEventDestroy(ev[k]);
+  if (rc != CHNS_OK) return rc;
+  return nk < maxk ? nk : maxk;
+}
+
+const char* chns_status_string(int s) {
+  switch (s) {
+    case CHNS_OK: return "ok";
+    case CHNS_ERR_ARG: return "bad argument";
+    case CHNS_ERR_CUDA: return "CUDA error";
+    case CHNS_ERR_NONFINITE: return "non-finite or blown-up state";
+    case CHNS_ERR_TIMEOUT: return "device wait timed out";
+    case CHNS_ERR_UNSUPPORTED: return "unsupported size or option";
+    case CHNS_ERR_NOMEM: return "out of memory";
+  }
+  return "unknown status";
+}
+
+}  // extern "C"

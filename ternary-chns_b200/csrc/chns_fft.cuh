@@ -37,14 +37,14 @@ template <class R> __device__ __forceinline__ cx<R> cmulc(cx<R> a, cx<R> b) {
 
 // Rounded arithmetic without contraction: used wherever the reference's
 // expression order must be kept (the FFT butterflies are free to use FMA).
-__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
-__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
+static __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+static __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+static __device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+static __device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
+static __device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+static __device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+static __device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+static __device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
 
 // multiply by DIR*i: forward transforms use DIR = -1 (kernel exp(-2 pi i jk/N))
 template <int DIR, class R> __device__ __forceinline__ cx<R> mul_i(cx<R> a) {
@@ -146,7 +146,7 @@ template <int DIR, int RADIX, int STRIDE, class R> __device__ __forceinline__ vo
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 
 // shared-memory slot of element q of one group's buffer (one pad per 16)
-__device__ __forceinline__ int spad(int q) { return q + (q >> 4); }
+static __device__ __forceinline__ int spad(int q) { return q + (q >> 4); }
 
 template <int N> struct FftShape {
   static constexpr int NT = N / 16;                   // threads per transform

@@ -1,0 +1,3 @@
+// Launchers of the ETD2RK passes for a 4096^2 grid (FP64 and FP32).
+#include "chns_launch.cuh"
+CHNS_INSTANTIATE(4096)

@@ -1,0 +1,86 @@
+// chns_internal.h -- context of the C ABI and the per-size launch tables.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/chns.h"
+
+struct chns_ctx;
+
+namespace chns {
+
+// Launchers instantiated per grid size and precision (chns_inst_*.cu).
+struct Launchers {
+  // one ETD2RK stage (1 or 2) of the context's model; returns launches enqueued
+  int (*stage)(chns_ctx* c, int stage);
+  // S-layout field -> truncated in place
+  int (*truncate)(chns_ctx* c, void* s);
+  // device real (R, nx*ny) -> S-layout spectrum (unnormalised r2c)
+  int (*dfft)(chns_ctx* c, const void* real, void* s);
+  // S-layout spectrum -> device real (R), c2r * 1/(nx ny)
+  int (*ifft)(chns_ctx* c, const void* s, void* real);
+  // FFTW-layout double <-> S layout
+  int (*from_fftw)(chns_ctx* c, const double* src, void* s);
+  int (*to_fftw)(chns_ctx* c, const void* s, double* dst);
+  // free energy and kinetic energy reductions (double results in c->red)
+  int (*diag)(chns_ctx* c);
+};
+
+const Launchers* launchers_f64(int logn);
+const Launchers* launchers_f32(int logn);
+
+}  // namespace chns
+
+struct chns_ctx {
+  chns_params p;
+  int n, nr, jt;
+  bool f32;
+  size_t rsz;  // bytes per real scalar (4 or 8)
+  cudaStream_t stream;
+  bool own_stream;
+  // device memory
+  void* state[3];
+  void* saved[3];
+  void* nw;
+  void* g[12];
+  void* h[7];
+  void* coef;
+  int* mrow;
+  void* tw;
+  double* k0;       // [12] k = 0 modes (FP32 contexts)
+  double* stage;    // FFTW-layout double staging, n * nr complex
+  void* realbuf;    // n * n reals of the context precision
+  double* realdbl;  // n * n doubles
+  double* red;      // reduction results
+  void* redscratch;
+  // host-side parameters
+  double k0coef[6];
+  double fx, fy;
+  double gamma[3], del;
+  int force_j;
+  double force_hat;
+  // launch bookkeeping
+  const chns::Launchers* L;
+  int launches_per_step;
+  cudaGraphExec_t step_graph;
+  bool graph_ok;
+  void* hostpin;    // pinned staging for host transfers
+  size_t hostpin_bytes;
+  // tracing: when prof_ev is set, every launch of a stage records an event
+  cudaEvent_t* prof_ev;
+  int* prof_kind;
+  int prof_n, prof_max;
+};
+
+namespace chns {
+// kernel kinds reported by chns_profile_step
+enum { KIND_SPEC_INV = 0, KIND_ROW_ADV = 1, KIND_SPEC_FWD_C = 2, KIND_ROW_FORCE = 3, KIND_SPEC_CURL_W = 4,
+       KIND_ROW_ADV_B = 5 };
+inline void mark(chns_ctx* c, int kind) {
+  if (c->prof_ev && c->prof_n < c->prof_max) {
+    cudaEventRecord(c->prof_ev[c->prof_n], c->stream);
+    c->prof_kind[c->prof_n] = kind;
+    c->prof_n++;
+  }
+}
+}  // namespace chns

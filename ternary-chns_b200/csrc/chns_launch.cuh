@@ -1,0 +1,339 @@
+// chns_launch.cuh -- host launchers for one grid size and precision.
+// Included by chns_inst_<N>.cu, which instantiates Launchers for N.
+#pragma once
+
+#include "chns_internal.h"
+#include "chns_kernels.cuh"
+#include "chns_diag.cuh"
+
+namespace chns {
+
+// groups (transforms) per CTA: 256 threads for N >= 256, fewer for tiny grids
+template <int N> constexpr int gpc_of() {
+  constexpr int nt = N / 16;
+  constexpr int a = 256 / nt;
+  constexpr int b = N / 16;
+  return a < b ? (a < 1 ? 1 : a) : (b < 1 ? 1 : b);
+}
+
+template <class R> Par<R> make_par(const chns_ctx* c) {
+  Par<R> P;
+  const chns_params& p = c->p;
+  P.n = c->n;
+  P.jt = c->jt;
+  P.fx = c->fx;
+  P.fy = c->fy;
+  P.scale = (R)(1.0 / (double)(p.nx * p.ny));
+  P.st15 = (R)(1.5 * p.sigma * p.epsilon);
+  P.st24 = (R)(24.0 * (p.sigma / p.epsilon));
+  P.lam = (R)p.lambda;
+  const double g1 = c->gamma[0], g2 = c->gamma[1], g3 = c->gamma[2];
+  if (p.model == CHNS_MODEL_TERNARY) {
+    P.mu1 = (R)(0.75 * g1 * p.epsilon);
+    P.mu2 = (R)(0.75 * g2 * p.epsilon);
+    P.lg1 = (R)(p.lambda / g1);
+    P.lg2 = (R)(p.lambda / g2);
+    P.w11 = (R)(1.0 + (g3 / g1));
+    P.w12 = (R)(g3 / g2);
+    P.w21 = (R)(g3 / g1);
+    P.w22 = (R)(1.0 + (g3 / g2));
+    P.g1 = (R)g1;
+    P.g2 = (R)g2;
+    P.g3 = (R)g3;
+    P.g1i = (R)(1.0 / g1);
+    P.g2i = (R)(1.0 / g2);
+    P.g3i = (R)(1.0 / g3);
+    P.six_lam = (R)(6.0 * p.xlambda);
+    P.fac_mu = (R)(2.0 * c->del / p.epsilon);
+  } else {
+    P.mu1 = P.mu2 = P.lg1 = P.lg2 = P.w11 = P.w12 = P.w21 = P.w22 = (R)0;
+    P.g1 = P.g2 = P.g3 = P.g1i = P.g2i = P.g3i = P.six_lam = P.fac_mu = (R)0;
+  }
+  P.force_j = c->force_j;
+  P.force_hat = (R)c->force_hat;
+  for (int k = 0; k < 6; k++) P.k0coef[k] = c->k0coef[k];
+  P.mrow = c->mrow;
+  P.coef = (const R*)c->coef;
+  P.tw = (const cx<R>*)c->tw;
+  P.k0 = c->k0;
+  return P;
+}
+
+template <class R> Bufs<R> make_bufs(const chns_ctx* c) {
+  Bufs<R> B;
+  B.w = (cx<R>*)c->state[0];
+  B.c1 = (cx<R>*)c->state[1];
+  B.c2 = (cx<R>*)c->state[2];
+  B.sw = (cx<R>*)c->saved[0];
+  B.s1 = (cx<R>*)c->saved[1];
+  B.s2 = (cx<R>*)c->saved[2];
+  B.nw = (cx<R>*)c->nw;
+  for (int k = 0; k < NG; k++) B.g[k] = (cx<R>*)c->g[k];
+  for (int k = 0; k < NH; k++) B.h[k] = (cx<R>*)c->h[k];
+  return B;
+}
+
+template <class K> static void set_smem(K kern, size_t bytes) {
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int N, class R> struct Sizes {
+  static constexpr int GPC = gpc_of<N>();
+  static constexpr int NT = N / 16;
+  static constexpr int THREADS = GPC * NT;
+  static constexpr size_t FFT_SMEM = (size_t)GPC * FftShape<N>::SMEM * sizeof(cx<R>);
+  static constexpr size_t FRAG = (size_t)GPC * N * sizeof(cx<R>);
+  static int grid_rows(int rows) { return (rows + GPC - 1) / GPC; }
+};
+
+template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
+  using S = Sizes<N, R>;
+  constexpr int GPC = S::GPC;
+  const Par<R> P = make_par<R>(c);
+  const Bufs<R> B = make_bufs<R>(c);
+  cudaStream_t st = c->stream;
+  const int model = c->p.model;
+  const int rows_inv = S::grid_rows(c->jt + 1);
+  const int rows_all = S::grid_rows(N / 2 + 1);
+  const int pairs = S::grid_rows(N / 2);
+  int launches = 0;
+
+  // P1
+  if (model == CHNS_MODEL_NS) {
+    auto k = k_spec_inv<N, R, GPC, MODEL_NS>;
+    set_smem(k, S::FFT_SMEM);
+    k<<<rows_inv, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+  } else if (model == CHNS_MODEL_BINARY) {
+    auto k = k_spec_inv<N, R, GPC, MODEL_BINARY>;
+    set_smem(k, S::FFT_SMEM);
+    k<<<rows_inv, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+  } else {
+    auto k = k_spec_inv<N, R, GPC, MODEL_TERNARY>;
+    set_smem(k, S::FFT_SMEM);
+    k<<<rows_inv, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+  }
+  launches++;
+  mark(c, KIND_SPEC_INV);
+
+  // P2
+  if (model == CHNS_MODEL_NS) {
+    AdvIO<R> io{};
+    io.dx[0] = B.g[GDXW];
+    io.dy[0] = B.g[GDYW];
+    io.out[0] = B.h[HA];
+    auto k = k_row_adv<N, R, GPC, 1, 0>;
+    const size_t sm = S::FFT_SMEM + 1 * S::FRAG;
+    set_smem(k, sm);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P, io);
+    launches++;
+    mark(c, KIND_ROW_ADV);
+  } else if (model == CHNS_MODEL_BINARY) {
+    AdvIO<R> io{};
+    io.dx[0] = B.g[GDXW];
+    io.dy[0] = B.g[GDYW];
+    io.out[0] = B.h[HA];
+    io.dx[1] = B.g[GDX1];
+    io.dy[1] = B.g[GDY1];
+    io.out[1] = B.h[HB1];
+    auto k = k_row_adv<N, R, GPC, 2, 1>;
+    const size_t sm = S::FFT_SMEM + 2 * S::FRAG;
+    set_smem(k, sm);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P, io);
+    launches++;
+    mark(c, KIND_ROW_ADV);
+  } else {
+    AdvIO<R> io{};
+    io.dx[0] = B.g[GDXW];
+    io.dy[0] = B.g[GDYW];
+    io.out[0] = B.h[HA];
+    auto k = k_row_adv<N, R, GPC, 1, 2>;
+    const size_t sm = S::FFT_SMEM + 1 * S::FRAG;
+    set_smem(k, sm);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P, io);
+    mark(c, KIND_ROW_ADV);
+    AdvIO<R> io2{};
+    io2.dx[0] = B.g[GDX1];
+    io2.dy[0] = B.g[GDY1];
+    io2.out[0] = B.h[HB1];
+    io2.dx[1] = B.g[GDX2];
+    io2.dy[1] = B.g[GDY2];
+    io2.out[1] = B.h[HB2];
+    auto k2 = k_row_adv<N, R, GPC, 2, 0>;
+    const size_t sm2 = S::FFT_SMEM + 2 * S::FRAG;
+    set_smem(k2, sm2);
+    k2<<<pairs, S::THREADS, sm2, st>>>(B, P, io2);
+    mark(c, KIND_ROW_ADV_B);
+    launches += 2;
+  }
+
+  if (model == CHNS_MODEL_NS) {
+    // P3 of pure Navier-Stokes: N_w = -F[u.grad w], ETD of w
+    if (stage == 1) {
+      auto k = k_spec_curl_w<N, R, GPC, false, 1>;
+      set_smem(k, S::FFT_SMEM);
+      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    } else {
+      auto k = k_spec_curl_w<N, R, GPC, false, 2>;
+      set_smem(k, S::FFT_SMEM);
+      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    }
+    mark(c, KIND_SPEC_CURL_W);
+    return launches + 1;
+  }
+
+  // P3
+  if (model == CHNS_MODEL_BINARY) {
+    if (stage == 1) {
+      auto k = k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1>;
+      set_smem(k, S::FFT_SMEM);
+      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    } else {
+      auto k = k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 2>;
+      set_smem(k, S::FFT_SMEM);
+      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    }
+  } else {
+    if (stage == 1) {
+      auto k = k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 1>;
+      set_smem(k, S::FFT_SMEM);
+      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    } else {
+      auto k = k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 2>;
+      set_smem(k, S::FFT_SMEM);
+      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    }
+  }
+  launches++;
+  mark(c, KIND_SPEC_FWD_C);
+
+  // P4
+  if (model == CHNS_MODEL_BINARY) {
+    auto k = k_row_force<N, R, GPC, MODEL_BINARY>;
+    set_smem(k, S::FFT_SMEM);
+    k<<<pairs, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+  } else {
+    auto k = k_row_force<N, R, GPC, MODEL_TERNARY>;
+    const size_t sm = S::FFT_SMEM + 2 * S::FRAG;
+    set_smem(k, sm);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P);
+  }
+  launches++;
+  mark(c, KIND_ROW_FORCE);
+
+  // P5
+  if (stage == 1) {
+    auto k = k_spec_curl_w<N, R, GPC, true, 1>;
+    set_smem(k, S::FFT_SMEM);
+    k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+  } else {
+    auto k = k_spec_curl_w<N, R, GPC, true, 2>;
+    set_smem(k, S::FFT_SMEM);
+    k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+  }
+  launches++;
+  mark(c, KIND_SPEC_CURL_W);
+  return launches;
+}
+
+template <class R> __global__ void k_truncate(cx<R>* s, const int* __restrict__ mrow, int n) {
+  const int row = blockIdx.y;
+  const int lim = mrow[row];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int ms = i <= n / 2 ? i : n - i;
+    if (ms > lim) s[(size_t)row * n + i] = czero<R>();
+  }
+}
+
+template <int N, class R> int truncate_impl(chns_ctx* c, void* s) {
+  dim3 grid((N + 255) / 256, N / 2 + 1);
+  k_truncate<R><<<grid, 256, 0, c->stream>>>((cx<R>*)s, c->mrow, N);
+  return 1;
+}
+
+template <int N, class R> int dfft_impl(chns_ctx* c, const void* real, void* s) {
+  using S = Sizes<N, R>;
+  auto k1 = k_row_r2c_plain<N, R, S::GPC>;
+  set_smem(k1, S::FFT_SMEM);
+  k1<<<S::grid_rows(N / 2), S::THREADS, S::FFT_SMEM, c->stream>>>((const R*)real, (cx<R>*)c->h[HA],
+                                                                   (const cx<R>*)c->tw);
+  auto k2 = k_col_plain<N, R, S::GPC, -1>;
+  set_smem(k2, S::FFT_SMEM);
+  k2<<<S::grid_rows(N / 2 + 1), S::THREADS, S::FFT_SMEM, c->stream>>>(
+      (const cx<R>*)c->h[HA], (cx<R>*)s, N / 2 + 1, (R)1, (const cx<R>*)c->tw);
+  return 2;
+}
+
+template <int N, class R> int ifft_impl(chns_ctx* c, const void* s, void* real) {
+  using S = Sizes<N, R>;
+  auto k1 = k_col_plain<N, R, S::GPC, +1>;
+  set_smem(k1, S::FFT_SMEM);
+  k1<<<S::grid_rows(N / 2 + 1), S::THREADS, S::FFT_SMEM, c->stream>>>(
+      (const cx<R>*)s, (cx<R>*)c->h[HB1], N / 2 + 1, (R)(1.0 / ((double)N * (double)N)), (const cx<R>*)c->tw);
+  auto k2 = k_row_c2r_plain<N, R, S::GPC>;
+  set_smem(k2, S::FFT_SMEM);
+  k2<<<S::grid_rows(N / 2), S::THREADS, S::FFT_SMEM, c->stream>>>((const cx<R>*)c->h[HB1], (R*)real, N / 2,
+                                                                   (const cx<R>*)c->tw);
+  return 2;
+}
+
+template <int N, class R> int from_fftw_impl(chns_ctx* c, const double* src, void* s) {
+  dim3 grid((N / 2 + 1 + 31) / 32, (N + 31) / 32);
+  k_fftw_to_s<R><<<grid, dim3(32, 8), 0, c->stream>>>((const double2*)src, (cx<R>*)s, N);
+  return 1;
+}
+
+template <int N, class R> int to_fftw_impl(chns_ctx* c, const void* s, double* dst) {
+  dim3 grid((N / 2 + 1 + 31) / 32, (N + 31) / 32);
+  k_s_to_fftw<R><<<grid, dim3(32, 8), 0, c->stream>>>((const cx<R>*)s, (double2*)dst, N);
+  return 1;
+}
+
+template <int N, class R> int diag_impl(chns_ctx* c) {
+  using S = Sizes<N, R>;
+  const Par<R> P = make_par<R>(c);
+  const Bufs<R> B = make_bufs<R>(c);
+  const size_t rsm = (size_t)NRED * S::THREADS * sizeof(double);
+  const size_t sm = S::FFT_SMEM > rsm ? S::FFT_SMEM : rsm;
+  const int model = c->p.model;
+  const int rows = S::grid_rows(N / 2 + 1);
+  const int pairs = S::grid_rows(N / 2);
+  double* part = (double*)c->redscratch;
+  if (model == CHNS_MODEL_NS) {
+    auto k1 = k_diag_spec<N, R, S::GPC, MODEL_NS>;
+    set_smem(k1, S::FFT_SMEM);
+    k1<<<rows, S::THREADS, S::FFT_SMEM, c->stream>>>(B, P);
+    auto k2 = k_diag_row<N, R, S::GPC, MODEL_NS>;
+    set_smem(k2, sm);
+    k2<<<pairs, S::THREADS, sm, c->stream>>>(B, P, part);
+  } else if (model == CHNS_MODEL_BINARY) {
+    auto k1 = k_diag_spec<N, R, S::GPC, MODEL_BINARY>;
+    set_smem(k1, S::FFT_SMEM);
+    k1<<<rows, S::THREADS, S::FFT_SMEM, c->stream>>>(B, P);
+    auto k2 = k_diag_row<N, R, S::GPC, MODEL_BINARY>;
+    set_smem(k2, sm);
+    k2<<<pairs, S::THREADS, sm, c->stream>>>(B, P, part);
+  } else {
+    auto k1 = k_diag_spec<N, R, S::GPC, MODEL_TERNARY>;
+    set_smem(k1, S::FFT_SMEM);
+    k1<<<rows, S::THREADS, S::FFT_SMEM, c->stream>>>(B, P);
+    auto k2 = k_diag_row<N, R, S::GPC, MODEL_TERNARY>;
+    set_smem(k2, sm);
+    k2<<<pairs, S::THREADS, sm, c->stream>>>(B, P, part);
+  }
+  k_diag_final<<<1, 256, 0, c->stream>>>(part, pairs, c->red);
+  return 3;
+}
+
+template <int N, class R> const Launchers* make_launchers() {
+  static const Launchers L = {stage_impl<N, R>, truncate_impl<N, R>, dfft_impl<N, R>, ifft_impl<N, R>,
+                              from_fftw_impl<N, R>, to_fftw_impl<N, R>, diag_impl<N, R>};
+  return &L;
+}
+
+}  // namespace chns
+
+#define CHNS_INSTANTIATE(NN)                                                       \
+  namespace chns {                                                                 \
+  const Launchers* launchers_f64_##NN() { return make_launchers<NN, double>(); } \
+  const Launchers* launchers_f32_##NN() { return make_launchers<NN, float>(); }  \
+  }
