@@ -120,25 +120,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def kernel_bytes(n: int, jt: int, rsz: int) -> dict:
-    """Algorithmic bytes per launch of the binary stage kernels:
-    complex fields of the S/H layouts hold (n/2+1) x n values, G fields (jt+1) x n;
-    P1 loads only the modes inside the truncation disc."""
-    cx = 2 * rsz
-    S = (n // 2 + 1) * n * cx
-    G = (jt + 1) * n * cx
-    disc = 0
-    for j in range(jt + 1):
-        pass
-    return {
-        "spec_inv": None,  # filled by caller with the exact disc size
-        "row_adv": 7 * G + 3 * S,
-        "spec_fwd_c": 3 * S + S + G + S + S + S,   # HA,HF,HB + c, -> nw, G_mu, c, saved
-        "row_force": 3 * G + 2 * S,
-        "spec_curl_w": 2 * S + S + S + S + S,      # HFX,HFY,nw,w -> w, saved
-    }
-
-
 def run_gpu(args):
     import numpy as np
     import torch
@@ -198,7 +179,6 @@ def run_gpu(args):
 
     # ---------------- FP64 plain step on the same workload ----------------
     ctx64 = C.Context(workload_params(n, C.FP64, coef_mode=0))
-    ctx64.set_state(*ctx.get_state()) if False else None
     ctx64.set_phase_real(c0)
     s64 = ctx64.get_state()
     s64[0] = w0

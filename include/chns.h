@@ -124,6 +124,7 @@ int chns_profile_step(chns_ctx *ctx, int reps, float *ms, int *kind, int maxk);
 
 const char *chns_status_string(int status);
 
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,9 +57,9 @@ CONFIGS = {
     "ter64": dict(_TER, n=64),
     "bindef64": dict(_BIN_DEF, n=64),
     "terdef64": dict(_TER_DEF, n=64),
-    # binary, 256^2, L = 2 pi, dt = 1e-3
+    # binary spinodal run, 256^2, L = 2 pi, dt = 1e-3 (1000 steps)
     "bin256": dict(_BIN, n=256),
-    # ternary, 512^2.  Its dt = 5e-4 diverges in the
+    # ternary spinodal run, 512^2 (2000 steps).  dt = 5e-4 diverges in the
     # reference (NaN by step 5: the explicit chemical-potential term is unstable);
     # dt = 5e-5 is the largest tested value that runs the 2000 steps
     "ter512": dict(_TER, n=512, dt="(5e-5)"),
@@ -107,17 +107,26 @@ def reference_present() -> bool:
     return all(os.path.isfile(os.path.join(REF, f)) for f in REF_SOURCES + ["global.h"])
 
 
-def lib_path(name: str) -> str:
-    return os.path.join(OUT, name, "libref.so")
+def lib_path(name: str, dropin: bool = False) -> str:
+    return os.path.join(OUT, name + ("_dropin" if dropin else ""), "libref.so")
 
 
-def build(name: str, force: bool = False) -> str:
+def build(name: str, force: bool = False, dropin: bool = False) -> str:
+    """dropin=True links ternary-chns_b200/csrc/etd2rk_dropin.c (the GPU step behind
+    the reference's own etd2rk signature) in place of the reference's etd2rk.c."""
     cfg = CONFIGS[name]
-    bdir = os.path.join(OUT, name)
-    lib = lib_path(name)
+    bdir = os.path.join(OUT, name + ("_dropin" if dropin else ""))
+    lib = lib_path(name, dropin)
+    repo = os.path.dirname(HERE)
+    chns_lib_dir = os.path.join(repo, "ternary-chns_b200", "lib")
+    if dropin and not os.path.isfile(os.path.join(chns_lib_dir, "libchns_b200.so")):
+        raise FileNotFoundError("build libchns_b200.so before the drop-in oracle")
     deps = [os.path.join(HERE, f) for f in ("ref_harness.c", "fft_cpu.c", "fft_cpu.h", "build_ref.py",
                                             "shim/shim.c", "shim/mpi.h", "shim/fftw3-mpi.h")]
     deps += [os.path.join(REF, f) for f in REF_SOURCES + ["global.h"]]
+    if dropin:
+        deps += [os.path.join(repo, "ternary-chns_b200", "csrc", "etd2rk_dropin.c"),
+                 os.path.join(repo, "include", "chns.h"), os.path.join(chns_lib_dir, "libchns_b200.so")]
     if not force and os.path.isfile(lib):
         t = os.path.getmtime(lib)
         if all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d)):
@@ -134,9 +143,16 @@ def build(name: str, force: bool = False) -> str:
     # free_energy.c only compiles with a phase field (it prints to `fe`, which
     # global.h declares under BINARY/TERNARY only)
     sources = [s for s in REF_SOURCES if cfg["model"] != 0 or s != "free_energy.c"]
+    if dropin:
+        sources = [s for s in sources if s != "etd2rk.c"]
     for s in sources:
         o = os.path.join(bdir, s.replace(".c", ".o"))
         _run([cc, *flags, *inc, "-c", os.path.join(REF, s), "-o", o])
+        objs.append(o)
+    if dropin:
+        o = os.path.join(bdir, "etd2rk_dropin.o")
+        _run([cc, *flags, *inc, "-I", os.path.join(repo, "include"), "-c",
+              os.path.join(repo, "ternary-chns_b200", "csrc", "etd2rk_dropin.c"), "-o", o])
         objs.append(o)
     for s in ("ref_harness.c",):
         o = os.path.join(bdir, s.replace(".c", ".o"))
@@ -147,17 +163,30 @@ def build(name: str, force: bool = False) -> str:
         _run([cc, *flags, "-I", os.path.join(HERE, "shim"), "-c", os.path.join(HERE, s), "-o", o])
         objs.append(o)
     tmp = lib + ".tmp"
-    _run([cc, "-shared", "-Wl,-Bsymbolic", "-o", tmp, *objs, "-lm", "-lpthread"])
+    link = ["-lm", "-lpthread"]
+    if dropin:
+        rel = os.path.relpath(chns_lib_dir, bdir)
+        link = ["-L", chns_lib_dir, "-lchns_b200", f"-Wl,-rpath,$ORIGIN/{rel}"] + link
+    _run([cc, "-shared", "-Wl,-Bsymbolic", "-o", tmp, *objs, *link])
     os.replace(tmp, lib)
     for o in objs:
         os.remove(o)
     return lib
 
 
-def build_all(names=None, force=False) -> list[str]:
+# configurations also built with the drop-in etd2rk (needs libchns_b200.so)
+DROPIN_CONFIGS = ["ns32", "bin32", "ter32", "bindef64", "terdef64"]
+
+
+def build_all(names=None, force=False, dropin: bool = True) -> list[str]:
     if not reference_present():
         return []
-    return [build(n, force) for n in (names or list(CONFIGS))]
+    out = [build(n, force) for n in (names or list(CONFIGS))]
+    if dropin:
+        for n in DROPIN_CONFIGS:
+            if names is None or n in names:
+                out.append(build(n, force, dropin=True))
+    return out
 
 
 if __name__ == "__main__":

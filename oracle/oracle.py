@@ -215,8 +215,8 @@ def ref_config_params(name: str) -> dict:
 class RefLib:
     """The reference's own etd2rk/nonlin/... compiled for one configuration (oracle/_ref)."""
 
-    def __init__(self, name: str, nthreads: int = 1):
-        path = build_ref.lib_path(name)
+    def __init__(self, name: str, nthreads: int = 1, dropin: bool = False):
+        path = build_ref.lib_path(name, dropin)
         if not os.path.isfile(path):
             raise FileNotFoundError(path)
         L = ctypes.CDLL(path, mode=getattr(os, "RTLD_LOCAL", 0) | getattr(os, "RTLD_NOW", 2))

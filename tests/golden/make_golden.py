@@ -39,9 +39,9 @@ SMALL = [
     ("terdef64", 20, 4, 6, 3.0, 0.5),
 ]
 FULL = [
-    # binary 256^2, omega = 0, spinodal c, 1000 steps
+    # binary spinodal run: 256^2, omega = 0, c = (1 + U(+-0.05) - mean)/2, 1000 steps
     ("bin256", 1000, 100, None, 0.0, 0.0),
-    # ternary 512^2, omega = 0, c_i = 1/3 + U(+-0.02), 2000 steps
+    # ternary spinodal run: 512^2, omega = 0, c_i = 1/3 + U(+-0.02), 2000 steps at dt = 5e-5
     ("ter512", 2000, 101, None, 0.0, 0.0),
 ]
 

@@ -1,0 +1,65 @@
+"""CPU tests of the C ABI library: it loads without a GPU, exports every
+function include/chns.h declares, and validates arguments before touching CUDA."""
+import ctypes
+import math
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "chns.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(chns_[a-z0-9_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import chns_b200
+
+    if not os.path.isfile(chns_b200.LIB_PATH):
+        pytest.fail("libchns_b200.so is not built (run __graft_entry__.build())")
+    return chns_b200.load_library()
+
+
+def test_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert "chns_create" in names and "chns_step" in names
+    for nm in names:
+        assert hasattr(lib, nm), nm
+
+
+def test_default_params_are_the_reference_defaults(lib):
+    import chns_b200
+
+    p = chns_b200.default_params(chns_b200.MODEL_BINARY, 1024)
+    # global.h:20-31, 102-104
+    assert p["lx"] == 4.0 * math.pi and p["dt"] == 1e-4 and p["nu"] == 0.01
+    assert p["sigma"] == 2.0 and p["lambda"] == 1e-6 and p["epsilon"] == 3.0 * (4.0 * math.pi / 1024)
+    q = chns_b200.default_params(chns_b200.MODEL_TERNARY, 1024)
+    assert (q["sigma12"], q["sigma23"], q["sigma13"], q["lambda"], q["xlambda"]) == (0.2, 0.45, 0.2, 1e-4, 2.0)
+
+
+@pytest.mark.parametrize("bad", [dict(nx=100), dict(nx=8192), dict(ny=512), dict(dealias_div=2.0),
+                                 dict(dt=0.0), dict(model=3), dict(precision=7), dict(coef_mode=4),
+                                 dict(force_amp=1.0, force_k=4.5)])
+def test_create_rejects_bad_parameters_without_cuda(lib, bad):
+    import chns_b200
+
+    p = dict(model=1, nx=256, ny=256, dt=1e-3, nu=0.01, sigma=0.2, epsilon=0.05)
+    p["lambda"] = 0.005
+    p.update(bad)
+    if "nx" in bad and "ny" not in bad:
+        p["ny"] = bad["nx"]
+    s = chns_b200.make_params(p)
+    h = ctypes.c_void_p()
+    rc = lib.chns_create(ctypes.byref(s), ctypes.byref(h))
+    assert rc in (-1, -5) and not h.value
+
+
+def test_status_strings(lib):
+    for s in (0, -1, -2, -3, -4, -5, -6):
+        assert lib.chns_status_string(s)

@@ -2,7 +2,7 @@
 (the reference's own code run here: golden fixtures, and the C restatement).
 
 Tolerances: FP64 relative L2 <= 1e-11 after 20 steps on small grids and
-<= 1e-10 after 1000 / 2000 steps on BASELINE configurations 0 and 1 (the only
+<= 1e-10 after 1000 / 2000 steps on the binary 256^2 and ternary 512^2 runs (the only
 differences are FFT round-off, ~1e-16 per transform); FP32 <= 1e-5.
 """
 import math
@@ -102,8 +102,8 @@ def test_phase_init_matches_reference(chns, name):
 
 @pytest.mark.parametrize("name,seed", [("bin256", 100), ("ter512", 101)])
 def test_baseline_configs_match_reference(chns, name, seed):
-    """BASELINE configurations 0 (binary 256^2, 1000 steps) and 1 (ternary 512^2,
-    2000 steps) against the reference's run: fingerprint (low modes, random
+    """The binary 256^2 (1000 steps) and ternary 512^2 (2000 steps, dt = 5e-5)
+    spinodal runs against the reference's run: fingerprint (low modes, random
     projections, norm) within 1e-10, mean concentration conserved to round-off."""
     g = load_full(name)
     p = g["params"]

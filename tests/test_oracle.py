@@ -78,7 +78,7 @@ def test_restatement_bitwise_vs_live_reference(name):
 
 
 def test_restatement_cfg0_full_fingerprint():
-    """BASELINE configuration 0 (binary 256^2, 1000 steps) against the reference run."""
+    """Binary spinodal 256^2, 1000 steps, against the reference run."""
     g = load_full("bin256")
     p = g["params"]
     o = O.Oracle(p, nthreads=1)
