@@ -124,6 +124,25 @@ int chns_profile_step(chns_ctx *ctx, int reps, float *ms, int *kind, int maxk);
 
 const char *chns_status_string(int status);
 
+/* Largest grid of chns_dfft_noalloc. */
+#define CHNS_NOALLOC_MAX_N 512
+
+/* The reference's dfft (fft.c:11-14) for callers that cannot allocate device
+ * memory.  This entry point has no counterpart in the reference: it exists for
+ * code that must not call cudaMalloc when it transforms (code running inside
+ * another library's allocator or memory pool, or whose device memory is handed
+ * out by a host application that owns it).  It needs no context: `real` (n x n
+ * doubles) and `spec` (FFTW layout, n x (n/2+1) complex doubles) are DEVICE
+ * pointers the caller owns; the transform's one intermediate field lives in a
+ * fixed device array of 2 x 257 x 512 complex doubles (4.2 MB) that every GPU
+ * loading this library holds until exit, so n must be a power of two with
+ * 32 <= n <= CHNS_NOALLOC_MAX_N (else CHNS_ERR_UNSUPPORTED).  The first call on a
+ * device does a one-time set-up for that device (symbol lookup and twiddle
+ * upload); make it before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race, so order them on one stream.  Work is
+ * enqueued on `stream` (a cudaStream_t, NULL = legacy default stream); the call
+ * returns without waiting for it. */
+int chns_dfft_noalloc(const double *real, double *spec, int n, void *stream);
 
 #ifdef __cplusplus
 }

@@ -75,6 +75,8 @@ def load_library(path: str = LIB_PATH):
     L.chns_launches_per_step.argtypes = [vp]
     L.chns_profile_step.argtypes = [vp, ip, vp, vp, ip]
     L.chns_profile_step.restype = ip
+    L.chns_dfft_noalloc.argtypes = [vp, vp, ip, vp]
+    L.chns_dfft_noalloc.restype = ip
     L.chns_status_string.restype = ctypes.c_char_p
     L.chns_status_string.argtypes = [ip]
     _lib = L

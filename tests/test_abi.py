@@ -27,7 +27,7 @@ def lib():
 
 def test_exports_every_declared_symbol(lib):
     names = declared_functions()
-    assert "chns_create" in names and "chns_step" in names
+    assert "chns_create" in names and "chns_step" in names and "chns_dfft_noalloc" in names
     for nm in names:
         assert hasattr(lib, nm), nm
 
@@ -58,6 +58,12 @@ def test_create_rejects_bad_parameters_without_cuda(lib, bad):
     h = ctypes.c_void_p()
     rc = lib.chns_create(ctypes.byref(s), ctypes.byref(h))
     assert rc in (-1, -5) and not h.value
+
+
+def test_noalloc_rejects_sizes_before_touching_the_device(lib):
+    for n in (1024, 2048, 100, 16):
+        assert lib.chns_dfft_noalloc(ctypes.c_void_p(8), ctypes.c_void_p(8), n, None) == -5
+    assert lib.chns_dfft_noalloc(None, None, 64, None) == -1
 
 
 def test_status_strings(lib):
