@@ -156,6 +156,23 @@ template <int N> struct FftShape {
   static constexpr int SMEM = N + N / 16;            // complex slots per group
 };
 
+// Multiplies u[r], r = 1..15, by w^r (conj for the inverse), w = tw[base]:
+// w, w^2, w^4, w^8 are read from the table and the other powers formed by at
+// most two complex products.
+template <int DIR, class R>
+__device__ __forceinline__ void apply_tw16(cx<R>* u, const cx<R>* __restrict__ tw, int base, int mask) {
+  const cx<R> w1 = tw[base & mask], w2 = tw[(2 * base) & mask];
+  const cx<R> w4 = tw[(4 * base) & mask], w8 = tw[(8 * base) & mask];
+  const cx<R> w3 = cmul(w1, w2), w12 = cmul(w8, w4);
+  cx<R> w[16];
+  w[1] = w1; w[2] = w2; w[3] = w3; w[4] = w4;
+  w[5] = cmul(w4, w1); w[6] = cmul(w4, w2); w[7] = cmul(w4, w3);
+  w[8] = w8; w[9] = cmul(w8, w1); w[10] = cmul(w8, w2); w[11] = cmul(w8, w3);
+  w[12] = w12; w[13] = cmul(w12, w1); w[14] = cmul(w12, w2); w[15] = cmul(w12, w3);
+#pragma unroll
+  for (int r = 1; r < 16; r++) u[r] = DIR < 0 ? cmul(u[r], w[r]) : cmulc(u[r], w[r]);
+}
+
 // One Stockham stage: radix RADIX, span NS (product of the earlier radices).
 // v holds x[t + NT*m]; writes the stage output to sh (padded).
 template <int N, int DIR, int RADIX, int NS, class R>
@@ -170,12 +187,9 @@ __device__ __forceinline__ void fft_stage_to_smem(cx<R>* v, cx<R>* sh, int t, co
 #pragma unroll
     for (int r = 0; r < RADIX; r++) u[r] = v[b + r * B];
     if (NS > 1) {
-      // twiddle W_{NS*RADIX}^{k r} = tw[k r N/(NS RADIX)], conjugated for the inverse
-#pragma unroll
-      for (int r = 1; r < RADIX; r++) {
-        cx<R> w = tw[(k * r * (N / (NS * RADIX))) & (N - 1)];
-        u[r] = DIR < 0 ? cmul(u[r], w) : cmulc(u[r], w);
-      }
+      // twiddles W_{NS*RADIX}^{k r} = tw[k r N/(NS RADIX)] (conjugated for the inverse)
+      static_assert(NS == 1 || RADIX == 16, "twiddled stages are radix 16");
+      apply_tw16<DIR>(u, tw, k * (N / (NS * RADIX)), N - 1);
     }
     dft<DIR, RADIX, 1>(u);
     const int base = (j / NS) * NS * RADIX + k;
@@ -195,14 +209,7 @@ __device__ __forceinline__ void fft_load_smem(cx<R>* v, const cx<R>* sh, int t) 
 template <int N, int DIR, class R>
 __device__ __forceinline__ void fft_last_stage(cx<R>* v, int t, const cx<R>* __restrict__ tw) {
   constexpr int NS = N / 16;
-  if (NS > 1) {
-    const int k = t;  // j = t < NS
-#pragma unroll
-    for (int r = 1; r < 16; r++) {
-      cx<R> w = tw[(k * r) & (N - 1)];
-      v[r] = DIR < 0 ? cmul(v[r], w) : cmulc(v[r], w);
-    }
-  }
+  if (NS > 1) apply_tw16<DIR>(v, tw, t, N - 1);  // j = t < NS, twiddles tw[t r]
   dft<DIR, 16, 1>(v);
 }
 

@@ -61,6 +61,9 @@ template <class R> struct Bufs {
   cx<R>* h[NH];
 };
 
+// FP32 step kernels are built for two CTAs per SM (<= 128 registers), FP64 for one
+#define CHNS_STEP_BOUNDS(N, R, GPC) __launch_bounds__((GPC) * ((N) / 16), sizeof(R) == 4 ? 2 : 1)
+
 template <class R> __device__ __forceinline__ cx<R> czero() { return mk<R>((R)0, (R)0); }
 
 // signed wavenumber index of column i (functions.c:17-24: Nyquist positive)
@@ -151,7 +154,7 @@ template <int N, class R> struct Frag {
 
 // What P1 emits, per model, into the G slots.
 template <int N, class R, int GPC, int MODEL>
-__global__ void __launch_bounds__(GPC * (N / 16)) k_spec_inv(const Bufs<R> B, const Par<R> P) {
+__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_inv(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
@@ -253,7 +256,7 @@ template <class R> struct AdvIO {
 };
 
 template <int N, class R, int GPC, int NACC, int PRE>
-__global__ void __launch_bounds__(GPC * (N / 16))
+__global__ void CHNS_STEP_BOUNDS(N, R, GPC)
 k_row_adv(const Bufs<R> B, const Par<R> P, const AdvIO<R> io) {
   constexpr int NT = N / 16;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -338,7 +341,7 @@ k_row_adv(const Bufs<R> B, const Par<R> P, const AdvIO<R> io) {
 // the reference are summed before the transform: F[a] + F[b] = F[a + b])
 // ---------------------------------------------------------------------------
 template <int N, class R, int GPC, int MODEL>
-__global__ void __launch_bounds__(GPC * (N / 16)) k_row_force(const Bufs<R> B, const Par<R> P) {
+__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
@@ -445,7 +448,7 @@ __device__ __forceinline__ void etd_k0(double* st, double* sv, double nx, double
 //          nonlin.c:300-377, etd2rk.c:117-130 / 191-206
 // ---------------------------------------------------------------------------
 template <int N, class R, int GPC, int MODEL, int STAGE>
-__global__ void __launch_bounds__(GPC * (N / 16)) k_spec_fwd_c(const Bufs<R> B, const Par<R> P) {
+__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
   constexpr bool F32 = sizeof(R) == 4;
@@ -540,7 +543,7 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_spec_fwd_c(const Bufs<R> B, 
 // P3 for pure Navier-Stokes: NACC = 0 (N_w = -F[u.grad w] only)
 // ---------------------------------------------------------------------------
 template <int N, class R, int GPC, bool CURL, int STAGE>
-__global__ void __launch_bounds__(GPC * (N / 16)) k_spec_curl_w(const Bufs<R> B, const Par<R> P) {
+__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
   constexpr bool F32 = sizeof(R) == 4;
