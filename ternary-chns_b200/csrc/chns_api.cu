@@ -350,8 +350,9 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
     twd[2 * q + 1] = (double)-sinl(a);
   }
 
-  const size_t ncx = (size_t)nr * n;           // complex per S/H field
-  const size_t ngx = (size_t)(c->jt + 1) * n;  // complex per G field
+  const size_t ncx = (size_t)nr * n;                // complex per S field
+  const size_t ngx = (size_t)(c->jt + 1) * 2 * n;   // complex per G slot (pair width)
+  const size_t nhx = (size_t)nr * 2 * n;            // complex per H slot (pair width)
   const size_t cxsz = 2 * c->rsz;
   const int nfields = p.model + 1;
   rc = CHNS_OK;
@@ -362,8 +363,8 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
     }
   }
   if (rc == CHNS_OK) rc = dmalloc(&c->nw, ncx * cxsz);
-  for (int k = 0; k < 12 && rc == CHNS_OK; k++) rc = dmalloc(&c->g[k], ngx * cxsz);
-  for (int k = 0; k < 7 && rc == CHNS_OK; k++) rc = dmalloc(&c->h[k], ncx * cxsz);
+  for (int k = 0; k < chns::kNumG && rc == CHNS_OK; k++) rc = dmalloc(&c->g[k], ngx * cxsz);
+  for (int k = 0; k < chns::kNumH && rc == CHNS_OK; k++) rc = dmalloc(&c->h[k], nhx * cxsz);
   if (rc == CHNS_OK) rc = dmalloc(&c->coef, 6 * tsz * c->rsz);
   if (rc == CHNS_OK) rc = dmalloc((void**)&c->mrow, nr * sizeof(int));
   if (rc == CHNS_OK) rc = dmalloc(&c->tw, (size_t)n * cxsz);

@@ -16,12 +16,36 @@ namespace chns {
 
 constexpr int NRED = 8;  // partial sums per CTA
 
+// inverse y transform with direct loads (diagnostics only)
+template <int N, class R>
+__device__ __forceinline__ void row_c2r_direct(cx<R>* v, RowSrc<R> s, int jt, bool live, int t, cx<R>* sh,
+                                               const Tw<R>& tw) {
+  constexpr int NT = N / 16;
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    const int k = t + NT * m;
+    const bool cj = k > N / 2;
+    const int kk = cj ? N - k : k;
+    cx<R> a = czero<R>(), b = czero<R>();
+    if (live && kk <= jt) {
+      const cx<R>* p = s.base + (size_t)kk * s.stride + s.off;
+      a = p[0];
+      b = p[1];
+    }
+    if (kk == 0 || kk == N / 2) { a.y = (R)0; b.y = (R)0; }
+    v[m] = cj ? mk<R>(a.x + b.y, b.x - a.y) : mk<R>(a.x - b.y, a.y + b.x);
+  }
+  fft<N, +1>(v, sh, t, tw);
+}
+
 template <int N, class R, int GPC, int MODEL>
 __global__ void __launch_bounds__(GPC * (N / 16)) k_diag_spec(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = blockIdx.x * GPC + g;
   const bool live = row < NR;
@@ -36,27 +60,33 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_diag_spec(const Bufs<R> B, c
 #pragma unroll
     for (int f = 0; f < (MODEL == MODEL_TERNARY ? 2 : 1); f++) {
       load_row<N>(in, f == 0 ? B.c1 : B.c2, row, live, t);
-      // c (untruncated, free_energy.c:21-22)
+      // c, untruncated (free_energy.c:21-22)
 #pragma unroll
       for (int m = 0; m < 16; m++) v[m] = mk<R>(in[m].x * sc, in[m].y * sc);
-      fft<N, +1>(v, sh, t, P.tw);
-      store_row<N>(v, B.h[f == 0 ? HA : HF1], row, live, t);
-      // grad c (untruncated, free_energy.c:72-78 / 107-119)
+      fft<N, +1>(v, sh, t, TW);
+      if (MODEL == MODEL_BINARY) store_row<N>(v, B.h[HF], row, live, t);
+      else store_row_pair<N>(v, B.h[HF], row, f, live, t);
+      // grad c, untruncated (free_energy.c:72-78 / 107-119)
 #pragma unroll
-      for (int m = 0; m < 16; m++) { const R kx = kxm(m); v[m] = mk<R>(-rmul(kx, in[m].y) * sc, rmul(kx, in[m].x) * sc); }
-      fft<N, +1>(v, sh, t, P.tw);
-      store_row<N>(v, B.h[f == 0 ? HB1 : HF2], row, live, t);
+      for (int d = 0; d < 2; d++) {
 #pragma unroll
-      for (int m = 0; m < 16; m++) v[m] = mk<R>(-rmul(ky, in[m].y) * sc, rmul(ky, in[m].x) * sc);
-      fft<N, +1>(v, sh, t, P.tw);
-      store_row<N>(v, B.h[f == 0 ? HB2 : HFX], row, live, t);
+        for (int m = 0; m < 16; m++) {
+          const R k = d == 0 ? kxm(m) : ky;
+          v[m] = mk<R>(-rmul(k, in[m].y) * sc, rmul(k, in[m].x) * sc);
+        }
+        fft<N, +1>(v, sh, t, TW);
+        store_row_pair<N>(v, B.h[f == 0 ? HAB : HFF], row, d, live, t);
+      }
       // truncated c for the phase masks (kinetic_energy.c:23-32)
       if (tr) {
 #pragma unroll
         for (int m = 0; m < 16; m++)
-          v[m] = amask<N, R>(t, m) <= mlim ? mk<R>(in[m].x * sc, in[m].y * sc) : czero<R>();
-        fft<N, +1>(v, sh, t, P.tw);
-        if (row <= P.jt) store_row<N>(v, B.g[f == 0 ? GC1 : GC2], row, live, t);
+          v[m] = amask<N>(t, m) <= mlim ? mk<R>(in[m].x * sc, in[m].y * sc) : czero<R>();
+        fft<N, +1>(v, sh, t, TW);
+        if (row <= P.jt) {
+          if (MODEL == MODEL_BINARY) store_row<N>(v, B.g[GCT], row, live, t);
+          else store_row_pair<N>(v, B.g[GCT], row, f, live, t);
+        }
       }
     }
   }
@@ -69,11 +99,11 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_diag_spec(const Bufs<R> B, c
       for (int m = 0; m < 16; m++) {
         const R kx = kxm(m), ks = ksq(kx, ky);
         R a = (R)0, b = (R)0;
-        if (ks > (R)1e-12 && amask<N, R>(t, m) <= mlim) { a = rdiv(in[m].x, ks); b = rdiv(in[m].y, ks); }
+        if (ks > (R)1e-12 && amask<N>(t, m) <= mlim) { a = rdiv(in[m].x, ks); b = rdiv(in[m].y, ks); }
         v[m] = d == 0 ? mk<R>(-rmul(ky, b) * sc, rmul(ky, a) * sc) : mk<R>(rmul(kx, b) * sc, -rmul(kx, a) * sc);
       }
-      fft<N, +1>(v, sh, t, P.tw);
-      if (row <= P.jt) store_row<N>(v, B.g[d == 0 ? GU : GV], row, live, t);
+      fft<N, +1>(v, sh, t, TW);
+      if (row <= P.jt) store_row_pair<N>(v, B.g[GUV], row, d, live, t);
     }
   }
 }
@@ -82,85 +112,74 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_diag_spec(const Bufs<R> B, c
 template <int N, class R, int GPC, int MODEL>
 __global__ void __launch_bounds__(GPC * (N / 16)) k_diag_row(const Bufs<R> B, const Par<R> P, double* part) {
   constexpr int NT = N / 16;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int pair = blockIdx.x * GPC + g;
   const bool live = pair < N / 2;
   const int i0 = 2 * pair;
   const int jt = P.jt;
+  auto pf = [&](cx<R>* base, int i) { return RowSrc<R>{base, 2 * N, 2 * i}; };
   double acc[NRED] = {0, 0, 0, 0, 0, 0, 0, 0};
-  cx<R> a[16], b[16];
-  // velocity: eu, and keep 0.5|u|^2 for the phase sums
-  row_c2r<N>(a, B.g[GU], i0, jt, live, t, sh, P.tw);
-  row_c2r<N>(b, B.g[GV], i0, jt, live, t, sh, P.tw);
-  double ke[16][2];
-#pragma unroll
-  for (int m = 0; m < 16; m++) {
-    ke[m][0] = 0.5 * ((double)a[m].x * (double)a[m].x + (double)b[m].x * (double)b[m].x);
-    ke[m][1] = 0.5 * ((double)a[m].y * (double)a[m].y + (double)b[m].y * (double)b[m].y);
-    acc[2] += ke[m][0] + ke[m][1];
-  }
+  cx<R> a[16], b[16], c[16];
   if constexpr (MODEL == MODEL_BINARY) {
-    row_c2r<N>(a, B.g[GC1], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-    for (int m = 0; m < 16; m++) {
-      if (a[m].x >= (R)0.5) { acc[3] += ke[m][0]; acc[5] += 1.0; }
-      if (a[m].y >= (R)0.5) { acc[3] += ke[m][1]; acc[5] += 1.0; }
-    }
-    row_c2r<N>(a, B.h[HA], i0, N / 2, live, t, sh, P.tw);
+    row_c2r_direct<N>(c, RowSrc<R>{B.g[GCT], N, i0}, jt, live, t, sh, TW);  // c_t of x-rows i0, i1
+    row_c2r_direct<N>(a, RowSrc<R>{B.h[HF], N, i0}, N / 2, live, t, sh, TW);  // c (untruncated)
 #pragma unroll
     for (int m = 0; m < 16; m++) {
       const double c0 = a[m].x, c1 = a[m].y;
       acc[0] += c0 * c0 * (1.0 - c0) * (1.0 - c0) + c1 * c1 * (1.0 - c1) * (1.0 - c1);
     }
-    row_c2r<N>(a, B.h[HB1], i0, N / 2, live, t, sh, P.tw);
-    row_c2r<N>(b, B.h[HB2], i0, N / 2, live, t, sh, P.tw);
 #pragma unroll
-    for (int m = 0; m < 16; m++)
-      acc[1] += (double)a[m].x * a[m].x + (double)b[m].x * b[m].x + (double)a[m].y * a[m].y + (double)b[m].y * b[m].y;
-  } else if constexpr (MODEL == MODEL_TERNARY) {
-    row_c2r<N>(a, B.g[GC1], i0, jt, live, t, sh, P.tw);
-    row_c2r<N>(b, B.g[GC2], i0, jt, live, t, sh, P.tw);
+    for (int h = 0; h < 2; h++) {
+      row_c2r_direct<N>(a, pf(B.g[GUV], i0 + h), jt, live, t, sh, TW);
 #pragma unroll
-    for (int m = 0; m < 16; m++) {
-      if (a[m].x >= (R)0.5) { acc[3] += ke[m][0]; acc[5] += 1.0; }
-      if (a[m].y >= (R)0.5) { acc[3] += ke[m][1]; acc[5] += 1.0; }
-      if (b[m].x >= (R)0.5) { acc[4] += ke[m][0]; acc[6] += 1.0; }
-      if (b[m].y >= (R)0.5) { acc[4] += ke[m][1]; acc[6] += 1.0; }
+      for (int m = 0; m < 16; m++) {
+        const double ke = 0.5 * ((double)a[m].x * a[m].x + (double)a[m].y * a[m].y);
+        acc[2] += ke;
+        if ((h ? c[m].y : c[m].x) >= (R)0.5) { acc[3] += ke; acc[5] += 1.0; }
+      }
+      row_c2r_direct<N>(b, pf(B.h[HAB], i0 + h), N / 2, live, t, sh, TW);
+#pragma unroll
+      for (int m = 0; m < 16; m++) acc[1] += (double)b[m].x * b[m].x + (double)b[m].y * b[m].y;
     }
+  } else if constexpr (MODEL == MODEL_TERNARY) {
     const double g1 = P.g1, g2 = P.g2, g3 = P.g3;
-    row_c2r<N>(a, B.h[HA], i0, N / 2, live, t, sh, P.tw);
-    row_c2r<N>(b, B.h[HF1], i0, N / 2, live, t, sh, P.tw);
 #pragma unroll
-    for (int m = 0; m < 16; m++) {
+    for (int h = 0; h < 2; h++) {
+      const int i = i0 + h;
+      row_c2r_direct<N>(c, pf(B.g[GCT], i), jt, live, t, sh, TW);  // (c1_t, c2_t)
+      row_c2r_direct<N>(a, pf(B.g[GUV], i), jt, live, t, sh, TW);
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const double p = h ? a[m].y : a[m].x, q = h ? b[m].y : b[m].x, r = 1.0 - p - q;
+      for (int m = 0; m < 16; m++) {
+        const double ke = 0.5 * ((double)a[m].x * a[m].x + (double)a[m].y * a[m].y);
+        acc[2] += ke;
+        if (c[m].x >= (R)0.5) { acc[3] += ke; acc[5] += 1.0; }
+        if (c[m].y >= (R)0.5) { acc[4] += ke; acc[6] += 1.0; }
+      }
+      row_c2r_direct<N>(a, pf(B.h[HF], i), N / 2, live, t, sh, TW);  // (c1, c2) untruncated
+#pragma unroll
+      for (int m = 0; m < 16; m++) {
+        const double p = a[m].x, q = a[m].y, r = 1.0 - p - q;
         acc[0] += g1 * p * p * (1.0 - p) * (1.0 - p) + g2 * q * q * (1.0 - q) * (1.0 - q) + g3 * r * r * (p + q) * (p + q);
       }
-    }
-    // gradients: c1x (HB1), c1y (HB2), c2x (HF2), c2y (HFX)
-    cx<R> c[16];
-    row_c2r<N>(a, B.h[HB1], i0, N / 2, live, t, sh, P.tw);
-    row_c2r<N>(b, B.h[HF2], i0, N / 2, live, t, sh, P.tw);
+      row_c2r_direct<N>(a, pf(B.h[HAB], i), N / 2, live, t, sh, TW);  // (c1x, c1y)
+      row_c2r_direct<N>(b, pf(B.h[HFF], i), N / 2, live, t, sh, TW);  // (c2x, c2y)
 #pragma unroll
-    for (int m = 0; m < 16; m++) {
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const double x1 = h ? a[m].y : a[m].x, x2 = h ? b[m].y : b[m].x;
-        acc[1] += g1 * x1 * x1 + g2 * x2 * x2 + g3 * (x1 + x2) * (x1 + x2);
+      for (int m = 0; m < 16; m++) {
+        const double x1 = a[m].x, y1 = a[m].y, x2 = b[m].x, y2 = b[m].y;
+        acc[1] += g1 * (x1 * x1 + y1 * y1) + g2 * (x2 * x2 + y2 * y2) + g3 * (x1 + x2) * (x1 + x2) +
+                  g3 * (y1 + y2) * (y1 + y2);
       }
     }
-    row_c2r<N>(a, B.h[HB2], i0, N / 2, live, t, sh, P.tw);
-    row_c2r<N>(c, B.h[HFX], i0, N / 2, live, t, sh, P.tw);
+  } else {
 #pragma unroll
-    for (int m = 0; m < 16; m++) {
+    for (int h = 0; h < 2; h++) {
+      row_c2r_direct<N>(a, pf(B.g[GUV], i0 + h), jt, live, t, sh, TW);
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const double y1 = h ? a[m].y : a[m].x, y2 = h ? c[m].y : c[m].x;
-        acc[1] += g1 * y1 * y1 + g2 * y2 * y2 + g3 * (y1 + y2) * (y1 + y2);
-      }
+      for (int m = 0; m < 16; m++) acc[2] += 0.5 * ((double)a[m].x * a[m].x + (double)a[m].y * a[m].y);
     }
   }
   if (!live) {

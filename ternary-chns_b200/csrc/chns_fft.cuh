@@ -173,10 +173,58 @@ __device__ __forceinline__ void apply_tw16(cx<R>* u, const cx<R>* __restrict__ t
   for (int r = 1; r < 16; r++) u[r] = DIR < 0 ? cmul(u[r], w[r]) : cmulc(u[r], w[r]);
 }
 
+// Twiddles of the two twiddled stages of a transform, precomputed once per
+// thread and kept in shared memory: slot 0 serves the first twiddled radix-16
+// stage (span R0 when R0 > 1, else span 16 when there are three radix-16
+// stages), slot 1 the last stage (span N/16).  Element (slot, q) of thread tid
+// holds w^(2^q), q = 0..3, at p[(4 slot + q) * stride] with p = base + tid.
+template <class R> struct Tw {
+  const cx<R>* p;
+  int stride;
+};
+
+template <int N, class R> constexpr size_t tw_smem_per_thread() { return 8 * sizeof(cx<R>); }
+
+// Fills this thread's slots from the table tw[q] = exp(-2 pi i q / N).
+template <int N, class R>
+__device__ __forceinline__ Tw<R> tw_setup(cx<R>* smem, const cx<R>* __restrict__ tw, int t) {
+  constexpr int NT = N / 16;
+  constexpr int LOGN = ilog2c(N);
+  constexpr int R0 = 1 << (LOGN % 4);
+  constexpr int N16 = LOGN / 4;
+  const int tid = threadIdx.x, stride = blockDim.x;
+  int base0 = -1;
+  if (R0 > 1 && N16 >= 2) base0 = (t % R0) * (N / (R0 * 16));
+  else if (N16 >= 3) base0 = (t % 16) * (N / 256);
+  const int base1 = NT > 1 ? t : -1;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    if (base0 >= 0) smem[(0 * 4 + q) * stride + tid] = tw[(base0 << q) & (N - 1)];
+    if (base1 >= 0) smem[(1 * 4 + q) * stride + tid] = tw[(base1 << q) & (N - 1)];
+  }
+  return Tw<R>{smem + tid, stride};
+}
+
+// Multiplies u[r], r = 1..15, by w^r (conj for the inverse) from the
+// precomputed w, w^2, w^4, w^8 of `slot`; other powers by at most two products.
+template <int DIR, class R>
+__device__ __forceinline__ void apply_tw16_pre(cx<R>* u, const Tw<R>& T, int slot) {
+  const cx<R> w1 = T.p[(4 * slot + 0) * T.stride], w2 = T.p[(4 * slot + 1) * T.stride];
+  const cx<R> w4 = T.p[(4 * slot + 2) * T.stride], w8 = T.p[(4 * slot + 3) * T.stride];
+  const cx<R> w3 = cmul(w1, w2), w12 = cmul(w8, w4);
+  cx<R> w[16];
+  w[1] = w1; w[2] = w2; w[3] = w3; w[4] = w4;
+  w[5] = cmul(w4, w1); w[6] = cmul(w4, w2); w[7] = cmul(w4, w3);
+  w[8] = w8; w[9] = cmul(w8, w1); w[10] = cmul(w8, w2); w[11] = cmul(w8, w3);
+  w[12] = w12; w[13] = cmul(w12, w1); w[14] = cmul(w12, w2); w[15] = cmul(w12, w3);
+#pragma unroll
+  for (int r = 1; r < 16; r++) u[r] = DIR < 0 ? cmul(u[r], w[r]) : cmulc(u[r], w[r]);
+}
+
 // One Stockham stage: radix RADIX, span NS (product of the earlier radices).
 // v holds x[t + NT*m]; writes the stage output to sh (padded).
 template <int N, int DIR, int RADIX, int NS, class R>
-__device__ __forceinline__ void fft_stage_to_smem(cx<R>* v, cx<R>* sh, int t, const cx<R>* __restrict__ tw) {
+__device__ __forceinline__ void fft_stage_to_smem(cx<R>* v, cx<R>* sh, int t, const Tw<R>& tw) {
   constexpr int NT = N / 16;
   constexpr int B = 16 / RADIX;  // butterflies per thread
 #pragma unroll
@@ -189,7 +237,7 @@ __device__ __forceinline__ void fft_stage_to_smem(cx<R>* v, cx<R>* sh, int t, co
     if (NS > 1) {
       // twiddles W_{NS*RADIX}^{k r} = tw[k r N/(NS RADIX)] (conjugated for the inverse)
       static_assert(NS == 1 || RADIX == 16, "twiddled stages are radix 16");
-      apply_tw16<DIR>(u, tw, k * (N / (NS * RADIX)), N - 1);
+      apply_tw16_pre<DIR>(u, tw, 0);
     }
     dft<DIR, RADIX, 1>(u);
     const int base = (j / NS) * NS * RADIX + k;
@@ -207,9 +255,9 @@ __device__ __forceinline__ void fft_load_smem(cx<R>* v, const cx<R>* sh, int t) 
 
 // Last radix-16 stage (NS = N/16): result stays in registers in natural order.
 template <int N, int DIR, class R>
-__device__ __forceinline__ void fft_last_stage(cx<R>* v, int t, const cx<R>* __restrict__ tw) {
+__device__ __forceinline__ void fft_last_stage(cx<R>* v, int t, const Tw<R>& tw) {
   constexpr int NS = N / 16;
-  if (NS > 1) apply_tw16<DIR>(v, tw, t, N - 1);  // j = t < NS, twiddles tw[t r]
+  if (NS > 1) apply_tw16_pre<DIR>(v, tw, 1);  // j = t < NS, twiddles tw[t r]
   dft<DIR, 16, 1>(v);
 }
 
@@ -217,7 +265,7 @@ __device__ __forceinline__ void fft_last_stage(cx<R>* v, int t, const cx<R>* __r
 // (it uses __syncthreads); sh is this group's padded buffer of FftShape<N>::SMEM.
 // The leading barrier protects the buffer from the previous transform's readers.
 template <int N, int DIR, class R>
-__device__ __forceinline__ void fft(cx<R>* v, cx<R>* sh, int t, const cx<R>* __restrict__ tw) {
+__device__ __forceinline__ void fft(cx<R>* v, cx<R>* sh, int t, const Tw<R>& tw) {
   using S = FftShape<N>;
   if constexpr (S::N16 == 1 && S::R0 == 1) {
     fft_last_stage<N, DIR>(v, t, tw);  // N = 16: single stage

@@ -8,6 +8,9 @@
 struct chns_ctx;
 
 namespace chns {
+// intermediate buffers of a step: G slots (rows 0..jt) and H slots (rows
+// 0..n/2), each of width 2n complex (see chns_kernels.cuh)
+constexpr int kNumG = 6, kNumH = 4;
 
 // Launchers instantiated per grid size and precision (chns_inst_*.cu).
 struct Launchers {

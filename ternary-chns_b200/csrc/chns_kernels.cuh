@@ -1,24 +1,31 @@
 // chns_kernels.cuh -- the fused passes of one ETD2RK stage on sm_100a.
 //
 // Data layout in HBM (see also chns_api.cu):
-//   S layout  : spectral field, row j' (ky index, 0..n/2) of n complex along kx
-//               (the transpose of FFTW's n x (n/2+1) layout, global.h:13-14), so
-//               the column transforms along x are contiguous rows.
-//   G layout  : like S but only rows 0..jt, jt = the last ky row that survives
-//               the truncation (functions.c:47-84).  Holds fields that went
-//               through the column (x) inverse transform and wait for the row
-//               (y) inverse transform.
-//   H layout  : like S; holds fields after the row (y) forward transform,
-//               waiting for the column (x) forward transform.
+//   S layout : spectral field, row j' (ky index 0..n/2) of n complex along kx
+//              (the transpose of FFTW's n x (n/2+1) layout, global.h:13-14), so
+//              the x transforms read and write contiguous rows.
+//   G layout : fields after the x inverse transform, rows 0..jt only (jt = the
+//              last ky row that survives the truncation, functions.c:47-84).
+//   H layout : fields after the y forward transform, rows 0..n/2.
+//   A "pair field" interleaves two fields of the same x index: element
+//   [row][2 i + e], e = 0, 1 (row stride 2n).  The y transform of a pair field
+//   at x-row i is one complex transform of z = f0 + i f1, so products such as
+//   u.grad w = Re(z_uv) Re(z_w) + Im(z_uv) Im(z_w) come straight out of two
+//   transforms.  A "plain" field (row stride n) is transformed two x-rows at a
+//   time, z = f(i0) + i f(i0+1).
 //
 // One stage (etd2rk.c:28-135 or :146-212) of the binary model is five kernels:
-//   P1 spec_inv     : S -> G : velocity, gradients, truncation, 1/(nx ny), x-iFFT
-//   P2 row_adv      : G -> H : y-c2r of x-row pairs, u.grad w, u.grad c, f(c), y-r2c
-//   P3 spec_fwd_c   : H -> S : x-FFT; mu_hat and its x-iFFT (-> G); N_c; ETD of c
-//   P4 row_force    : G -> H : y-c2r of mu and grad c, mu grad c, y-r2c
-//   P5 spec_curl_w  : H -> S : x-FFT; curl; N_w; ETD of w
-// Ternary adds the chemical potential (chem_potential.c) to P2 and uses two
-// row kernels for P2.  Pure Navier-Stokes is P1, P2 and P3-ns.
+//   P1 spec_inv    : S -> G : velocity, gradients, truncation, 1/(nx ny), x-iFFT
+//   P2 row_adv     : G -> H : y-c2r, u.grad w, u.grad c, f(c), y-r2c
+//   P3 spec_fwd_c  : H -> S, G : x-FFT; -F[u.grad w]; mu and its x-iFFT; N_c; ETD of c
+//   P4 row_force   : G -> H : y-c2r of mu and grad c, mu grad c, y-r2c
+//   P5 spec_curl_w : H -> S : x-FFT; curl; N_w; ETD of w
+// Ternary adds the chemical potential (chem_potential.c) to P2.  Pure
+// Navier-Stokes is P1, P2 and P5 without the curl.
+//
+// The row passes stream their inputs through a shared-memory tile filled with
+// cp.async: the copy of the next transform's input is in flight while the
+// current transform runs.
 #pragma once
 
 #include "chns_fft.cuh"
@@ -27,10 +34,14 @@ namespace chns {
 
 enum { MODEL_NS = 0, MODEL_BINARY = 1, MODEL_TERNARY = 2 };
 
-// G-layout buffer slots
-enum { GU = 0, GV, GDXW, GDYW, GC1, GC2, GDX1, GDY1, GDX2, GDY2, GMU1, GMU2, NG };
-// H-layout buffer slots
-enum { HA = 0, HB1, HB2, HF1, HF2, HFX, HFY, NH };
+// G slots: pair fields (u,v), (dx w, dy w), (dx c1, dy c1), (dx c2, dy c2);
+// GCT truncated c (binary plain, ternary pair (c1,c2)); GMU mu (binary plain,
+// ternary pair (mu1, mu2)).  Every slot holds rows 0..jt of width 2n.
+enum { GUV = 0, GW, GD1, GD2, GCT, GMU, NG };
+// H slots: HAB pair (A, B1) = (u.grad w, u.grad c1) (pure Navier-Stokes: plain
+// A); HF binary plain f(c), ternary pair (mu^F_1, mu^F_2); HB2 plain
+// u.grad c2; HFF pair (Fx, Fy).  Every slot holds rows 0..n/2 of width 2n.
+enum { HAB = 0, HF, HB2, HFF, NH };
 
 template <class R> struct Par {
   int n, jt;               // grid; last G row that can hold a nonzero mode
@@ -72,21 +83,75 @@ template <int N> __device__ __forceinline__ int sidx(int i) { return i <= N / 2 
 template <class R> __device__ __forceinline__ R ksq(R kx, R ky) { return radd(rmul(kx, kx), rmul(ky, ky)); }
 
 // ---------------------------------------------------------------------------
-// row (y) transforms of a pair of x-rows
+// asynchronous tile copies (cp.async, 16 bytes each) into shared memory
 // ---------------------------------------------------------------------------
+static __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+static __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// two adjacent complex values (columns i0, i0+1, i0 even): one 16-byte access in FP32
-static __device__ __forceinline__ void ld_pair(const cxf* p, cxf& a, cxf& b) {
-  const float4 q = __ldg(reinterpret_cast<const float4*>(p));
-  a = mk<float>(q.x, q.y);
-  b = mk<float>(q.z, q.w);
+// The input of one y inverse transform: two complex values per G row k at
+// base[k * stride + off .. + 1] (a pair field at x-row i: stride 2n, off 2i;
+// a plain field at x-rows i0, i0+1: stride n, off i0).
+template <class R> struct RowSrc {
+  const cx<R>* base;
+  int stride, off;
+};
+
+// Group-cooperative copy of rows 0..jt of `s` into this group's tile
+// (2 complex per row) with cp.async; the caller commits.
+template <int N, class R>
+__device__ __forceinline__ void tile_issue(cx<R>* tile, RowSrc<R> s, int jt, bool live, int t) {
+  constexpr int NT = N / 16;
+  constexpr int CH = (int)(2 * sizeof(cx<R>) / 16);  // 16-byte chunks per row
+  if (!live) return;
+  for (int q = t; q < (jt + 1) * CH; q += NT) {
+    const int r = q / CH, c = q % CH;
+    cp_async16(reinterpret_cast<char*>(tile + 2 * r) + 16 * c,
+               reinterpret_cast<const char*>(s.base + (size_t)r * s.stride + s.off) + 16 * c);
+  }
 }
-static __device__ __forceinline__ void ld_pair(const cxd* p, cxd& a, cxd& b) {
-  const double2 q0 = __ldg(reinterpret_cast<const double2*>(p));
-  const double2 q1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
-  a = mk<double>(q0.x, q0.y);
-  b = mk<double>(q1.x, q1.y);
+
+// Builds Z = X0 + i X1 with the Hermitian extension from a tile (Im of the ky = 0
+// and ky = n/2 bins ignored: FFTW's c2r convention).  v[m] holds Z[t + NT m].
+template <int N, class R>
+__device__ __forceinline__ void build_c2r_input(cx<R>* v, const cx<R>* tile, int jt, int t) {
+  constexpr int NT = N / 16;
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    const int k = t + NT * m;
+    const bool cj = k > N / 2;
+    const int kk = cj ? N - k : k;
+    cx<R> a = czero<R>(), b = czero<R>();
+    if (kk <= jt) {
+      a = tile[2 * kk];
+      b = tile[2 * kk + 1];
+    }
+    if (kk == 0 || kk == N / 2) { a.y = (R)0; b.y = (R)0; }
+    v[m] = cj ? mk<R>(a.x + b.y, b.x - a.y) : mk<R>(a.x - b.y, a.y + b.x);
+  }
 }
+
+// Inverse y transform of the input already in flight to `tile`; issues the
+// copy of `next` (when has_next) as soon as the tile has been read.  Output:
+// v[m] = (f0[y], f1[y]) at y = t + NT m.
+template <int N, class R>
+__device__ __forceinline__ void row_c2r_tiled(cx<R>* v, cx<R>* tile, bool has_next, RowSrc<R> next, int jt,
+                                              bool live, int t, cx<R>* sh, const Tw<R>& tw) {
+  cp_async_wait_all();
+  __syncthreads();
+  build_c2r_input<N>(v, tile, jt, t);
+  __syncthreads();
+  if (has_next) {
+    tile_issue<N>(tile, next, jt, live, t);
+    cp_async_commit();
+  }
+  fft<N, +1>(v, sh, t, tw);
+}
+
+// two adjacent complex values (one 16-byte access in FP32)
 static __device__ __forceinline__ void st_pair(cxf* p, cxf a, cxf b) {
   *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
 }
@@ -95,32 +160,11 @@ static __device__ __forceinline__ void st_pair(cxd* p, cxd a, cxd b) {
   reinterpret_cast<double2*>(p)[1] = make_double2(b.x, b.y);
 }
 
-// Inverse y transform (c2r) of x-rows i0, i0+1 of a G-layout field: builds
-// Z = X_{i0} + i X_{i0+1} with the Hermitian extension (Im of the ky = 0 and
-// ky = n/2 bins ignored, FFTW's c2r convention) and transforms.  Output:
-// v[m] = (x_{i0}[y], x_{i0+1}[y]) at y = t + NT m.
+// Forward y transform of v = f0 + i f1, split into the two half spectra and
+// stored as (F0[k], F1[k]) at base[k * stride + off .. + 1], k = 0..n/2.
 template <int N, class R>
-__device__ __forceinline__ void row_c2r(cx<R>* v, const cx<R>* __restrict__ G, int i0, int jt, bool live,
-                                        int t, cx<R>* sh, const cx<R>* __restrict__ tw) {
-  constexpr int NT = N / 16;
-#pragma unroll
-  for (int m = 0; m < 16; m++) {
-    const int k = t + NT * m;
-    const bool cj = k > N / 2;
-    const int kk = cj ? N - k : k;
-    cx<R> a = czero<R>(), b = czero<R>();
-    if (live && kk <= jt) ld_pair(G + (size_t)kk * N + i0, a, b);
-    if (kk == 0 || kk == N / 2) { a.y = (R)0; b.y = (R)0; }
-    v[m] = cj ? mk<R>(a.x + b.y, b.x - a.y) : mk<R>(a.x - b.y, a.y + b.x);
-  }
-  fft<N, +1>(v, sh, t, tw);
-}
-
-// Forward y transform (r2c) of x-rows i0, i0+1 packed as v = a + i b, split
-// into the two half spectra and stored to rows 0..n/2 of an H-layout field.
-template <int N, class R>
-__device__ __forceinline__ void row_r2c_store(cx<R>* v, cx<R>* __restrict__ H, int i0, bool live, int t,
-                                              cx<R>* sh, const cx<R>* __restrict__ tw) {
+__device__ __forceinline__ void row_r2c_store(cx<R>* v, cx<R>* __restrict__ base, int stride, int off, bool live,
+                                              int t, cx<R>* sh, const Tw<R>& tw) {
   constexpr int NT = N / 16;
   fft<N, -1>(v, sh, t, tw);
   __syncthreads();
@@ -135,261 +179,36 @@ __device__ __forceinline__ void row_r2c_store(cx<R>* v, cx<R>* __restrict__ H, i
       const cx<R> q = sh[spad((N - k) & (N - 1))];
       const cx<R> A = mk<R>((R)0.5 * (z.x + q.x), (R)0.5 * (z.y - q.y));
       const cx<R> B = mk<R>((R)0.5 * (z.y + q.y), (R)0.5 * (q.x - z.x));
-      if (live) st_pair(H + (size_t)k * N + i0, A, B);
+      if (live) st_pair(base + (size_t)k * stride + off, A, B);
     }
   }
 }
 
-// thread-private frag slots in shared memory: element m of thread t at [t + NT m]
+// thread-private real slots in shared memory: element m of thread t at [t + NT m]
 template <int N, class R> struct Frag {
-  cx<R>* p;
-  __device__ __forceinline__ cx<R>& operator[](int m) const { return p[(threadIdx.x % (N / 16)) + (N / 16) * m]; }
+  R* p;
+  __device__ __forceinline__ R& operator[](int m) const { return p[(threadIdx.x % (N / 16)) + (N / 16) * m]; }
+};
+
+// shared memory of a row kernel: GPC transform buffers, GPC tiles, NFRAG real frags per group
+template <int N, class R, int GPC> struct RowSmem {
+  cx<R>* sh;
+  cx<R>* tile;
+  R* frag;
+  __device__ __forceinline__ RowSmem(unsigned char* raw, int g, int jt) {
+    cx<R>* base = reinterpret_cast<cx<R>*>(raw);
+    sh = base + g * FftShape<N>::SMEM;
+    tile = base + GPC * FftShape<N>::SMEM + (size_t)g * 2 * (jt + 1);
+    frag = reinterpret_cast<R*>(base + GPC * FftShape<N>::SMEM + (size_t)GPC * 2 * (jt + 1)) + (size_t)g * N;
+  }
+  static size_t bytes(int jt, int nfrag) {
+    return (size_t)GPC * FftShape<N>::SMEM * sizeof(cx<R>) + (size_t)GPC * 2 * (jt + 1) * sizeof(cx<R>) +
+           (size_t)nfrag * GPC * N * sizeof(R);
+  }
 };
 
 // ---------------------------------------------------------------------------
-// P1: spectral fan-out + x inverse transform   (S -> G)
-// nonlin.c:30-48, velocity.c:12-42, surface_tension.c:20-22,57-75,
-// nonlin.c:177-198,259-284, chem_potential.c:256-261
-// ---------------------------------------------------------------------------
-
-// What P1 emits, per model, into the G slots.
-template <int N, class R, int GPC, int MODEL>
-__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_inv(const Bufs<R> B, const Par<R> P) {
-  constexpr int NT = N / 16;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int g = threadIdx.x / NT, t = threadIdx.x % NT;
-  cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
-  const int row = blockIdx.x * GPC + g;
-  const bool live = row <= P.jt;
-  const int mlim = live ? P.mrow[row] : -1;
-  const R ky = (R)(P.fy * (double)row);
-  const R sc = P.scale;
-
-  uint32_t inmask = 0;
-#pragma unroll
-  for (int m = 0; m < 16; m++) {
-    const int ms = sidx<N>(t + NT * m);
-    if ((ms < 0 ? -ms : ms) <= mlim) inmask |= 1u << m;
-  }
-  auto kxm = [&](int m) -> R { return (R)(P.fx * (double)sidx<N>(t + NT * m)); };
-  auto store = [&](cx<R>* v, int slot) {
-    if (live) {
-      cx<R>* p = B.g[slot] + (size_t)row * N;
-#pragma unroll
-      for (int m = 0; m < 16; m++) p[t + NT * m] = v[m];
-    }
-  };
-
-  cx<R> in[16], v[16];
-  // omega_hat
-#pragma unroll
-  for (int m = 0; m < 16; m++)
-    in[m] = ((inmask >> m) & 1) ? B.w[(size_t)row * N + t + NT * m] : czero<R>();
-  // u = I ky psi, v = -I kx psi, psi = w / k^2  (velocity.c:12-42)
-#pragma unroll
-  for (int m = 0; m < 16; m++) {
-    const R kx = kxm(m), ks = ksq(kx, ky);
-    R a = (R)0, b = (R)0;
-    if (ks > (R)1e-12) { a = rdiv(in[m].x, ks); b = rdiv(in[m].y, ks); }
-    v[m] = mk<R>(-rmul(ky, b) * sc, rmul(ky, a) * sc);
-  }
-  fft<N, +1>(v, sh, t, P.tw);
-  store(v, GU);
-#pragma unroll
-  for (int m = 0; m < 16; m++) {
-    const R kx = kxm(m), ks = ksq(kx, ky);
-    R a = (R)0, b = (R)0;
-    if (ks > (R)1e-12) { a = rdiv(in[m].x, ks); b = rdiv(in[m].y, ks); }
-    v[m] = mk<R>(rmul(kx, b) * sc, -rmul(kx, a) * sc);
-  }
-  fft<N, +1>(v, sh, t, P.tw);
-  store(v, GV);
-  // grad omega: I kx w, I ky w  (nonlin.c:36-37)
-#pragma unroll
-  for (int m = 0; m < 16; m++) { const R kx = kxm(m); v[m] = mk<R>(-rmul(kx, in[m].y) * sc, rmul(kx, in[m].x) * sc); }
-  fft<N, +1>(v, sh, t, P.tw);
-  store(v, GDXW);
-#pragma unroll
-  for (int m = 0; m < 16; m++) v[m] = mk<R>(-rmul(ky, in[m].y) * sc, rmul(ky, in[m].x) * sc);
-  fft<N, +1>(v, sh, t, P.tw);
-  store(v, GDYW);
-
-  if constexpr (MODEL >= MODEL_BINARY) {
-#pragma unroll
-    for (int f = 0; f < (MODEL == MODEL_TERNARY ? 2 : 1); f++) {
-      const cx<R>* src = f == 0 ? B.c1 : B.c2;
-#pragma unroll
-      for (int m = 0; m < 16; m++)
-        in[m] = ((inmask >> m) & 1) ? src[(size_t)row * N + t + NT * m] : czero<R>();
-      // truncated c (surface_tension.c:20-22, nonlin.c:217, chem_potential.c:256-261)
-#pragma unroll
-      for (int m = 0; m < 16; m++) v[m] = mk<R>(in[m].x * sc, in[m].y * sc);
-      fft<N, +1>(v, sh, t, P.tw);
-      store(v, f == 0 ? GC1 : GC2);
-      // grad c: I kx c, I ky c (surface_tension.c:57-58, nonlin.c:187-188, 272-273, 314-315)
-#pragma unroll
-      for (int m = 0; m < 16; m++) { const R kx = kxm(m); v[m] = mk<R>(-rmul(kx, in[m].y) * sc, rmul(kx, in[m].x) * sc); }
-      fft<N, +1>(v, sh, t, P.tw);
-      store(v, f == 0 ? GDX1 : GDX2);
-#pragma unroll
-      for (int m = 0; m < 16; m++) v[m] = mk<R>(-rmul(ky, in[m].y) * sc, rmul(ky, in[m].x) * sc);
-      fft<N, +1>(v, sh, t, P.tw);
-      store(v, f == 0 ? GDY1 : GDY2);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// P2: advection products (+ bulk chemical potential) on x-row pairs (G -> H)
-// nonlin.c:56-74 (u.grad w), :201-215 (binary u.grad c), :286-300/328-348
-// (ternary u.grad c_i); surface_tension.c:24-35 / nonlin.c:217-230 (f(c));
-// chem_potential.c:263-320 (ternary mu^F)
-// ---------------------------------------------------------------------------
-
-// acc_a = u . (dx_a, dy_a) for NACC pairs of G slots, accumulated in shared memory
-// frags, forward transformed to H slots.  PRE selects extra work done first:
-// 0 none; 1 binary f(c) -> HF1; 2 ternary mu^F_1, mu^F_2 -> HF1, HF2.
-template <class R> struct AdvIO {
-  const cx<R>* dx[3];
-  const cx<R>* dy[3];
-  cx<R>* out[3];
-};
-
-template <int N, class R, int GPC, int NACC, int PRE>
-__global__ void CHNS_STEP_BOUNDS(N, R, GPC)
-k_row_adv(const Bufs<R> B, const Par<R> P, const AdvIO<R> io) {
-  constexpr int NT = N / 16;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int g = threadIdx.x / NT, t = threadIdx.x % NT;
-  cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
-  cx<R>* accbase = reinterpret_cast<cx<R>*>(smem_raw) + GPC * FftShape<N>::SMEM;
-  const int pair = blockIdx.x * GPC + g;
-  const bool live = pair < N / 2;
-  const int i0 = 2 * pair;
-  const int jt = P.jt;
-
-  cx<R> u[16], v[16];
-  if constexpr (PRE == 1) {
-    // f(c) = c (1 - c)(1 - 2c) on the truncated c (surface_tension.c:30-31, nonlin.c:225)
-    row_c2r<N>(v, B.g[GC1], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-    for (int m = 0; m < 16; m++) {
-      const R a = v[m].x, b = v[m].y;
-      v[m] = mk<R>(rmul(rmul(a, rsub((R)1, a)), rsub((R)1, rmul((R)2, a))),
-                   rmul(rmul(b, rsub((R)1, b)), rsub((R)1, rmul((R)2, b))));
-    }
-    row_r2c_store<N>(v, B.h[HF1], i0, live, t, sh, P.tw);
-  } else if constexpr (PRE == 2) {
-    // ternary bulk chemical potentials (chem_potential.c:303-315)
-    row_c2r<N>(u, B.g[GC1], i0, jt, live, t, sh, P.tw);
-    row_c2r<N>(v, B.g[GC2], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-    for (int m = 0; m < 16; m++) {
-      R o1[2], o2[2];
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const R c1 = h ? u[m].y : u[m].x, c2 = h ? v[m].y : v[m].x;
-        const R c3 = rsub(rsub((R)1, c1), c2);
-        const R c123 = rmul(rmul(c1, c2), c3);
-        const R fc1 = rmul(rmul(c1, rsub((R)1, c1)), rsub((R)1, rmul((R)2, c1)));
-        const R fc2 = rmul(rmul(c2, rsub((R)1, c2)), rsub((R)1, rmul((R)2, c2)));
-        const R fc3 = rmul(rmul(c3, rsub((R)1, c3)), rsub((R)1, rmul((R)2, c3)));
-        const R G1 = radd(rmul(P.g1, fc1), rmul(rmul(rmul(P.six_lam, c123), c2), c3));
-        const R G2 = radd(rmul(P.g2, fc2), rmul(rmul(rmul(P.six_lam, c123), c1), c3));
-        const R G3 = radd(rmul(P.g3, fc3), rmul(rmul(rmul(P.six_lam, c123), c1), c2));
-        const R m1 = radd(rmul(rsub(G1, G2), P.g2i), rmul(rsub(G1, G3), P.g3i));
-        const R m2 = radd(rmul(rsub(G2, G1), P.g1i), rmul(rsub(G2, G3), P.g3i));
-        o1[h] = rmul(m1, P.fac_mu);
-        o2[h] = rmul(m2, P.fac_mu);
-      }
-      u[m] = mk<R>(o1[0], o1[1]);
-      v[m] = mk<R>(o2[0], o2[1]);
-    }
-    row_r2c_store<N>(u, B.h[HF1], i0, live, t, sh, P.tw);
-    row_r2c_store<N>(v, B.h[HF2], i0, live, t, sh, P.tw);
-  }
-
-  if constexpr (NACC > 0) {
-    // first factor u: acc_a = u * dx_a
-    row_c2r<N>(u, B.g[GU], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-    for (int a = 0; a < NACC; a++) {
-      Frag<N, R> acc{accbase + (size_t)(a * GPC + g) * N};
-      row_c2r<N>(v, io.dx[a], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-      for (int m = 0; m < 16; m++) acc[m] = mk<R>(rmul(u[m].x, v[m].x), rmul(u[m].y, v[m].y));
-    }
-    // second factor: acc_a += v * dy_a, then the forward y transform
-    row_c2r<N>(u, B.g[GV], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-    for (int a = 0; a < NACC; a++) {
-      Frag<N, R> acc{accbase + (size_t)(a * GPC + g) * N};
-      row_c2r<N>(v, io.dy[a], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-      for (int m = 0; m < 16; m++) {
-        const cx<R> s = acc[m];
-        v[m] = mk<R>(radd(s.x, rmul(u[m].x, v[m].x)), radd(s.y, rmul(u[m].y, v[m].y)));
-      }
-      row_r2c_store<N>(v, io.out[a], i0, live, t, sh, P.tw);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// P4: surface-tension force mu grad c on x-row pairs (G -> H)
-// binary surface_tension.c:70-99; ternary :136-160, :188-210 (the two curls of
-// the reference are summed before the transform: F[a] + F[b] = F[a + b])
-// ---------------------------------------------------------------------------
-template <int N, class R, int GPC, int MODEL>
-__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const Par<R> P) {
-  constexpr int NT = N / 16;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int g = threadIdx.x / NT, t = threadIdx.x % NT;
-  cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
-  cx<R>* fbase = reinterpret_cast<cx<R>*>(smem_raw) + GPC * FftShape<N>::SMEM;
-  const int pair = blockIdx.x * GPC + g;
-  const bool live = pair < N / 2;
-  const int i0 = 2 * pair;
-  const int jt = P.jt;
-  cx<R> a[16], b[16];
-  if constexpr (MODEL == MODEL_BINARY) {
-    row_c2r<N>(a, B.g[GMU1], i0, jt, live, t, sh, P.tw);  // mu_t
-#pragma unroll
-    for (int d = 0; d < 2; d++) {
-      row_c2r<N>(b, B.g[d == 0 ? GDX1 : GDY1], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-      for (int m = 0; m < 16; m++) b[m] = mk<R>(rmul(b[m].x, a[m].x), rmul(b[m].y, a[m].y));
-      row_r2c_store<N>(b, B.h[d == 0 ? HFX : HFY], i0, live, t, sh, P.tw);
-    }
-  } else {
-    // weights w1 = (1+g3/g1) mu1 + (g3/g2) mu2, w2 = (g3/g1) mu1 + (1+g3/g2) mu2
-    Frag<N, R> w1{fbase + (size_t)(0 * GPC + g) * N};
-    Frag<N, R> w2{fbase + (size_t)(1 * GPC + g) * N};
-    row_c2r<N>(a, B.g[GMU1], i0, jt, live, t, sh, P.tw);
-    row_c2r<N>(b, B.g[GMU2], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-    for (int m = 0; m < 16; m++) {
-      w1[m] = mk<R>(radd(rmul(P.w11, a[m].x), rmul(P.w12, b[m].x)), radd(rmul(P.w11, a[m].y), rmul(P.w12, b[m].y)));
-      w2[m] = mk<R>(radd(rmul(P.w21, a[m].x), rmul(P.w22, b[m].x)), radd(rmul(P.w21, a[m].y), rmul(P.w22, b[m].y)));
-    }
-#pragma unroll
-    for (int d = 0; d < 2; d++) {
-      row_c2r<N>(a, B.g[d == 0 ? GDX1 : GDY1], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-      for (int m = 0; m < 16; m++) { const cx<R> s = w1[m]; a[m] = mk<R>(rmul(a[m].x, s.x), rmul(a[m].y, s.y)); }
-      row_c2r<N>(b, B.g[d == 0 ? GDX2 : GDY2], i0, jt, live, t, sh, P.tw);
-#pragma unroll
-      for (int m = 0; m < 16; m++) {
-        const cx<R> s = w2[m];
-        a[m] = mk<R>(radd(a[m].x, rmul(b[m].x, s.x)), radd(a[m].y, rmul(b[m].y, s.y)));
-      }
-      row_r2c_store<N>(a, B.h[d == 0 ? HFX : HFY], i0, live, t, sh, P.tw);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// helpers of the forward spectral passes
+// spectral-pass helpers
 // ---------------------------------------------------------------------------
 
 template <int N, class R>
@@ -397,6 +216,15 @@ __device__ __forceinline__ void load_row(cx<R>* v, const cx<R>* __restrict__ src
   constexpr int NT = N / 16;
 #pragma unroll
   for (int m = 0; m < 16; m++) v[m] = live ? src[(size_t)row * N + t + NT * m] : czero<R>();
+}
+
+// element e of a pair field's row: src[row][2 i + e]
+template <int N, class R>
+__device__ __forceinline__ void load_row_pair(cx<R>* v, const cx<R>* __restrict__ src, int row, int e, bool live,
+                                              int t) {
+  constexpr int NT = N / 16;
+#pragma unroll
+  for (int m = 0; m < 16; m++) v[m] = live ? src[(size_t)row * 2 * N + 2 * (t + NT * m) + e] : czero<R>();
 }
 
 template <int N, class R>
@@ -408,10 +236,330 @@ __device__ __forceinline__ void store_row(const cx<R>* v, cx<R>* __restrict__ ds
   }
 }
 
-template <int N, class R> __device__ __forceinline__ int amask(int t, int m) {
+template <int N, class R>
+__device__ __forceinline__ void store_row_pair(const cx<R>* v, cx<R>* __restrict__ dst, int row, int e, bool live,
+                                               int t) {
+  constexpr int NT = N / 16;
+  if (live) {
+#pragma unroll
+    for (int m = 0; m < 16; m++) dst[(size_t)row * 2 * N + 2 * (t + NT * m) + e] = v[m];
+  }
+}
+
+template <int N> __device__ __forceinline__ int amask(int t, int m) {
   const int ms = sidx<N>(t + (N / 16) * m);
   return ms < 0 ? -ms : ms;
 }
+
+// ---------------------------------------------------------------------------
+// P1: spectral fan-out + x inverse transform   (S -> G)
+// nonlin.c:30-48, velocity.c:12-42, surface_tension.c:20-22,57-75,
+// nonlin.c:177-198,259-284, chem_potential.c:256-261
+// ---------------------------------------------------------------------------
+template <int N, class R, int GPC, int MODEL>
+__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_inv(const Bufs<R> B, const Par<R> P) {
+  constexpr int NT = N / 16;
+  extern __shared__ __align__(16) unsigned char smem_all[];
+  const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
+  const int row = blockIdx.x * GPC + g;
+  const bool live = row <= P.jt;
+  const int mlim = live ? P.mrow[row] : -1;
+  const R ky = (R)(P.fy * (double)row);
+  const R sc = P.scale;
+
+  uint32_t inmask = 0;
+#pragma unroll
+  for (int m = 0; m < 16; m++)
+    if (amask<N>(t, m) <= mlim) inmask |= 1u << m;
+  auto kxm = [&](int m) -> R { return (R)(P.fx * (double)sidx<N>(t + NT * m)); };
+
+  cx<R> in[16], v[16];
+  // omega_hat
+#pragma unroll
+  for (int m = 0; m < 16; m++)
+    in[m] = ((inmask >> m) & 1) ? B.w[(size_t)row * N + t + NT * m] : czero<R>();
+  // u = I ky psi, v = -I kx psi, psi = w / k^2  (velocity.c:12-42)
+#pragma unroll
+  for (int d = 0; d < 2; d++) {
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const R kx = kxm(m), ks = ksq(kx, ky);
+      R a = (R)0, b = (R)0;
+      if (ks > (R)1e-12) { a = rdiv(in[m].x, ks); b = rdiv(in[m].y, ks); }
+      v[m] = d == 0 ? mk<R>(-rmul(ky, b) * sc, rmul(ky, a) * sc) : mk<R>(rmul(kx, b) * sc, -rmul(kx, a) * sc);
+    }
+    fft<N, +1>(v, sh, t, TW);
+    store_row_pair<N>(v, B.g[GUV], row, d, live, t);
+  }
+  // grad omega: I kx w, I ky w  (nonlin.c:36-37)
+#pragma unroll
+  for (int d = 0; d < 2; d++) {
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const R k = d == 0 ? kxm(m) : ky;
+      v[m] = mk<R>(-rmul(k, in[m].y) * sc, rmul(k, in[m].x) * sc);
+    }
+    fft<N, +1>(v, sh, t, TW);
+    store_row_pair<N>(v, B.g[GW], row, d, live, t);
+  }
+
+  if constexpr (MODEL >= MODEL_BINARY) {
+#pragma unroll
+    for (int f = 0; f < (MODEL == MODEL_TERNARY ? 2 : 1); f++) {
+      const cx<R>* src = f == 0 ? B.c1 : B.c2;
+#pragma unroll
+      for (int m = 0; m < 16; m++)
+        in[m] = ((inmask >> m) & 1) ? src[(size_t)row * N + t + NT * m] : czero<R>();
+      // truncated c (surface_tension.c:20-22, nonlin.c:217, chem_potential.c:256-261)
+#pragma unroll
+      for (int m = 0; m < 16; m++) v[m] = mk<R>(in[m].x * sc, in[m].y * sc);
+      fft<N, +1>(v, sh, t, TW);
+      if (MODEL == MODEL_BINARY) store_row<N>(v, B.g[GCT], row, live, t);
+      else store_row_pair<N>(v, B.g[GCT], row, f, live, t);
+      // grad c: I kx c, I ky c (surface_tension.c:57-58, nonlin.c:187-188, 272-273, 314-315)
+#pragma unroll
+      for (int d = 0; d < 2; d++) {
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+          const R k = d == 0 ? kxm(m) : ky;
+          v[m] = mk<R>(-rmul(k, in[m].y) * sc, rmul(k, in[m].x) * sc);
+        }
+        fft<N, +1>(v, sh, t, TW);
+        store_row_pair<N>(v, B.g[f == 0 ? GD1 : GD2], row, d, live, t);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// P2: advection products (+ bulk chemical potential) on x-row pairs (G -> H)
+// nonlin.c:56-74 (u.grad w), :201-215 (binary u.grad c), :286-300/328-348
+// (ternary u.grad c_i); surface_tension.c:24-35 / nonlin.c:217-230 (f(c));
+// chem_potential.c:263-320 (ternary mu^F)
+// ---------------------------------------------------------------------------
+
+// binary f(c) = c (1 - c)(1 - 2c)  (surface_tension.c:30-31, nonlin.c:225)
+template <class R> __device__ __forceinline__ R bulk_f(R a) {
+  return rmul(rmul(a, rsub((R)1, a)), rsub((R)1, rmul((R)2, a)));
+}
+
+// ternary mu^F_1, mu^F_2 at one point (chem_potential.c:269-315)
+template <class R> __device__ __forceinline__ void mu_ternary(const Par<R>& P, R c1, R c2, R& o1, R& o2) {
+  const R c3 = rsub(rsub((R)1, c1), c2);
+  const R c123 = rmul(rmul(c1, c2), c3);
+  const R fc1 = rmul(rmul(c1, rsub((R)1, c1)), rsub((R)1, rmul((R)2, c1)));
+  const R fc2 = rmul(rmul(c2, rsub((R)1, c2)), rsub((R)1, rmul((R)2, c2)));
+  const R fc3 = rmul(rmul(c3, rsub((R)1, c3)), rsub((R)1, rmul((R)2, c3)));
+  const R G1 = radd(rmul(P.g1, fc1), rmul(rmul(rmul(P.six_lam, c123), c2), c3));
+  const R G2 = radd(rmul(P.g2, fc2), rmul(rmul(rmul(P.six_lam, c123), c1), c3));
+  const R G3 = radd(rmul(P.g3, fc3), rmul(rmul(rmul(P.six_lam, c123), c1), c2));
+  const R m1 = radd(rmul(rsub(G1, G2), P.g2i), rmul(rsub(G1, G3), P.g3i));
+  const R m2 = radd(rmul(rsub(G2, G1), P.g1i), rmul(rsub(G2, G3), P.g3i));
+  o1 = rmul(m1, P.fac_mu);
+  o2 = rmul(m2, P.fac_mu);
+}
+
+// dot product of two pair-field transforms: f0 g0 + f1 g1 (e.g. ux*tux + uy*tuy)
+template <class R> __device__ __forceinline__ R dot2(cx<R> f, cx<R> g) { return radd(rmul(f.x, g.x), rmul(f.y, g.y)); }
+
+// The row kernels run a fixed schedule of inverse y transforms as a loop with
+// one call site per transform direction (the unrolled transforms are long, so
+// one copy of each keeps the kernel inside the instruction cache).  Step `it`
+// of the schedule reads src(it); the copy of src(it + 1) is in flight while
+// step it computes.
+
+// binary P2 schedule: 0 c_t (plain, x-rows i0, i1); then per x-row i:
+// 1 + 3h: (u, v); 2 + 3h: (dx w, dy w); 3 + 3h: (dx c, dy c)
+// ternary P2 schedule: 0, 1: (c1_t, c2_t) of x-rows i0, i1; then per x-row:
+// 2 + 4h: (u, v); 3 + 4h: (dx w, dy w); 4 + 4h: (dx c1, dy c1); 5 + 4h: (dx c2, dy c2)
+// pure Navier-Stokes P2 schedule: per x-row 2h: (u, v); 2h + 1: (dx w, dy w)
+template <int MODEL> struct AdvSchedule {
+  static constexpr int PRE = MODEL == MODEL_BINARY ? 1 : (MODEL == MODEL_TERNARY ? 2 : 0);
+  static constexpr int PER = MODEL == MODEL_TERNARY ? 4 : (MODEL == MODEL_BINARY ? 3 : 2);
+  static constexpr int STEPS = PRE + 2 * PER;
+};
+
+template <int N, class R, int MODEL>
+__device__ __forceinline__ RowSrc<R> adv_src(const Bufs<R>& B, int it, int i0) {
+  using Sc = AdvSchedule<MODEL>;
+  if (it < Sc::PRE) {
+    if (MODEL == MODEL_BINARY) return RowSrc<R>{B.g[GCT], N, i0};
+    return RowSrc<R>{B.g[GCT], 2 * N, 2 * (i0 + it)};
+  }
+  const int q = it - Sc::PRE, h = q / Sc::PER, r = q % Sc::PER;
+  const int slot = r == 0 ? GUV : (r == 1 ? GW : (r == 2 ? GD1 : GD2));
+  return RowSrc<R>{B.g[slot], 2 * N, 2 * (i0 + h)};
+}
+
+template <int N, class R, int GPC, int MODEL>
+__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par<R> P) {
+  using Sc = AdvSchedule<MODEL>;
+  constexpr int NT = N / 16;
+  extern __shared__ __align__(16) unsigned char smem_all[];
+  const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  const int jt = P.jt;
+  const RowSmem<N, R, GPC> S(smem_raw, g, jt);
+  const int pair = blockIdx.x * GPC + g;
+  const bool live = pair < N / 2;
+  const int i0 = 2 * pair;
+  Frag<N, R> keep{S.frag};
+  cx<R> z[16], v[16];
+  R a[16];
+
+  tile_issue<N>(S.tile, adv_src<N, R, MODEL>(B, 0, i0), jt, live, t);
+  cp_async_commit();
+#pragma unroll 1
+  for (int it = 0; it < Sc::STEPS; it++) {
+    const bool more = it + 1 < Sc::STEPS;
+    row_c2r_tiled<N>(v, S.tile, more, adv_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t, S.sh, TW);
+    cx<R>* dst = nullptr;
+    int stride = 0, off = 0;
+    if (it < Sc::PRE) {
+      if (MODEL == MODEL_BINARY) {
+        // f(c_t) of x-rows i0, i1 (surface_tension.c:30-31, nonlin.c:225)
+#pragma unroll
+        for (int m = 0; m < 16; m++) v[m] = mk<R>(bulk_f(v[m].x), bulk_f(v[m].y));
+        dst = B.h[HF]; stride = N; off = i0;
+      } else {
+        // mu^F_1, mu^F_2 of x-row i0 + it (chem_potential.c:263-320)
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+          R o1, o2;
+          mu_ternary(P, v[m].x, v[m].y, o1, o2);
+          v[m] = mk<R>(o1, o2);
+        }
+        dst = B.h[HF]; stride = 2 * N; off = 2 * (i0 + it);
+      }
+    } else {
+      const int q = it - Sc::PRE, h = q / Sc::PER, r = q % Sc::PER;
+      if (r == 0) {
+        // (u, v) of x-row i0 + h
+#pragma unroll
+        for (int m = 0; m < 16; m++) z[m] = v[m];
+      } else if (r == 1) {
+        // A = u dx w + v dy w (nonlin.c:62)
+#pragma unroll
+        for (int m = 0; m < 16; m++) a[m] = dot2(z[m], v[m]);
+        if (MODEL == MODEL_NS) {
+          if (h == 0) {
+#pragma unroll
+            for (int m = 0; m < 16; m++) keep[m] = a[m];
+          } else {
+#pragma unroll
+            for (int m = 0; m < 16; m++) v[m] = mk<R>(keep[m], a[m]);
+            dst = B.h[HAB]; stride = N; off = i0;
+          }
+        }
+      } else if (r == 2) {
+        // B1 = u dx c1 + v dy c1 (nonlin.c:207 / 292-293), stored with A
+#pragma unroll
+        for (int m = 0; m < 16; m++) v[m] = mk<R>(a[m], dot2(z[m], v[m]));
+        dst = B.h[HAB]; stride = 2 * N; off = 2 * (i0 + h);
+      } else {
+        // B2 = u dx c2 + v dy c2 (nonlin.c:334-335) of x-rows i0, i1, transformed together
+        if (h == 0) {
+#pragma unroll
+          for (int m = 0; m < 16; m++) keep[m] = dot2(z[m], v[m]);
+        } else {
+#pragma unroll
+          for (int m = 0; m < 16; m++) v[m] = mk<R>(keep[m], dot2(z[m], v[m]));
+          dst = B.h[HB2]; stride = N; off = i0;
+        }
+      }
+    }
+    if (dst) row_r2c_store<N>(v, dst, stride, off, live, t, S.sh, TW);  // CTA-uniform
+  }
+}
+
+template <int MODEL> constexpr int row_adv_frags() { return 1; }
+
+// ---------------------------------------------------------------------------
+// P4: surface-tension force mu grad c on x-row pairs (G -> H)
+// binary surface_tension.c:70-99; ternary :136-160, :188-210 (the two curls of
+// the reference are summed before the transform: F[a] + F[b] = F[a + b])
+// binary schedule: 0 mu_t (plain, x-rows i0, i1); 1 + h: (dx c, dy c) of x-row i0 + h
+// ternary schedule: per x-row 3h: (mu1, mu2); 3h + 1: grad c1; 3h + 2: grad c2
+// ---------------------------------------------------------------------------
+template <int N, class R, int MODEL>
+__device__ __forceinline__ RowSrc<R> force_src(const Bufs<R>& B, int it, int i0) {
+  if (MODEL == MODEL_BINARY) {
+    if (it == 0) return RowSrc<R>{B.g[GMU], N, i0};
+    return RowSrc<R>{B.g[GD1], 2 * N, 2 * (i0 + it - 1)};
+  }
+  const int h = it / 3, r = it % 3;
+  return RowSrc<R>{B.g[r == 0 ? GMU : (r == 1 ? GD1 : GD2)], 2 * N, 2 * (i0 + h)};
+}
+
+template <int N, class R, int GPC, int MODEL>
+__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const Par<R> P) {
+  constexpr int NT = N / 16;
+  constexpr int STEPS = MODEL == MODEL_BINARY ? 3 : 6;
+  extern __shared__ __align__(16) unsigned char smem_all[];
+  const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  const int jt = P.jt;
+  const RowSmem<N, R, GPC> S(smem_raw, g, jt);
+  const int pair = blockIdx.x * GPC + g;
+  const bool live = pair < N / 2;
+  const int i0 = 2 * pair;
+  Frag<N, R> w1{S.frag}, w2{S.frag + N * GPC};
+  cx<R> a[16], v[16];
+  tile_issue<N>(S.tile, force_src<N, R, MODEL>(B, 0, i0), jt, live, t);
+  cp_async_commit();
+#pragma unroll 1
+  for (int it = 0; it < STEPS; it++) {
+    const bool more = it + 1 < STEPS;
+    row_c2r_tiled<N>(v, S.tile, more, force_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t, S.sh,
+                     TW);
+    bool store = false;
+    int i = i0;
+    if (MODEL == MODEL_BINARY) {
+      if (it == 0) {
+#pragma unroll
+        for (int m = 0; m < 16; m++) a[m] = v[m];  // mu_t of x-rows i0, i1
+      } else {
+        // tux *= nphi, tuy *= nphi (surface_tension.c:87-88)
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+          const R mu = it == 1 ? a[m].x : a[m].y;
+          v[m] = mk<R>(rmul(v[m].x, mu), rmul(v[m].y, mu));
+        }
+        store = true;
+        i = i0 + it - 1;
+      }
+    } else {
+      const int h = it / 3, r = it % 3;
+      if (r == 0) {
+        // w1 = (1+g3/g1) mu1 + (g3/g2) mu2, w2 = (g3/g1) mu1 + (1+g3/g2) mu2 (surface_tension.c:148-149, 199-200)
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+          w1[m] = radd(rmul(P.w11, v[m].x), rmul(P.w12, v[m].y));
+          w2[m] = radd(rmul(P.w21, v[m].x), rmul(P.w22, v[m].y));
+        }
+      } else if (r == 1) {
+#pragma unroll
+        for (int m = 0; m < 16; m++) { const R s = w1[m]; a[m] = mk<R>(rmul(v[m].x, s), rmul(v[m].y, s)); }
+      } else {
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+          const R s = w2[m];
+          v[m] = mk<R>(radd(a[m].x, rmul(v[m].x, s)), radd(a[m].y, rmul(v[m].y, s)));
+        }
+        store = true;
+        i = i0 + h;
+      }
+    }
+    if (store) row_r2c_store<N>(v, B.h[HFF], 2 * N, 2 * i, live, t, S.sh, TW);  // CTA-uniform
+  }
+}
+
+template <int MODEL> constexpr int row_force_frags() { return MODEL == MODEL_TERNARY ? 2 : 0; }
 
 // ETD update of one mode (etd2rk.c:99,113,129-130 / 174,188,205-206).
 // STAGE 1: u <- u e + N z1, save N.  STAGE 2: u <- u + (N - saved) z2.
@@ -452,8 +600,10 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
   constexpr bool F32 = sizeof(R) == 4;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = blockIdx.x * GPC + g;
   const bool live = row < NR;
@@ -467,8 +617,8 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
 
   cx<R> f[16], c[16], v[16];
   // N_w partial = -F[u.grad w]   (nonlin.c:74, 92)
-  load_row<N>(v, B.h[HA], row, live, t);
-  fft<N, -1>(v, sh, t, P.tw);
+  load_row_pair<N>(v, B.h[HAB], row, 0, live, t);
+  fft<N, -1>(v, sh, t, TW);
 #pragma unroll
   for (int m = 0; m < 16; m++) v[m] = mk<R>(v[m].x * (R)(-1), v[m].y * (R)(-1));
   store_row<N>(v, B.nw, row, live, t);
@@ -478,15 +628,16 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
     cx<R>* cst = fld == 0 ? B.c1 : B.c2;
     cx<R>* csv = fld == 0 ? B.s1 : B.s2;
     // F[f(c)] (binary) or F[mu^F_i] (ternary)
-    load_row<N>(f, B.h[fld == 0 ? HF1 : HF2], row, live, t);
-    fft<N, -1>(f, sh, t, P.tw);
+    if (MODEL == MODEL_BINARY) load_row<N>(f, B.h[HF], row, live, t);
+    else load_row_pair<N>(f, B.h[HF], row, fld, live, t);
+    fft<N, -1>(f, sh, t, TW);
     load_row<N>(c, cst, row, live, t);
     if (do_mu) {
       // binary: mu = T[1.5 sigma eps k^2 c + 24 (sigma/eps) F[f]]   (surface_tension.c:45-46)
       // ternary: mu_i = T[F[mu^F_i] + 0.75 gamma_i eps k^2 c_i]     (surface_tension.c:116-128)
 #pragma unroll
       for (int m = 0; m < 16; m++) {
-        if (amask<N, R>(t, m) <= mlim) {
+        if (amask<N>(t, m) <= mlim) {
           const R ks = ksq(kxm(m), ky);
           if (MODEL == MODEL_BINARY) {
             const R q = rmul(P.st15, ks);
@@ -500,16 +651,20 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
           v[m] = czero<R>();
         }
       }
-      fft<N, +1>(v, sh, t, P.tw);
-      if (row <= P.jt) store_row<N>(v, B.g[fld == 0 ? GMU1 : GMU2], row, live, t);
+      fft<N, +1>(v, sh, t, TW);
+      if (row <= P.jt) {
+        if (MODEL == MODEL_BINARY) store_row<N>(v, B.g[GMU], row, live, t);
+        else store_row_pair<N>(v, B.g[GMU], row, fld, live, t);
+      }
     }
     // N_c  binary: -F[u.grad c] - lambda (24 (sigma/eps) k^2) F[f]   (nonlin.c:240, 251)
     //      ternary: -F[u.grad c_i] - (lambda/gamma_i) k^2 F[mu^F_i]  (nonlin.c:369-370)
-    load_row<N>(v, B.h[fld == 0 ? HB1 : HB2], row, live, t);
-    fft<N, -1>(v, sh, t, P.tw);
+    if (fld == 0) load_row_pair<N>(v, B.h[HAB], row, 1, live, t);
+    else load_row<N>(v, B.h[HB2], row, live, t);
+    fft<N, -1>(v, sh, t, TW);
 #pragma unroll
     for (int m = 0; m < 16; m++) {
-      const int am = amask<N, R>(t, m);
+      const int am = amask<N>(t, m);
       const R ks = ksq(kxm(m), ky);
       cx<R> nl;
       if (MODEL == MODEL_BINARY) {
@@ -537,18 +692,20 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
 }
 
 // ---------------------------------------------------------------------------
-// P5 (phase-field models): x forward transforms of the force, curl, N_w and
-// the ETD update of w (H -> S)   surface_tension.c:98-111 / 159-173 / 209-223,
-// curl.c:16-31, etd2rk.c:88-99 / 162-174
-// P3 for pure Navier-Stokes: NACC = 0 (N_w = -F[u.grad w] only)
+// P5: x forward transforms of the force, curl, N_w and the ETD update of w
+// (H -> S)   surface_tension.c:98-111 / 159-173 / 209-223, curl.c:16-31,
+// etd2rk.c:88-99 / 162-174.  Pure Navier-Stokes (CURL = false):
+// N_w = -F[u.grad w] (nonlin.c:74-101) from the plain field in HAB.
 // ---------------------------------------------------------------------------
 template <int N, class R, int GPC, bool CURL, int STAGE>
 __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
   constexpr bool F32 = sizeof(R) == 4;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = blockIdx.x * GPC + g;
   const bool live = row < NR;
@@ -560,10 +717,10 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
 
   cx<R> a[16], b[16];
   if constexpr (CURL) {
-    load_row<N>(a, B.h[HFX], row, live, t);
-    fft<N, -1>(a, sh, t, P.tw);
-    load_row<N>(b, B.h[HFY], row, live, t);
-    fft<N, -1>(b, sh, t, P.tw);
+    load_row_pair<N>(a, B.h[HFF], row, 0, live, t);
+    fft<N, -1>(a, sh, t, TW);
+    load_row_pair<N>(b, B.h[HFF], row, 1, live, t);
+    fft<N, -1>(b, sh, t, TW);
     // N_w = N_w partial + I (kx F[Fy] - ky F[Fx])
 #pragma unroll
     for (int m = 0; m < 16; m++) {
@@ -574,9 +731,8 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
       a[m] = mk<R>(radd(p.x, -di), radd(p.y, dr));
     }
   } else {
-    // pure Navier-Stokes: N_w = -F[u.grad w]
-    load_row<N>(a, B.h[HA], row, live, t);
-    fft<N, -1>(a, sh, t, P.tw);
+    load_row<N>(a, B.h[HAB], row, live, t);
+    fft<N, -1>(a, sh, t, TW);
 #pragma unroll
     for (int m = 0; m < 16; m++) a[m] = mk<R>(a[m].x * (R)(-1), a[m].y * (R)(-1));
   }
@@ -584,7 +740,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
   load_row<N>(b, B.w, row, live, t);
 #pragma unroll
   for (int m = 0; m < 16; m++) {
-    const int am = amask<N, R>(t, m);
+    const int am = amask<N>(t, m);
     const size_t idx = (size_t)rowc * N + t + NT * m;
     const R e = cf[0 * cstride + am], z1 = cf[1 * cstride + am], z2 = cf[2 * cstride + am];
     cx<R> sv;
@@ -642,13 +798,15 @@ __global__ void k_s_to_fftw(const cx<R>* __restrict__ src, double2* __restrict__
   }
 }
 
-// real field (n x n, R, row-major, i = x) -> H layout: y-r2c of x-row pairs
+// real field (n x n, R, row-major, i = x) -> H layout (plain): y-r2c of x-row pairs
 template <int N, class R, int GPC>
 __global__ void __launch_bounds__(GPC * (N / 16)) k_row_r2c_plain(const R* __restrict__ x, cx<R>* __restrict__ H,
                                                                   const cx<R>* __restrict__ tw) {
   constexpr int NT = N / 16;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), tw, t);
+  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int pair = blockIdx.x * GPC + g;
   const bool live = pair < N / 2;
@@ -659,16 +817,18 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_row_r2c_plain(const R* __res
     const int y = t + NT * m;
     v[m] = live ? mk<R>(x[(size_t)i0 * N + y], x[(size_t)(i0 + 1) * N + y]) : czero<R>();
   }
-  row_r2c_store<N>(v, H, i0, live, t, sh, tw);
+  row_r2c_store<N>(v, H, N, i0, live, t, sh, TW);
 }
 
-// S/H layout row j': x transform in place (DIR), optional scale
+// S/H layout row j': x transform (DIR), optional scale
 template <int N, class R, int GPC, int DIR>
 __global__ void __launch_bounds__(GPC * (N / 16)) k_col_plain(const cx<R>* __restrict__ src, cx<R>* __restrict__ dst,
                                                               int nrows, R scale, const cx<R>* __restrict__ tw) {
   constexpr int NT = N / 16;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), tw, t);
+  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = blockIdx.x * GPC + g;
   const bool live = row < nrows;
@@ -676,23 +836,28 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_col_plain(const cx<R>* __res
   load_row<N>(v, src, row, live, t);
 #pragma unroll
   for (int m = 0; m < 16; m++) v[m] = mk<R>(v[m].x * scale, v[m].y * scale);
-  fft<N, DIR>(v, sh, t, tw);
+  fft<N, DIR>(v, sh, t, TW);
   store_row<N>(v, dst, row, live, t);
 }
 
-// G layout (all n/2+1 rows) -> real field: y-c2r of x-row pairs
+// plain layout (rows 0..n/2) -> real field: y-c2r of x-row pairs
 template <int N, class R, int GPC>
 __global__ void __launch_bounds__(GPC * (N / 16)) k_row_c2r_plain(const cx<R>* __restrict__ G, R* __restrict__ x,
-                                                                  int jt, const cx<R>* __restrict__ tw) {
+                                                                  const cx<R>* __restrict__ tw) {
   constexpr int NT = N / 16;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int JT = N / 2;
+  extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
-  cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
+  const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), tw, t);
+  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  const RowSmem<N, R, GPC> S(smem_raw, g, JT);
   const int pair = blockIdx.x * GPC + g;
   const bool live = pair < N / 2;
   const int i0 = 2 * pair;
   cx<R> v[16];
-  row_c2r<N>(v, G, i0, jt, live, t, sh, tw);
+  tile_issue<N>(S.tile, RowSrc<R>{G, N, i0}, JT, live, t);
+  cp_async_commit();
+  row_c2r_tiled<N>(v, S.tile, false, RowSrc<R>{nullptr, 0, 0}, JT, live, t, S.sh, TW);
   if (live) {
 #pragma unroll
     for (int m = 0; m < 16; m++) {

@@ -81,7 +81,8 @@ template <int N, class R> struct Sizes {
   static constexpr int GPC = gpc_of<N>();
   static constexpr int NT = N / 16;
   static constexpr int THREADS = GPC * NT;
-  static constexpr size_t FFT_SMEM = (size_t)GPC * FftShape<N>::SMEM * sizeof(cx<R>);
+  static constexpr size_t TW = tw_smem_per_thread<N, R>() * THREADS;  // precomputed twiddles
+  static constexpr size_t FFT_SMEM = TW + (size_t)GPC * FftShape<N>::SMEM * sizeof(cx<R>);
   static constexpr size_t FRAG = (size_t)GPC * N * sizeof(cx<R>);
   static int grid_rows(int rows) { return (rows + GPC - 1) / GPC; }
 };
@@ -93,12 +94,13 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   const Bufs<R> B = make_bufs<R>(c);
   cudaStream_t st = c->stream;
   const int model = c->p.model;
-  const int rows_inv = S::grid_rows(c->jt + 1);
+  const int jt = c->jt;
+  const int rows_inv = S::grid_rows(jt + 1);
   const int rows_all = S::grid_rows(N / 2 + 1);
   const int pairs = S::grid_rows(N / 2);
   int launches = 0;
 
-  // P1
+  // P1: spectral fan-out and x inverse transforms
   if (model == CHNS_MODEL_NS) {
     auto k = k_spec_inv<N, R, GPC, MODEL_NS>;
     set_smem(k, S::FFT_SMEM);
@@ -115,59 +117,28 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   launches++;
   mark(c, KIND_SPEC_INV);
 
-  // P2
+  // P2: advection products (+ chemical potential)
   if (model == CHNS_MODEL_NS) {
-    AdvIO<R> io{};
-    io.dx[0] = B.g[GDXW];
-    io.dy[0] = B.g[GDYW];
-    io.out[0] = B.h[HA];
-    auto k = k_row_adv<N, R, GPC, 1, 0>;
-    const size_t sm = S::FFT_SMEM + 1 * S::FRAG;
+    auto k = k_row_adv<N, R, GPC, MODEL_NS>;
+    const size_t sm = S::TW + RowSmem<N, R, GPC>::bytes(jt, row_adv_frags<MODEL_NS>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P, io);
-    launches++;
-    mark(c, KIND_ROW_ADV);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P);
   } else if (model == CHNS_MODEL_BINARY) {
-    AdvIO<R> io{};
-    io.dx[0] = B.g[GDXW];
-    io.dy[0] = B.g[GDYW];
-    io.out[0] = B.h[HA];
-    io.dx[1] = B.g[GDX1];
-    io.dy[1] = B.g[GDY1];
-    io.out[1] = B.h[HB1];
-    auto k = k_row_adv<N, R, GPC, 2, 1>;
-    const size_t sm = S::FFT_SMEM + 2 * S::FRAG;
+    auto k = k_row_adv<N, R, GPC, MODEL_BINARY>;
+    const size_t sm = S::TW + RowSmem<N, R, GPC>::bytes(jt, row_adv_frags<MODEL_BINARY>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P, io);
-    launches++;
-    mark(c, KIND_ROW_ADV);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P);
   } else {
-    AdvIO<R> io{};
-    io.dx[0] = B.g[GDXW];
-    io.dy[0] = B.g[GDYW];
-    io.out[0] = B.h[HA];
-    auto k = k_row_adv<N, R, GPC, 1, 2>;
-    const size_t sm = S::FFT_SMEM + 1 * S::FRAG;
+    auto k = k_row_adv<N, R, GPC, MODEL_TERNARY>;
+    const size_t sm = S::TW + RowSmem<N, R, GPC>::bytes(jt, row_adv_frags<MODEL_TERNARY>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P, io);
-    mark(c, KIND_ROW_ADV);
-    AdvIO<R> io2{};
-    io2.dx[0] = B.g[GDX1];
-    io2.dy[0] = B.g[GDY1];
-    io2.out[0] = B.h[HB1];
-    io2.dx[1] = B.g[GDX2];
-    io2.dy[1] = B.g[GDY2];
-    io2.out[1] = B.h[HB2];
-    auto k2 = k_row_adv<N, R, GPC, 2, 0>;
-    const size_t sm2 = S::FFT_SMEM + 2 * S::FRAG;
-    set_smem(k2, sm2);
-    k2<<<pairs, S::THREADS, sm2, st>>>(B, P, io2);
-    mark(c, KIND_ROW_ADV_B);
-    launches += 2;
+    k<<<pairs, S::THREADS, sm, st>>>(B, P);
   }
+  launches++;
+  mark(c, KIND_ROW_ADV);
 
   if (model == CHNS_MODEL_NS) {
-    // P3 of pure Navier-Stokes: N_w = -F[u.grad w], ETD of w
+    // pure Navier-Stokes: N_w = -F[u.grad w], ETD of w
     if (stage == 1) {
       auto k = k_spec_curl_w<N, R, GPC, false, 1>;
       set_smem(k, S::FFT_SMEM);
@@ -181,7 +152,7 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
     return launches + 1;
   }
 
-  // P3
+  // P3: x forward transforms, mu, N_c, ETD of c
   if (model == CHNS_MODEL_BINARY) {
     if (stage == 1) {
       auto k = k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1>;
@@ -206,21 +177,22 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   launches++;
   mark(c, KIND_SPEC_FWD_C);
 
-  // P4
+  // P4: surface-tension force
   if (model == CHNS_MODEL_BINARY) {
     auto k = k_row_force<N, R, GPC, MODEL_BINARY>;
-    set_smem(k, S::FFT_SMEM);
-    k<<<pairs, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    const size_t sm = S::TW + RowSmem<N, R, GPC>::bytes(jt, row_force_frags<MODEL_BINARY>());
+    set_smem(k, sm);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P);
   } else {
     auto k = k_row_force<N, R, GPC, MODEL_TERNARY>;
-    const size_t sm = S::FFT_SMEM + 2 * S::FRAG;
+    const size_t sm = S::TW + RowSmem<N, R, GPC>::bytes(jt, row_force_frags<MODEL_TERNARY>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P);
   }
   launches++;
   mark(c, KIND_ROW_FORCE);
 
-  // P5
+  // P5: curl, N_w, ETD of w
   if (stage == 1) {
     auto k = k_spec_curl_w<N, R, GPC, true, 1>;
     set_smem(k, S::FFT_SMEM);
@@ -254,12 +226,12 @@ template <int N, class R> int dfft_impl(chns_ctx* c, const void* real, void* s) 
   using S = Sizes<N, R>;
   auto k1 = k_row_r2c_plain<N, R, S::GPC>;
   set_smem(k1, S::FFT_SMEM);
-  k1<<<S::grid_rows(N / 2), S::THREADS, S::FFT_SMEM, c->stream>>>((const R*)real, (cx<R>*)c->h[HA],
+  k1<<<S::grid_rows(N / 2), S::THREADS, S::FFT_SMEM, c->stream>>>((const R*)real, (cx<R>*)c->h[HAB],
                                                                    (const cx<R>*)c->tw);
   auto k2 = k_col_plain<N, R, S::GPC, -1>;
   set_smem(k2, S::FFT_SMEM);
   k2<<<S::grid_rows(N / 2 + 1), S::THREADS, S::FFT_SMEM, c->stream>>>(
-      (const cx<R>*)c->h[HA], (cx<R>*)s, N / 2 + 1, (R)1, (const cx<R>*)c->tw);
+      (const cx<R>*)c->h[HAB], (cx<R>*)s, N / 2 + 1, (R)1, (const cx<R>*)c->tw);
   return 2;
 }
 
@@ -268,11 +240,11 @@ template <int N, class R> int ifft_impl(chns_ctx* c, const void* s, void* real) 
   auto k1 = k_col_plain<N, R, S::GPC, +1>;
   set_smem(k1, S::FFT_SMEM);
   k1<<<S::grid_rows(N / 2 + 1), S::THREADS, S::FFT_SMEM, c->stream>>>(
-      (const cx<R>*)s, (cx<R>*)c->h[HB1], N / 2 + 1, (R)(1.0 / ((double)N * (double)N)), (const cx<R>*)c->tw);
+      (const cx<R>*)s, (cx<R>*)c->h[HF], N / 2 + 1, (R)(1.0 / ((double)N * (double)N)), (const cx<R>*)c->tw);
   auto k2 = k_row_c2r_plain<N, R, S::GPC>;
-  set_smem(k2, S::FFT_SMEM);
-  k2<<<S::grid_rows(N / 2), S::THREADS, S::FFT_SMEM, c->stream>>>((const cx<R>*)c->h[HB1], (R*)real, N / 2,
-                                                                   (const cx<R>*)c->tw);
+  const size_t sm2 = S::TW + RowSmem<N, R, S::GPC>::bytes(N / 2, 0);
+  set_smem(k2, sm2);
+  k2<<<S::grid_rows(N / 2), S::THREADS, sm2, c->stream>>>((const cx<R>*)c->h[HF], (R*)real, (const cx<R>*)c->tw);
   return 2;
 }
 
@@ -292,7 +264,7 @@ template <int N, class R> int diag_impl(chns_ctx* c) {
   using S = Sizes<N, R>;
   const Par<R> P = make_par<R>(c);
   const Bufs<R> B = make_bufs<R>(c);
-  const size_t rsm = (size_t)NRED * S::THREADS * sizeof(double);
+  const size_t rsm = S::TW + (size_t)NRED * S::THREADS * sizeof(double);
   const size_t sm = S::FFT_SMEM > rsm ? S::FFT_SMEM : rsm;
   const int model = c->p.model;
   const int rows = S::grid_rows(N / 2 + 1);

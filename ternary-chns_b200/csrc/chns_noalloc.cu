@@ -87,7 +87,8 @@ template <int N> int run(const double* real, double* spec, const DeviceSetup* s,
   using chns::cxd;
   constexpr int GPC = gpc<N>();
   constexpr int THREADS = GPC * (N / 16);
-  constexpr size_t SMEM = (size_t)GPC * chns::FftShape<N>::SMEM * sizeof(cxd);
+  constexpr size_t SMEM = chns::tw_smem_per_thread<N, double>() * THREADS +
+                          (size_t)GPC * chns::FftShape<N>::SMEM * sizeof(cxd);
   cxd* h = s->scratch;           // after the y transforms (H layout)
   cxd* sl = s->scratch + kField;  // after the x transforms (S layout)
   const cxd* tw = s->tw + tw_offset(N);
