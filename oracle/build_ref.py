@@ -65,7 +65,7 @@ CONFIGS = {
     "ter512": dict(_TER, n=512, dt="(5e-5)"),
     # binary 4096^2 with the 4096^2 configuration's parameters (the reference has
     # no working forcing, so this is the unforced step; same cost per step)
-    "bin4096": dict(model=1, n=4096, lx="(2.0*pi)", dt="(2e-4)", nu="(1e-3)", lam="(1e-3)",
+    "bin4096": dict(model=1, n=4096, lx="(2.0*pi)", dt="(2e-6)", nu="(1e-3)", lam="(1e-3)",
                     sigma="(0.1)", eps="(2.0*dx)"),
 }
 

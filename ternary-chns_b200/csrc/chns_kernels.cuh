@@ -277,59 +277,49 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_inv(const Bufs<R> B, const Pa
   auto kxm = [&](int m) -> R { return (R)(P.fx * (double)sidx<N>(t + NT * m)); };
 
   cx<R> in[16], v[16];
-  // omega_hat
-#pragma unroll
-  for (int m = 0; m < 16; m++)
-    in[m] = ((inmask >> m) & 1) ? B.w[(size_t)row * N + t + NT * m] : czero<R>();
-  // u = I ky psi, v = -I kx psi, psi = w / k^2  (velocity.c:12-42)
-#pragma unroll
-  for (int d = 0; d < 2; d++) {
-#pragma unroll
-    for (int m = 0; m < 16; m++) {
-      const R kx = kxm(m), ks = ksq(kx, ky);
-      R a = (R)0, b = (R)0;
-      if (ks > (R)1e-12) { a = rdiv(in[m].x, ks); b = rdiv(in[m].y, ks); }
-      v[m] = d == 0 ? mk<R>(-rmul(ky, b) * sc, rmul(ky, a) * sc) : mk<R>(rmul(kx, b) * sc, -rmul(kx, a) * sc);
-    }
-    fft<N, +1>(v, sh, t, TW);
-    store_row_pair<N>(v, B.g[GUV], row, d, live, t);
-  }
-  // grad omega: I kx w, I ky w  (nonlin.c:36-37)
-#pragma unroll
-  for (int d = 0; d < 2; d++) {
-#pragma unroll
-    for (int m = 0; m < 16; m++) {
-      const R k = d == 0 ? kxm(m) : ky;
-      v[m] = mk<R>(-rmul(k, in[m].y) * sc, rmul(k, in[m].x) * sc);
-    }
-    fft<N, +1>(v, sh, t, TW);
-    store_row_pair<N>(v, B.g[GW], row, d, live, t);
-  }
-
-  if constexpr (MODEL >= MODEL_BINARY) {
-#pragma unroll
-    for (int f = 0; f < (MODEL == MODEL_TERNARY ? 2 : 1); f++) {
-      const cx<R>* src = f == 0 ? B.c1 : B.c2;
+  // outputs: 0 u, 1 v (velocity.c:12-42), 2 dx w, 3 dy w (nonlin.c:36-37); then per
+  // phase field: c_t (surface_tension.c:20-22, nonlin.c:217, chem_potential.c:256-261),
+  // dx c, dy c (surface_tension.c:57-58, nonlin.c:187-188, 272-273, 314-315).
+  // One loop with one inverse transform keeps the kernel small.
+  constexpr int NOUT = MODEL == MODEL_NS ? 4 : (MODEL == MODEL_BINARY ? 7 : 10);
+#pragma unroll 1
+  for (int o = 0; o < NOUT; o++) {
+    if (o == 0 || o == 4 || o == 7) {
+      const cx<R>* src = o == 0 ? B.w : (o == 4 ? B.c1 : B.c2);
 #pragma unroll
       for (int m = 0; m < 16; m++)
         in[m] = ((inmask >> m) & 1) ? src[(size_t)row * N + t + NT * m] : czero<R>();
-      // truncated c (surface_tension.c:20-22, nonlin.c:217, chem_potential.c:256-261)
+    }
+    const int q = o < 4 ? o : 4 + (o - 4) % 3;  // 0 u, 1 v, 2 dx, 3 dy (w); 4 c_t, 5 dx, 6 dy (c)
+    if (q < 2) {
+      // u = I ky psi, v = -I kx psi, psi = w / k^2
+#pragma unroll
+      for (int m = 0; m < 16; m++) {
+        const R kx = kxm(m), ks = ksq(kx, ky);
+        R a = (R)0, b = (R)0;
+        if (ks > (R)1e-12) { a = rdiv(in[m].x, ks); b = rdiv(in[m].y, ks); }
+        v[m] = q == 0 ? mk<R>(-rmul(ky, b) * sc, rmul(ky, a) * sc) : mk<R>(rmul(kx, b) * sc, -rmul(kx, a) * sc);
+      }
+    } else if (q == 4) {
 #pragma unroll
       for (int m = 0; m < 16; m++) v[m] = mk<R>(in[m].x * sc, in[m].y * sc);
-      fft<N, +1>(v, sh, t, TW);
-      if (MODEL == MODEL_BINARY) store_row<N>(v, B.g[GCT], row, live, t);
-      else store_row_pair<N>(v, B.g[GCT], row, f, live, t);
-      // grad c: I kx c, I ky c (surface_tension.c:57-58, nonlin.c:187-188, 272-273, 314-315)
+    } else {
+      // I kx f, I ky f
+      const bool dx = q == 2 || q == 5;
 #pragma unroll
-      for (int d = 0; d < 2; d++) {
-#pragma unroll
-        for (int m = 0; m < 16; m++) {
-          const R k = d == 0 ? kxm(m) : ky;
-          v[m] = mk<R>(-rmul(k, in[m].y) * sc, rmul(k, in[m].x) * sc);
-        }
-        fft<N, +1>(v, sh, t, TW);
-        store_row_pair<N>(v, B.g[f == 0 ? GD1 : GD2], row, d, live, t);
+      for (int m = 0; m < 16; m++) {
+        const R k = dx ? kxm(m) : ky;
+        v[m] = mk<R>(-rmul(k, in[m].y) * sc, rmul(k, in[m].x) * sc);
       }
+    }
+    fft<N, +1>(v, sh, t, TW);
+    if (q < 2) store_row_pair<N>(v, B.g[GUV], row, q, live, t);
+    else if (q < 4) store_row_pair<N>(v, B.g[GW], row, q - 2, live, t);
+    else if (q == 4) {
+      if (MODEL == MODEL_BINARY) store_row<N>(v, B.g[GCT], row, live, t);
+      else store_row_pair<N>(v, B.g[GCT], row, o < 7 ? 0 : 1, live, t);
+    } else {
+      store_row_pair<N>(v, B.g[o < 7 ? GD1 : GD2], row, q - 5, live, t);
     }
   }
 }
