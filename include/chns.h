@@ -110,6 +110,19 @@ int chns_ifft(chns_ctx *ctx, const double *spec, double *real, int where);
  * phase-1 mean, phase-2 mean}. */
 int chns_diagnostics(chns_ctx *ctx, double *out_fe, double *out_ke);
 
+/* Discrete adjoint of `nsteps` ETD2RK steps of the binary model (etd2rk.c with
+ * nonlin.c / surface_tension.c transposed operation by operation) from the
+ * current state.  Loss at the final state, with c and grad c untruncated as in
+ * free_energy.c:3-157:
+ *   J = w[0] E_bulk + w[1] E_grad + w[2] <|grad phi|^2>,  phi = 2c - 1
+ * (loss_w = NULL: all weights 1).  Outputs: *J; dJ/d(omega_hat_0), dJ/d(c_hat_0)
+ * in FFTW layout (gradients with respect to the stored real and imaginary
+ * parts; g_w / g_c may be NULL); g_params[3] = dJ/d(nu, lambda, sigma).  The
+ * state is kept every `ckpt` steps and recomputed in between.  The state is
+ * unchanged on return.  Other models return CHNS_ERR_UNSUPPORTED. */
+int chns_adjoint(chns_ctx *ctx, int nsteps, int ckpt, const double *loss_w, double *J, double *g_w,
+                 double *g_c, double *g_params, int where);
+
 /* Kernel launches of one step (known after the first chns_step). */
 int chns_launches_per_step(const chns_ctx *ctx);
 

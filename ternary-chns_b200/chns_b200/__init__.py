@@ -75,6 +75,8 @@ def load_library(path: str = LIB_PATH):
     L.chns_launches_per_step.argtypes = [vp]
     L.chns_profile_step.argtypes = [vp, ip, vp, vp, ip]
     L.chns_profile_step.restype = ip
+    L.chns_adjoint.argtypes = [vp, ip, ip, vp, vp, vp, vp, vp, ip]
+    L.chns_adjoint.restype = ip
     L.chns_dfft_noalloc.argtypes = [vp, vp, ip, vp]
     L.chns_dfft_noalloc.restype = ip
     L.chns_status_string.restype = ctypes.c_char_p
@@ -219,6 +221,20 @@ class Context:
         if rc not in (0, -3):
             _check(rc, "chns_diagnostics")
         return fe, ke, rc
+
+    def adjoint(self, nsteps: int, ckpt: int = 20, loss_w=(1.0, 1.0, 1.0)):
+        """Discrete adjoint of `nsteps` binary ETD2RK steps from the current state.
+        Returns (J, dJ/d omega_hat_0, dJ/d c_hat_0, dJ/d(nu, lambda, sigma)); the
+        state is unchanged.  J = w0 E_bulk + w1 E_grad + w2 <|grad phi|^2> at the
+        final state (phi = 2c - 1)."""
+        lw = np.ascontiguousarray(loss_w, np.float64)
+        J = np.zeros(1)
+        gw = np.empty(self.shape, np.complex128)
+        gc = np.empty(self.shape, np.complex128)
+        gp = np.zeros(3)
+        _check(self.L.chns_adjoint(self._h, int(nsteps), int(ckpt), _ptr(lw), _ptr(J), _ptr(gw), _ptr(gc),
+                                   _ptr(gp), HOST), "chns_adjoint")
+        return float(J[0]), gw, gc, gp
 
     def launches_per_step(self) -> int:
         return self.L.chns_launches_per_step(self._h)

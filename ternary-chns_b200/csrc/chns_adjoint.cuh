@@ -1,0 +1,363 @@
+// chns_adjoint.cuh -- kernels of the discrete adjoint of the binary ETD2RK step.
+//
+// The adjoint is the exact transpose (over the stored real and imaginary parts of
+// the half spectra) of the forward step of nonlin.c / surface_tension.c /
+// etd2rk.c.  Its building blocks, with X a half spectrum (n x (n/2+1) stored
+// modes) and x a real n x n field:
+//   ifft (fft.c:16-31)  : x = C(X)              ->  C^T(x_bar) = (w_j / n^2) dfft(x_bar)
+//   dfft (fft.c:11-14)  : X = F(x)              ->  F^T(X_bar) = n^2 ifft(X_bar / w_j)
+// where w_j = 2 for 0 < ky index j < n/2 and 1 for j = 0, n/2 (the Hermitian
+// extension counts the interior columns twice); a complex multiplier a becomes
+// conj(a), a real multiplier and the truncation mask are their own transposes.
+// Spectral fields here are in the S layout (row j', column i; see chns_kernels.cuh),
+// real fields are n x n row-major.
+#pragma once
+
+#include "chns_kernels.cuh"
+
+namespace chns {
+
+// scalars of one adjoint evaluation
+template <class R> struct AdjPar {
+  int n, jt;
+  double fx, fy;
+  R s1, s2, lam;        // 1.5 sigma eps, 24 sigma / eps, lambda
+  double ds1, ds2;      // d s1 / d sigma = 1.5 eps, d s2 / d sigma = 24 / eps
+  const int* mrow;
+};
+
+template <class R> struct ModeIdx {
+  int row, i, am;
+  R kx, ky, ks;
+  bool in;    // inside the truncation disc
+  R wj;       // Hermitian weight of the column ky = row
+};
+
+template <class R>
+__device__ __forceinline__ bool mode_of(const AdjPar<R>& P, size_t idx, ModeIdx<R>& m) {
+  const int n = P.n;
+  const size_t total = (size_t)(n / 2 + 1) * n;
+  if (idx >= total) return false;
+  m.row = (int)(idx / n);
+  m.i = (int)(idx % n);
+  const int ms = m.i <= n / 2 ? m.i : m.i - n;
+  m.am = ms < 0 ? -ms : ms;
+  m.kx = (R)(P.fx * (double)ms);
+  m.ky = (R)(P.fy * (double)m.row);
+  m.ks = radd(rmul(m.kx, m.kx), rmul(m.ky, m.ky));
+  m.in = m.row <= P.jt && m.am <= P.mrow[m.row];
+  m.wj = (m.row == 0 || m.row == n / 2) ? (R)1 : (R)2;
+  return true;
+}
+
+template <class R> __device__ __forceinline__ cx<R> cscale(cx<R> a, R s) { return mk<R>(a.x * s, a.y * s); }
+// a * (i k)  and  a * conj(i k) = a * (-i k)
+template <class R> __device__ __forceinline__ cx<R> mul_ik(cx<R> a, R k) { return mk<R>(-(k * a.y), k * a.x); }
+template <class R> __device__ __forceinline__ cx<R> mul_mik(cx<R> a, R k) { return mk<R>(k * a.y, -(k * a.x)); }
+template <class R> __device__ __forceinline__ double rdot(cx<R> a, cx<R> b) {
+  return (double)a.x * (double)b.x + (double)a.y * (double)b.y;
+}
+
+// block sum of up to 3 doubles, added atomically to acc[0..2]
+__device__ __forceinline__ void block_acc3(double a0, double a1, double a2, double* acc) {
+  __shared__ double red[3][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, o);
+    a1 += __shfl_down_sync(0xffffffffu, a1, o);
+    a2 += __shfl_down_sync(0xffffffffu, a2, o);
+  }
+  if (lane == 0) { red[0][wid] = a0; red[1][wid] = a1; red[2][wid] = a2; }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    a0 = lane < nw ? red[0][lane] : 0.0;
+    a1 = lane < nw ? red[1][lane] : 0.0;
+    a2 = lane < nw ? red[2][lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a0 += __shfl_down_sync(0xffffffffu, a0, o);
+      a1 += __shfl_down_sync(0xffffffffu, a1, o);
+      a2 += __shfl_down_sync(0xffffffffu, a2, o);
+    }
+    if (lane == 0) {
+      if (a0 != 0.0) atomicAdd(acc + 0, a0);
+      if (a1 != 0.0) atomicAdd(acc + 1, a1);
+      if (a2 != 0.0) atomicAdd(acc + 2, a2);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// forward fields of the right-hand side at a state (nonlin.c:30-48, 177-198,
+// surface_tension.c:20-75): op selects the truncated spectrum to transform
+// ---------------------------------------------------------------------------
+enum { FOP_U = 0, FOP_V, FOP_WX, FOP_WY, FOP_CT, FOP_CX, FOP_CY, FOP_MU };
+
+template <class R>
+__global__ void k_adj_fwd_prep(int op, const AdjPar<R> P, const cx<R>* __restrict__ w, const cx<R>* __restrict__ c,
+                               const cx<R>* __restrict__ Ff, cx<R>* __restrict__ out) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  if (!mode_of(P, idx, m)) return;
+  cx<R> r = czero<R>();
+  if (m.in) {
+    if (op <= FOP_V) {
+      const cx<R> a = w[idx];
+      cx<R> psi = czero<R>();
+      if (m.ks > (R)1e-12) psi = mk<R>(rdiv(a.x, m.ks), rdiv(a.y, m.ks));
+      r = op == FOP_U ? mul_ik(psi, m.ky) : mul_ik(psi, -m.kx);
+    } else if (op == FOP_WX) r = mul_ik(w[idx], m.kx);
+    else if (op == FOP_WY) r = mul_ik(w[idx], m.ky);
+    else if (op == FOP_CT) r = c[idx];
+    else if (op == FOP_CX) r = mul_ik(c[idx], m.kx);
+    else if (op == FOP_CY) r = mul_ik(c[idx], m.ky);
+    else {  // mu_hat = T[1.5 sigma eps k^2 c + 24 (sigma/eps) F[f]]  (surface_tension.c:45-46)
+      const R q = rmul(P.s1, m.ks);
+      const cx<R> a = c[idx], f = Ff[idx];
+      r = mk<R>(radd(rmul(q, a.x), rmul(P.s2, f.x)), radd(rmul(q, a.y), rmul(P.s2, f.y)));
+    }
+  }
+  out[idx] = r;
+}
+
+// out = i k in (dir 0: kx, 1: ky), no truncation
+template <class R>
+__global__ void k_spec_mul_ik(const AdjPar<R> P, const cx<R>* __restrict__ in, cx<R>* __restrict__ out, int dir) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  if (!mode_of(P, idx, m)) return;
+  out[idx] = mul_ik(in[idx], dir == 0 ? m.kx : m.ky);
+}
+
+// f(c) = c (1-c)(1-2c) in place
+template <class R> __global__ void k_adj_bulk(R* __restrict__ x, size_t nn) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
+    const R a = x[k];
+    x[k] = rmul(rmul(a, rsub((R)1, a)), rsub((R)1, rmul((R)2, a)));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// adjoint of the spectral tail of nonlin() (nonlin.c:74-101, 232-253,
+// surface_tension.c:98-111, curl.c): from N_bar, the spectra whose F^T
+// (= n^2 ifft(X / w)) gives the physical adjoints A_bar, B_bar, Fx_bar, Fy_bar.
+// op: 0 A_bar = -Nw_bar, 1 B_bar = -Nc_bar, 2 Fx_bar = conj(-i ky) Nw_bar,
+//     3 Fy_bar = conj(i kx) Nw_bar.  Output scaled by n^2 / w_j (ifft then
+// divides by n^2).
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_adj_tail(int op, const AdjPar<R> P, const cx<R>* __restrict__ nw, const cx<R>* __restrict__ nc,
+                           cx<R>* __restrict__ out) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  if (!mode_of(P, idx, m)) return;
+  const R sc = (R)((double)P.n * (double)P.n) / m.wj;
+  cx<R> r;
+  if (op == 0) r = cscale(nw[idx], (R)-1);
+  else if (op == 1) r = cscale(nc[idx], (R)-1);
+  else if (op == 2) r = mul_ik(nw[idx], m.ky);    // conj(-i ky) = i ky
+  else r = mul_mik(nw[idx], m.kx);                // conj(i kx) = -i kx
+  out[idx] = cscale(r, sc);
+}
+
+// lambda_bar, sigma_bar from N_c = -F[B] - lambda s2 k^2 F[f] (nonlin.c:240,251)
+template <class R>
+__global__ void k_adj_param_nc(const AdjPar<R> P, const cx<R>* __restrict__ nc, const cx<R>* __restrict__ Ff,
+                               double* acc) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  double dl = 0.0, ds = 0.0;
+  if (mode_of(P, idx, m)) {
+    const double d = -(double)m.ks * rdot(nc[idx], Ff[idx]);
+    dl = (double)P.s2 * d;
+    ds = (double)P.lam * P.ds2 * d;
+  }
+  block_acc3(0.0, dl, ds, acc);
+}
+
+// mu_bar_hat = T[(w_j / n^2) dfft(mu_bar)]; c_bar += s1 k^2 mu_bar_hat;
+// the spectrum of F[f]'s adjoint s2 mu_bar_hat - lambda s2 k^2 Nc_bar, scaled
+// n^2 / w_j for F^T; sigma_bar from the mu terms.
+template <class R>
+__global__ void k_adj_mu(const AdjPar<R> P, const cx<R>* __restrict__ mub_hat_raw, const cx<R>* __restrict__ c,
+                         const cx<R>* __restrict__ Ff, const cx<R>* __restrict__ nc, cx<R>* __restrict__ gc,
+                         cx<R>* __restrict__ fbar_spec, double* acc) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  double ds = 0.0;
+  if (mode_of(P, idx, m)) {
+    const R n2 = (R)((double)P.n * (double)P.n);
+    cx<R> mb = czero<R>();
+    if (m.in) mb = cscale(mub_hat_raw[idx], m.wj / n2);
+    const cx<R> g = gc[idx];
+    const R q = rmul(P.s1, m.ks);
+    gc[idx] = mk<R>(g.x + q * mb.x, g.y + q * mb.y);
+    const cx<R> a = c[idx], f = Ff[idx];
+    ds = rdot(mb, mk<R>((R)(P.ds1 * (double)m.ks) * a.x + (R)P.ds2 * f.x, (R)(P.ds1 * (double)m.ks) * a.y + (R)P.ds2 * f.y));
+    const R ql = rmul(rmul(P.lam, P.s2), m.ks);
+    const cx<R> nb = nc[idx];
+    const cx<R> fb = mk<R>(P.s2 * mb.x - ql * nb.x, P.s2 * mb.y - ql * nb.y);
+    fbar_spec[idx] = cscale(fb, n2 / m.wj);
+  }
+  block_acc3(0.0, 0.0, ds, acc);
+}
+
+// physical adjoints of the products (nonlin.c:62, 207; surface_tension.c:87-88):
+// mu_bar = Fx_bar cx + Fy_bar cy
+template <class R>
+__global__ void k_adj_mubar(const R* __restrict__ fxb, const R* __restrict__ fyb, const R* __restrict__ cxp,
+                            const R* __restrict__ cyp, R* __restrict__ mub, size_t nn) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x)
+    mub[k] = fxb[k] * cxp[k] + fyb[k] * cyp[k];
+}
+
+// in place: (Ab, Bb, Fxb, Fyb, fb) -> (u_bar, v_bar, wx_bar, wy_bar, ct_bar, cx_bar, cy_bar)
+//   u_bar = Ab wx + Bb cx, v_bar = Ab wy + Bb cy, wx_bar = Ab u, wy_bar = Ab v,
+//   cx_bar = Bb u + Fxb mu, cy_bar = Bb v + Fyb mu, ct_bar = fb f'(ct)
+template <class R> struct PhysFields {
+  R *u, *v, *wx, *wy, *ct, *cx, *cy, *mu;
+};
+template <class R> struct PhysAdj {
+  R *ab, *bb, *fxb, *fyb, *fb;         // inputs
+  R *ub, *vb, *wxb, *wyb, *ctb, *cxb, *cyb;  // outputs
+};
+template <class R>
+__global__ void k_adj_products(const PhysFields<R> F, const PhysAdj<R> A, size_t nn) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
+    const R ab = A.ab[k], bb = A.bb[k], fxb = A.fxb[k], fyb = A.fyb[k], fb = A.fb[k];
+    const R u = F.u[k], v = F.v[k], ct = F.ct[k], mu = F.mu[k];
+    A.ub[k] = ab * F.wx[k] + bb * F.cx[k];
+    A.vb[k] = ab * F.wy[k] + bb * F.cy[k];
+    A.wxb[k] = ab * u;
+    A.wyb[k] = ab * v;
+    A.cxb[k] = bb * u + fxb * mu;
+    A.cyb[k] = bb * v + fyb * mu;
+    A.ctb[k] = fb * ((R)1 - (R)6 * ct + (R)6 * ct * ct);
+  }
+}
+
+// accumulation of C^T(x_bar) = (w_j / n^2) dfft(x_bar) through the multipliers
+// of the forward fields into (gw, gc):
+//   u = T[i ky psi], v = T[-i kx psi], psi = w / k^2; wx = T[i kx w], wy = T[i ky w];
+//   ct = T[c], cx = T[i kx c], cy = T[i ky c]
+template <class R>
+__global__ void k_adj_acc(int op, const AdjPar<R> P, const cx<R>* __restrict__ xb_hat, cx<R>* __restrict__ gw,
+                          cx<R>* __restrict__ gc) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  if (!mode_of(P, idx, m) || !m.in) return;
+  const R n2 = (R)((double)P.n * (double)P.n);
+  const cx<R> x = cscale(xb_hat[idx], m.wj / n2);
+  cx<R> d;
+  if (op <= FOP_V) {
+    if (!(m.ks > (R)1e-12)) return;
+    const cx<R> pb = op == FOP_U ? mul_mik(x, m.ky) : mul_mik(x, -m.kx);
+    d = mk<R>(rdiv(pb.x, m.ks), rdiv(pb.y, m.ks));
+  } else if (op == FOP_WX) d = mul_mik(x, m.kx);
+  else if (op == FOP_WY) d = mul_mik(x, m.ky);
+  else if (op == FOP_CT) d = x;
+  else if (op == FOP_CX) d = mul_mik(x, m.kx);
+  else d = mul_mik(x, m.ky);
+  cx<R>* g = op <= FOP_WY ? gw : gc;
+  const cx<R> o = g[idx];
+  g[idx] = mk<R>(o.x + d.x, o.y + d.y);
+}
+
+// ---------------------------------------------------------------------------
+// ETD2RK adjoint (etd2rk.c:81-135, 155-212) with parameter derivatives.
+// coef [6][nr][nr] (eta_w, z1_w, z2_w, beta_c, z1_c, z2_c); dcoef [9][nr][nr]:
+// d(eta_w, z1_w, z2_w)/d nu, d(beta_c, z1_c, z2_c)/d lambda, ... / d sigma.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_adj_etd2(const AdjPar<R> P, const R* __restrict__ coef, const double* __restrict__ dcoef,
+                           const cx<R>* __restrict__ gw, const cx<R>* __restrict__ gc,
+                           const cx<R>* __restrict__ nsw, const cx<R>* __restrict__ nsc,
+                           const cx<R>* __restrict__ nw, const cx<R>* __restrict__ nc,
+                           cx<R>* __restrict__ nbs_w, cx<R>* __restrict__ nbs_c,
+                           cx<R>* __restrict__ nba_w, cx<R>* __restrict__ nba_c, double* acc) {
+  // stage 2: u1 = u* + z2 (N* - N):  N*_bar = z2 u1_bar, N_bar (partial) = -z2 u1_bar
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  double dnu = 0.0, dl = 0.0, dsg = 0.0;
+  if (mode_of(P, idx, m)) {
+    const int nr = P.n / 2 + 1;
+    const size_t t = (size_t)nr * nr, o = (size_t)m.row * nr + m.am;
+    const R z2w = coef[2 * t + o], z2c = coef[5 * t + o];
+    const cx<R> bw = gw[idx], bc = gc[idx];
+    nbs_w[idx] = cscale(bw, z2w);
+    nbs_c[idx] = cscale(bc, z2c);
+    nba_w[idx] = cscale(bw, -z2w);
+    nba_c[idx] = cscale(bc, -z2c);
+    const cx<R> dw = nsw[idx] - nw[idx], dc = nsc[idx] - nc[idx];
+    dnu = dcoef[2 * t + o] * rdot(bw, dw);
+    dl = dcoef[5 * t + o] * rdot(bc, dc);
+    dsg = dcoef[8 * t + o] * rdot(bc, dc);
+  }
+  block_acc3(dnu, dl, dsg, acc);
+}
+
+template <class R>
+__global__ void k_adj_etd1(const AdjPar<R> P, const R* __restrict__ coef, const double* __restrict__ dcoef,
+                           cx<R>* __restrict__ gw, cx<R>* __restrict__ gc, const cx<R>* __restrict__ uw,
+                           const cx<R>* __restrict__ uc, const cx<R>* __restrict__ nw, const cx<R>* __restrict__ nc,
+                           cx<R>* __restrict__ nbw, cx<R>* __restrict__ nbc, double* acc) {
+  // stage 1: u* = e u + z1 N(u):  u_bar = e u*_bar, N_bar += z1 u*_bar
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  double dnu = 0.0, dl = 0.0, dsg = 0.0;
+  if (mode_of(P, idx, m)) {
+    const int nr = P.n / 2 + 1;
+    const size_t t = (size_t)nr * nr, o = (size_t)m.row * nr + m.am;
+    const R ew = coef[0 * t + o], z1w = coef[1 * t + o], ec = coef[3 * t + o], z1c = coef[4 * t + o];
+    const cx<R> bw = gw[idx], bc = gc[idx];
+    const cx<R> a = nbw[idx], b = nbc[idx];
+    nbw[idx] = mk<R>(a.x + z1w * bw.x, a.y + z1w * bw.y);
+    nbc[idx] = mk<R>(b.x + z1c * bc.x, b.y + z1c * bc.y);
+    gw[idx] = cscale(bw, ew);
+    gc[idx] = cscale(bc, ec);
+    dnu = dcoef[0 * t + o] * rdot(bw, uw[idx]) + dcoef[1 * t + o] * rdot(bw, nw[idx]);
+    dl = dcoef[3 * t + o] * rdot(bc, uc[idx]) + dcoef[4 * t + o] * rdot(bc, nc[idx]);
+    dsg = dcoef[6 * t + o] * rdot(bc, uc[idx]) + dcoef[7 * t + o] * rdot(bc, nc[idx]);
+  }
+  block_acc3(dnu, dl, dsg, acc);
+}
+
+// ---------------------------------------------------------------------------
+// loss J = a_bulk E_bulk + a_grad E_grad + a_phi <|grad phi|^2>, phi = 2c - 1,
+// at the final state (free_energy.c: c and its gradient NOT truncated)
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_adj_loss(const R* __restrict__ c, const R* __restrict__ cxp, const R* __restrict__ cyp,
+                           R* __restrict__ cb, R* __restrict__ cxb, R* __restrict__ cyb, size_t nn, double kb,
+                           double kg, double dkb, double dkg, double* acc) {
+  // per point: J = kb c^2 (1-c)^2 + kg (cx^2 + cy^2), kb/kg include 1/n^2;
+  // acc[0] += J, acc[2] += d J / d sigma through kb, kg (dkb, dkg)
+  double sj = 0.0, ssg = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
+    const double a = c[k], x = cxp[k], y = cyp[k];
+    const double b = a * a * (1.0 - a) * (1.0 - a), g = x * x + y * y;
+    sj += kb * b + kg * g;
+    ssg += dkb * b + dkg * g;
+    cb[k] = (R)(kb * 2.0 * a * (1.0 - a) * (1.0 - 2.0 * a));
+    cxb[k] = (R)(kg * 2.0 * x);
+    cyb[k] = (R)(kg * 2.0 * y);
+  }
+  block_acc3(sj, 0.0, ssg, acc);
+}
+
+// (gw, gc) of the loss: gc = (w_j/n^2)(dfft(cb) - i kx dfft(cxb) - i ky dfft(cyb))
+template <class R>
+__global__ void k_adj_loss_acc(int op, const AdjPar<R> P, const cx<R>* __restrict__ xb_hat, cx<R>* __restrict__ gc) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  if (!mode_of(P, idx, m)) return;
+  const R n2 = (R)((double)P.n * (double)P.n);
+  const cx<R> x = cscale(xb_hat[idx], m.wj / n2);
+  cx<R> d = op == 0 ? x : (op == 1 ? mul_mik(x, m.kx) : mul_mik(x, m.ky));
+  const cx<R> o = op == 0 ? czero<R>() : gc[idx];
+  gc[idx] = mk<R>(o.x + d.x, o.y + d.y);
+}
+
+}  // namespace chns

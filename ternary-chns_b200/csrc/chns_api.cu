@@ -155,6 +155,7 @@ int validate(const chns_params* p) {
 
 void free_all(chns_ctx* c) {
   if (!c) return;
+  chns_adj_free(c);
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   void* ptrs[] = {c->state[0], c->state[1], c->state[2], c->saved[0], c->saved[1], c->saved[2], c->nw,
                   c->coef, c->mrow, c->tw, c->k0, c->stage, c->realbuf, c->realdbl, c->red, c->redscratch};

@@ -6,6 +6,8 @@
 #include "../../include/chns.h"
 
 struct chns_ctx;
+struct chns_adj;
+void chns_adj_free(chns_ctx* c);
 
 namespace chns {
 // intermediate buffers of a step: G slots (rows 0..jt) and H slots (rows
@@ -69,6 +71,8 @@ struct chns_ctx {
   bool graph_ok;
   void* hostpin;    // pinned staging for host transfers
   size_t hostpin_bytes;
+  // discrete-adjoint buffers (allocated by the first chns_adjoint call)
+  chns_adj* adj;
   // tracing: when prof_ev is set, every launch of a stage records an event
   cudaEvent_t* prof_ev;
   int* prof_kind;
