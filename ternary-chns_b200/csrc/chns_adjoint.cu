@@ -3,12 +3,13 @@
 // Gradient of a final-time functional J(c_T) with respect to the initial spectral
 // state (omega_hat_0, c_hat_0) and to nu, lambda (the mobility M) and sigma.
 // Reverse sweep with two-level checkpointing: the forward pass keeps the state
-// every `ckpt` steps; each segment is recomputed forward from its checkpoint,
-// keeping its states, and reversed step by step.  Reversing step n re-runs the
-// forward stage kernels to get u* = stage1(u_n), N(u_n) and N(u*), then applies
-// the transposed stage-2 update, the transposed right-hand side at u*, the
-// transposed stage-1 update and the transposed right-hand side at u_n (kernels
-// in chns_adjoint.cuh).
+// every `ckpt` steps; each segment is recomputed forward from its checkpoint
+// (the last one is recorded during the forward pass), keeping per step u_n, the
+// stage-1 state u*, N(u_n) and N(u*) (the stage-2 kernels store N(u*) when the
+// context's nstar pointers are set).  Reversing a step applies the transposed
+// stage-2 update, the transposed right-hand side at u*, the transposed stage-1
+// update and the transposed right-hand side at u_n (kernels in
+// chns_adjoint.cuh), captured once as a CUDA graph on fixed buffers.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
@@ -64,22 +65,44 @@ void dcoef_dc(double c, double h, double* o) {
 
 }  // namespace
 
+// Device buffers of the adjoint, kept in the context between calls.
+//   spec: NSPEC S-layout fields in one allocation (slot k at k ncx complex)
+//   phys: NPHYS real n x n fields in one allocation
+//   bscr: scratch of the batched transforms (7 fields)
+//   seg:  per step of the current segment, 8 fields: u_n, u*, N(u_n), N(u*)
 struct chns_adj {
-  int cap_states;            // segment length the buffers were sized for
-  void* seg;                 // segment states: cap_states x 2 S fields (+ k0 in FP32)
-  double* segk0;             // cap_states x 16
-  void** ckpt;               // checkpoints (host array of device pointers)
+  int cap_states;
+  void* seg;
+  void** ckpt;
   double** ckptk0;
   int nckpt_cap;
-  void* dcoef;               // [9][nr][nr] double
-  double* acc;               // [4] J, dJ/dlambda, dJ/dsigma accumulators; [0] also nu in etd kernels
-  double* pacc;              // [3] nu, lambda, sigma
-  void* spec[16];            // S-layout scratch
-  void* phys[20];            // real scratch
+  void* dcoef;        // [9][nr][nr] double
+  double* acc;        // [8]: J, -, dJ/dsigma (loss part), -, nu, lambda, sigma (step part)
+  void* spec;
+  void* phys;
+  void* bscr;
+  cudaGraphExec_t rev;  // one reverse step (fixed buffers), or null
+  bool rev_tried;
   size_t ncx, nn;
 };
 
 namespace {
+
+// spectral slots
+enum {
+  SB0 = 0,               // batch of 7 (SB0 .. SB0+6)
+  SFF = 7, SX, SY,       // F[f(c_t)], scratch
+  SNBW, SNBC,            // N*_bar
+  SNBAW, SNBAC,          // N(u_n)_bar
+  SGW, SGC,              // running gradient (w_bar, c_bar)
+  // current step, in the segment slot layout: u_n, u*, N(u_n), N(u*)
+  CUW, CUC, CSW, CSC, CNW, CNC, CXW, CXC,
+  NSPEC
+};
+// physical slots
+enum { PU = 0, PV, PWX, PWY, PCT, PCX, PCY, PMU, PFB, PAB, PBB, PFXB, PFYB, PUB, PVB, PWXB, PWYB, PCTB, PCXB, PCYB,
+       NPHYS };
+constexpr int SLOT_FIELDS = 8;
 
 template <class R> struct Adj {
   chns_ctx* c;
@@ -89,61 +112,71 @@ template <class R> struct Adj {
   size_t ncx, nn;
   int blocks_s, blocks_p;
 
-  cx<R>* S(int k) const { return (cx<R>*)a->spec[k]; }
-  R* F(int k) const { return (R*)a->phys[k]; }
+  cx<R>* S(int k) const { return (cx<R>*)a->spec + (size_t)k * ncx; }
+  R* F(int k) const { return (R*)a->phys + (size_t)k * nn; }
 
-  // physical-field slots
-  enum { PU = 0, PV, PWX, PWY, PCT, PCX, PCY, PMU, PAB, PBB, PFXB, PFYB, PFB, PUB, PVB, PWXB, PWYB, PCTB, PCXB, PCYB };
-  // spectral slots
-  enum { SFF = 0, SX, SY, SNW_S, SNC_S, SNW_N, SNC_N, SNBW, SNBC, SNBAW, SNBAC, SUSW, SUSC, SGW, SGC, NSPEC };
+  void ifft(const cx<R>* s, R* x, int nb) { c->L->ifftb(c, s, ncx, x, nn, nb, a->bscr); }
+  void dfft(const R* x, cx<R>* s, int nb) { c->L->dfftb(c, x, nn, s, ncx, nb, a->bscr); }
 
-  int ifft(const cx<R>* s, R* x) { return c->L->ifft(c, s, x); }
-  int dfft(const R* x, cx<R>* s) { return c->L->dfft(c, x, s); }
-
-  // forward physical fields of the right-hand side at state (w, cc)
-  void fwd_fields(const cx<R>* w, const cx<R>* cc) {
-    const int ops[7] = {FOP_U, FOP_V, FOP_WX, FOP_WY, FOP_CT, FOP_CX, FOP_CY};
-    const int dst[7] = {PU, PV, PWX, PWY, PCT, PCX, PCY};
-    for (int k = 0; k < 7; k++) {
-      k_adj_fwd_prep<R><<<blocks_s, 256, 0, st>>>(ops[k], P, w, cc, nullptr, S(SX));
-      ifft(S(SX), F(dst[k]));
-    }
-    // F[f(c_t)] and mu (surface_tension.c:20-75)
-    cudaMemcpyAsync(F(PFB), F(PCT), nn * sizeof(R), cudaMemcpyDeviceToDevice, st);
-    k_adj_bulk<R><<<blocks_p, 256, 0, st>>>(F(PFB), nn);
-    dfft(F(PFB), S(SFF));
-    k_adj_fwd_prep<R><<<blocks_s, 256, 0, st>>>(FOP_MU, P, w, cc, S(SFF), S(SX));
-    ifft(S(SX), F(PMU));
-  }
-
-  // (gw, gc) += J_N(state)^T (nbw, nbc); parameter partials into pacc
+  // (gw, gc) += J_N(w, cc)^T (nbw, nbc); parameter partials into acc[4..6]
   void vjp(const cx<R>* w, const cx<R>* cc, const cx<R>* nbw, const cx<R>* nbc, cx<R>* gw, cx<R>* gc) {
-    fwd_fields(w, cc);
-    double* pacc = a->pacc;
-    k_adj_param_nc<R><<<blocks_s, 256, 0, st>>>(P, nbc, S(SFF), pacc);
-    const int tail_dst[4] = {PAB, PBB, PFXB, PFYB};
-    for (int op = 0; op < 4; op++) {
-      k_adj_tail<R><<<blocks_s, 256, 0, st>>>(op, P, nbw, nbc, S(SX));
-      ifft(S(SX), F(tail_dst[op]));
-    }
-    // mu_bar -> mu_bar_hat -> c_bar (s1 k^2), f_bar
+    double* pacc = a->acc + 4;
+    // forward fields at the state
+    k_adj_fwd_prep7<R><<<blocks_s, 256, 0, st>>>(P, w, cc, S(SB0), ncx);
+    ifft(S(SB0), F(PU), FOP_N);
+    k_adj_bulk<R><<<blocks_p, 256, 0, st>>>(F(PCT), F(PFB), nn);
+    dfft(F(PFB), S(SFF), 1);
+    k_adj_mu_prep<R><<<blocks_s, 256, 0, st>>>(P, cc, S(SFF), S(SX));
+    ifft(S(SX), F(PMU), 1);
+    // transposed spectral tail -> A_bar, B_bar, Fx_bar, Fy_bar
+    k_adj_tail4<R><<<blocks_s, 256, 0, st>>>(P, nbw, nbc, S(SB0), ncx);
+    ifft(S(SB0), F(PAB), 4);
+    // mu_bar -> c_bar (s1 k^2), f_bar, lambda and sigma partials
     k_adj_mubar<R><<<blocks_p, 256, 0, st>>>(F(PFXB), F(PFYB), F(PCX), F(PCY), F(PUB), nn);
-    dfft(F(PUB), S(SX));
+    dfft(F(PUB), S(SX), 1);
     k_adj_mu<R><<<blocks_s, 256, 0, st>>>(P, S(SX), cc, S(SFF), nbc, gc, S(SY), pacc);
-    ifft(S(SY), F(PFB));
-    // products
+    ifft(S(SY), F(PFB), 1);
+    // products, then C^T of the seven forward fields
     PhysFields<R> pf{F(PU), F(PV), F(PWX), F(PWY), F(PCT), F(PCX), F(PCY), F(PMU)};
     PhysAdj<R> pa{F(PAB), F(PBB), F(PFXB), F(PFYB), F(PFB), F(PUB), F(PVB), F(PWXB), F(PWYB), F(PCTB), F(PCXB),
                   F(PCYB)};
     k_adj_products<R><<<blocks_p, 256, 0, st>>>(pf, pa, nn);
-    const int ops[7] = {FOP_U, FOP_V, FOP_WX, FOP_WY, FOP_CT, FOP_CX, FOP_CY};
-    const int src[7] = {PUB, PVB, PWXB, PWYB, PCTB, PCXB, PCYB};
-    for (int k = 0; k < 7; k++) {
-      dfft(F(src[k]), S(SX));
-      k_adj_acc<R><<<blocks_s, 256, 0, st>>>(ops[k], P, S(SX), gw, gc);
-    }
+    dfft(F(PUB), S(SB0), FOP_N);
+    k_adj_acc7<R><<<blocks_s, 256, 0, st>>>(P, S(SB0), gw, gc, ncx);
+  }
+
+  // one reversed step from the current-step slots (CUW..CXC): the transposed
+  // stage 2, right-hand side at u*, stage 1 and right-hand side at u_n
+  void reverse_step(const R* coef, const double* dcoef) {
+    double* pacc = a->acc + 4;
+    cx<R>* gw = S(SGW);
+    cx<R>* gc = S(SGC);
+    k_adj_etd2<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(CXW), S(CXC), S(CNW), S(CNC), S(SNBW),
+                                            S(SNBC), S(SNBAW), S(SNBAC), pacc);
+    vjp(S(CSW), S(CSC), S(SNBW), S(SNBC), gw, gc);
+    k_adj_etd1<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(CUW), S(CUC), S(CNW), S(CNC), S(SNBAW),
+                                            S(SNBAC), pacc);
+    vjp(S(CUW), S(CUC), S(SNBAW), S(SNBAC), gw, gc);
   }
 };
+
+// one forward step that also records u_n, u*, N(u_n) and N(u*) into a segment slot
+int record_step(chns_ctx* c, char* slot, size_t fbytes) {
+  cudaStream_t st = c->stream;
+  ACK(cudaMemcpyAsync(slot, c->state[0], fbytes, cudaMemcpyDeviceToDevice, st));
+  ACK(cudaMemcpyAsync(slot + fbytes, c->state[1], fbytes, cudaMemcpyDeviceToDevice, st));
+  c->L->stage(c, 1);
+  ACK(cudaMemcpyAsync(slot + 2 * fbytes, c->state[0], fbytes, cudaMemcpyDeviceToDevice, st));
+  ACK(cudaMemcpyAsync(slot + 3 * fbytes, c->state[1], fbytes, cudaMemcpyDeviceToDevice, st));
+  ACK(cudaMemcpyAsync(slot + 4 * fbytes, c->saved[0], fbytes, cudaMemcpyDeviceToDevice, st));
+  ACK(cudaMemcpyAsync(slot + 5 * fbytes, c->saved[1], fbytes, cudaMemcpyDeviceToDevice, st));
+  c->nstar[0] = slot + 6 * fbytes;
+  c->nstar[1] = slot + 7 * fbytes;
+  c->L->stage(c, 2);
+  c->nstar[0] = nullptr;
+  c->nstar[1] = nullptr;
+  return CHNS_OK;
+}
 
 int snapshot_save(chns_ctx* c, void* dst, double* dstk0) {
   const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
@@ -167,16 +200,15 @@ int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
   }
   chns_adj* a = c->adj;
   const size_t ncx = (size_t)c->n * c->nr, nn = (size_t)c->n * c->n;
-  const size_t snap = 2 * ncx * 2 * c->rsz;
+  const size_t fbytes = ncx * 2 * c->rsz;  // one S-layout field
+  const size_t snap = 2 * fbytes;
   a->ncx = ncx;
   a->nn = nn;
   if (!a->dcoef) {
-    for (int k = 0; k < 16; k++)
-      if (cudaMalloc(&a->spec[k], ncx * 2 * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
-    for (int k = 0; k < 20; k++)
-      if (cudaMalloc(&a->phys[k], nn * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->spec, NSPEC * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->phys, NPHYS * nn * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->bscr, FOP_N * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMalloc((void**)&a->acc, 8 * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
-    a->pacc = a->acc + 4;
     // derivative tables of the ETD coefficients: d/dnu (w), d/dlambda, d/dsigma (c)
     const int nr = c->nr;
     const chns_params& p = c->p;
@@ -200,9 +232,9 @@ int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
   }
   if (seglen > a->cap_states) {
     if (a->seg) cudaFree(a->seg);
-    if (a->segk0) cudaFree(a->segk0);
-    if (cudaMalloc(&a->seg, snap * seglen) != cudaSuccess) return CHNS_ERR_NOMEM;
-    if (cudaMalloc((void**)&a->segk0, 16 * sizeof(double) * seglen) != cudaSuccess) return CHNS_ERR_NOMEM;
+    a->seg = nullptr;
+    a->cap_states = 0;
+    if (cudaMalloc(&a->seg, SLOT_FIELDS * fbytes * seglen) != cudaSuccess) return CHNS_ERR_NOMEM;
     a->cap_states = seglen;
   }
   if (nckpt > a->nckpt_cap) {
@@ -214,6 +246,10 @@ int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
     free(a->ckptk0);
     a->ckpt = (void**)calloc(nckpt, sizeof(void*));
     a->ckptk0 = (double**)calloc(nckpt, sizeof(double*));
+    if (!a->ckpt || !a->ckptk0) {
+      a->nckpt_cap = 0;
+      return CHNS_ERR_NOMEM;
+    }
     a->nckpt_cap = nckpt;
     for (int k = 0; k < nckpt; k++) {
       if (cudaMalloc(&a->ckpt[k], snap) != cudaSuccess) return CHNS_ERR_NOMEM;
@@ -250,81 +286,65 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
   A.P.ds2 = 24.0 / p.epsilon;
   A.P.mrow = c->mrow;
   cudaStream_t st = c->stream;
-  const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
-  const size_t snap = 2 * bytes;
+  const size_t bytes = A.ncx * sizeof(cx<R>);
   const R* coef = (const R*)c->coef;
   const double* dcoef = (const double*)a->dcoef;
   ACK(cudaMemsetAsync(a->acc, 0, 8 * sizeof(double), st));
 
-  // forward sweep with checkpoints; checkpoint nseg keeps u_0 for restoring
+  // forward sweep with checkpoints (checkpoint nseg keeps u_0 for restoring);
+  // the last segment is recorded on the way
+  char* segbase = (char*)a->seg;
+  const size_t slot = SLOT_FIELDS * bytes;
+  const int nlast = (nseg - 1) * ckpt;
   if ((rc = snapshot_save(c, a->ckpt[nseg], a->ckptk0[nseg]))) return rc;
   for (int n = 0; n < nsteps; n++) {
     if (n % ckpt == 0 && (rc = snapshot_save(c, a->ckpt[n / ckpt], a->ckptk0[n / ckpt]))) return rc;
-    c->L->stage(c, 1);
-    c->L->stage(c, 2);
+    rc = n >= nlast ? record_step(c, segbase + (size_t)(n - nlast) * slot, bytes) : chns_step(c, 1);
+    if (rc) return rc;
   }
   // loss at the final state and its gradient (free_energy.c:3-157: c and grad c untruncated)
-  cx<R>* gradw = A.S(A.SGW);
-  cx<R>* gradc = A.S(A.SGC);
   {
-    const cx<R>* ch = (const cx<R>*)c->state[1];
-    ACK(cudaMemcpyAsync(A.S(A.SX), ch, bytes, cudaMemcpyDeviceToDevice, st));
-    A.ifft(A.S(A.SX), A.F(A.PCT));
-    k_spec_mul_ik<R><<<A.blocks_s, 256, 0, st>>>(A.P, ch, A.S(A.SX), 0);
-    A.ifft(A.S(A.SX), A.F(A.PCX));
-    k_spec_mul_ik<R><<<A.blocks_s, 256, 0, st>>>(A.P, ch, A.S(A.SX), 1);
-    A.ifft(A.S(A.SX), A.F(A.PCY));
+    k_adj_loss_prep3<R><<<A.blocks_s, 256, 0, st>>>(A.P, (const cx<R>*)c->state[1], A.S(SB0), A.ncx);
+    A.ifft(A.S(SB0), A.F(PCT), 3);
     const double inv = 1.0 / ((double)c->n * (double)c->n);
     const double kb = lw[0] * 12.0 * (p.sigma / p.epsilon) * inv;
     const double kg = (lw[1] * 0.75 * p.sigma * p.epsilon + 4.0 * lw[2]) * inv;
     const double dkb = lw[0] * 12.0 / p.epsilon * inv;
     const double dkg = lw[1] * 0.75 * p.epsilon * inv;
-    k_adj_loss<R><<<A.blocks_p, 256, 0, st>>>(A.F(A.PCT), A.F(A.PCX), A.F(A.PCY), A.F(A.PUB), A.F(A.PVB),
-                                              A.F(A.PWXB), A.nn, kb, kg, dkb, dkg, a->acc);
-    const int srcs[3] = {A.PUB, A.PVB, A.PWXB};
-    for (int op = 0; op < 3; op++) {
-      A.dfft(A.F(srcs[op]), A.S(A.SX));
-      k_adj_loss_acc<R><<<A.blocks_s, 256, 0, st>>>(op, A.P, A.S(A.SX), gradc);
-    }
-    ACK(cudaMemsetAsync(gradw, 0, bytes, st));
+    k_adj_loss<R><<<A.blocks_p, 256, 0, st>>>(A.F(PCT), A.F(PCX), A.F(PCY), A.F(PUB), A.F(PVB), A.F(PWXB), A.nn, kb,
+                                              kg, dkb, dkg, a->acc);
+    A.dfft(A.F(PUB), A.S(SB0), 3);
+    k_adj_loss_acc3<R><<<A.blocks_s, 256, 0, st>>>(A.P, A.S(SB0), A.S(SGC), A.S(SGW), A.ncx);
   }
-  // reverse sweep
-  char* segbase = (char*)a->seg;
-  for (int s = nseg - 1; s >= 0; s--) {
-    const int n0 = s * ckpt, len = (n0 + ckpt <= nsteps) ? ckpt : nsteps - n0;
-    if ((rc = snapshot_load(c, a->ckpt[s], a->ckptk0[s]))) return rc;
-    for (int k = 0; k < len; k++) {
-      if ((rc = snapshot_save(c, segbase + (size_t)k * snap, a->segk0 + 16 * k))) return rc;
-      if (k + 1 < len) {
-        c->L->stage(c, 1);
-        c->L->stage(c, 2);
+  // the reversed step as a CUDA graph on its fixed buffers (eager if capture fails)
+  if (!a->rev && !a->rev_tried) {
+    a->rev_tried = true;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      A.reverse_step(coef, dcoef);
+      if (cudaStreamEndCapture(st, &g) == cudaSuccess && g) {
+        if (cudaGraphInstantiate(&a->rev, g, 0) != cudaSuccess) a->rev = nullptr;
+        cudaGraphDestroy(g);
       }
     }
+    cudaGetLastError();
+  }
+  // reverse sweep: each segment but the last is recomputed from its checkpoint,
+  // recording its steps, then its steps are reversed
+  for (int s = nseg - 1; s >= 0; s--) {
+    const int n0 = s * ckpt, len = (n0 + ckpt <= nsteps) ? ckpt : nsteps - n0;
+    if (s != nseg - 1) {
+      if ((rc = snapshot_load(c, a->ckpt[s], a->ckptk0[s]))) return rc;
+      for (int k = 0; k < len; k++)
+        if ((rc = record_step(c, segbase + (size_t)k * slot, bytes))) return rc;
+    }
     for (int k = len - 1; k >= 0; k--) {
-      const cx<R>* un_w = (const cx<R>*)(segbase + (size_t)k * snap);
-      const cx<R>* un_c = (const cx<R>*)(segbase + (size_t)k * snap + bytes);
-      // u* = stage1(u_n) and N(u_n)
-      if ((rc = snapshot_load(c, un_w, a->segk0 + 16 * k))) return rc;
-      c->L->stage(c, 1);
-      ACK(cudaMemcpyAsync(A.S(A.SNW_N), c->saved[0], bytes, cudaMemcpyDeviceToDevice, st));
-      ACK(cudaMemcpyAsync(A.S(A.SNC_N), c->saved[1], bytes, cudaMemcpyDeviceToDevice, st));
-      ACK(cudaMemcpyAsync(A.S(A.SUSW), c->state[0], bytes, cudaMemcpyDeviceToDevice, st));
-      ACK(cudaMemcpyAsync(A.S(A.SUSC), c->state[1], bytes, cudaMemcpyDeviceToDevice, st));
-      // N(u*): stage 1 again from u* (its state update is discarded)
-      c->L->stage(c, 1);
-      ACK(cudaMemcpyAsync(A.S(A.SNW_S), c->saved[0], bytes, cudaMemcpyDeviceToDevice, st));
-      ACK(cudaMemcpyAsync(A.S(A.SNC_S), c->saved[1], bytes, cudaMemcpyDeviceToDevice, st));
-      // stage 2 transposed: N*_bar -> (SNBW, SNBC), the N(u_n)_bar part -> (SNBAW, SNBAC)
-      k_adj_etd2<R><<<A.blocks_s, 256, 0, st>>>(A.P, coef, dcoef, gradw, gradc, A.S(A.SNW_S), A.S(A.SNC_S),
-                                                A.S(A.SNW_N), A.S(A.SNC_N), A.S(A.SNBW), A.S(A.SNBC),
-                                                A.S(A.SNBAW), A.S(A.SNBAC), a->pacc);
-      // transposed right-hand side at u*
-      A.vjp(A.S(A.SUSW), A.S(A.SUSC), A.S(A.SNBW), A.S(A.SNBC), gradw, gradc);
-      // stage 1 transposed
-      k_adj_etd1<R><<<A.blocks_s, 256, 0, st>>>(A.P, coef, dcoef, gradw, gradc, un_w, un_c, A.S(A.SNW_N),
-                                                A.S(A.SNC_N), A.S(A.SNBAW), A.S(A.SNBAC), a->pacc);
-      // transposed right-hand side at u_n
-      A.vjp(un_w, un_c, A.S(A.SNBAW), A.S(A.SNBAC), gradw, gradc);
+      ACK(cudaMemcpyAsync(A.S(CUW), segbase + (size_t)k * slot, slot, cudaMemcpyDeviceToDevice, st));
+      if (a->rev) {
+        ACK(cudaGraphLaunch(a->rev, st));
+      } else {
+        A.reverse_step(coef, dcoef);
+      }
     }
   }
   ACK(cudaGetLastError());
@@ -340,15 +360,14 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
     g_par[2] = h[6] + h[2];  // sigma: through the step and through the loss
   }
   const size_t fb = 2 * (size_t)c->n * c->nr * sizeof(double);
+  const cudaMemcpyKind kind = where == CHNS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   if (g_w) {
-    c->L->to_fftw(c, gradw, c->stage);
-    ACK(cudaMemcpyAsync(g_w, c->stage, fb, where == CHNS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                        st));
+    c->L->to_fftw(c, A.S(SGW), c->stage);
+    ACK(cudaMemcpyAsync(g_w, c->stage, fb, kind, st));
   }
   if (g_c) {
-    c->L->to_fftw(c, gradc, c->stage);
-    ACK(cudaMemcpyAsync(g_c, c->stage, fb, where == CHNS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                        st));
+    c->L->to_fftw(c, A.S(SGC), c->stage);
+    ACK(cudaMemcpyAsync(g_c, c->stage, fb, kind, st));
   }
   ACK(cudaStreamSynchronize(st));
   return CHNS_OK;
@@ -359,10 +378,10 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
 void chns_adj_free(chns_ctx* c) {
   chns_adj* a = c->adj;
   if (!a) return;
-  for (int k = 0; k < 16; k++)
-    if (a->spec[k]) cudaFree(a->spec[k]);
-  for (int k = 0; k < 20; k++)
-    if (a->phys[k]) cudaFree(a->phys[k]);
+  if (a->rev) cudaGraphExecDestroy(a->rev);
+  if (a->spec) cudaFree(a->spec);
+  if (a->phys) cudaFree(a->phys);
+  if (a->bscr) cudaFree(a->bscr);
   for (int k = 0; k < a->nckpt_cap; k++) {
     cudaFree(a->ckpt[k]);
     cudaFree(a->ckptk0[k]);
@@ -370,7 +389,6 @@ void chns_adj_free(chns_ctx* c) {
   free(a->ckpt);
   free(a->ckptk0);
   if (a->seg) cudaFree(a->seg);
-  if (a->segk0) cudaFree(a->segk0);
   if (a->dcoef) cudaFree(a->dcoef);
   if (a->acc) cudaFree(a->acc);
   free(a);

@@ -91,102 +91,94 @@ __device__ __forceinline__ void block_acc3(double a0, double a1, double a2, doub
 
 // ---------------------------------------------------------------------------
 // forward fields of the right-hand side at a state (nonlin.c:30-48, 177-198,
-// surface_tension.c:20-75): op selects the truncated spectrum to transform
+// surface_tension.c:20-75).  The seven truncated spectra u, v, wx, wy, ct, cx, cy
+// are written as one batch (field k at out + k ncx) for one batched inverse
+// transform.
 // ---------------------------------------------------------------------------
-enum { FOP_U = 0, FOP_V, FOP_WX, FOP_WY, FOP_CT, FOP_CX, FOP_CY, FOP_MU };
+enum { FOP_U = 0, FOP_V, FOP_WX, FOP_WY, FOP_CT, FOP_CX, FOP_CY, FOP_N };
 
 template <class R>
-__global__ void k_adj_fwd_prep(int op, const AdjPar<R> P, const cx<R>* __restrict__ w, const cx<R>* __restrict__ c,
-                               const cx<R>* __restrict__ Ff, cx<R>* __restrict__ out) {
+__global__ void k_adj_fwd_prep7(const AdjPar<R> P, const cx<R>* __restrict__ w, const cx<R>* __restrict__ c,
+                                cx<R>* __restrict__ out, size_t ncx) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  if (!mode_of(P, idx, m)) return;
+  cx<R> r[FOP_N];
+#pragma unroll
+  for (int k = 0; k < FOP_N; k++) r[k] = czero<R>();
+  if (m.in) {
+    const cx<R> a = w[idx], b = c[idx];
+    cx<R> psi = czero<R>();
+    if (m.ks > (R)1e-12) psi = mk<R>(rdiv(a.x, m.ks), rdiv(a.y, m.ks));
+    r[FOP_U] = mul_ik(psi, m.ky);
+    r[FOP_V] = mul_ik(psi, -m.kx);
+    r[FOP_WX] = mul_ik(a, m.kx);
+    r[FOP_WY] = mul_ik(a, m.ky);
+    r[FOP_CT] = b;
+    r[FOP_CX] = mul_ik(b, m.kx);
+    r[FOP_CY] = mul_ik(b, m.ky);
+  }
+#pragma unroll
+  for (int k = 0; k < FOP_N; k++) out[k * ncx + idx] = r[k];
+}
+
+// mu_hat = T[1.5 sigma eps k^2 c + 24 (sigma/eps) F[f]]  (surface_tension.c:45-46)
+template <class R>
+__global__ void k_adj_mu_prep(const AdjPar<R> P, const cx<R>* __restrict__ c, const cx<R>* __restrict__ Ff,
+                              cx<R>* __restrict__ out) {
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
   if (!mode_of(P, idx, m)) return;
   cx<R> r = czero<R>();
   if (m.in) {
-    if (op <= FOP_V) {
-      const cx<R> a = w[idx];
-      cx<R> psi = czero<R>();
-      if (m.ks > (R)1e-12) psi = mk<R>(rdiv(a.x, m.ks), rdiv(a.y, m.ks));
-      r = op == FOP_U ? mul_ik(psi, m.ky) : mul_ik(psi, -m.kx);
-    } else if (op == FOP_WX) r = mul_ik(w[idx], m.kx);
-    else if (op == FOP_WY) r = mul_ik(w[idx], m.ky);
-    else if (op == FOP_CT) r = c[idx];
-    else if (op == FOP_CX) r = mul_ik(c[idx], m.kx);
-    else if (op == FOP_CY) r = mul_ik(c[idx], m.ky);
-    else {  // mu_hat = T[1.5 sigma eps k^2 c + 24 (sigma/eps) F[f]]  (surface_tension.c:45-46)
-      const R q = rmul(P.s1, m.ks);
-      const cx<R> a = c[idx], f = Ff[idx];
-      r = mk<R>(radd(rmul(q, a.x), rmul(P.s2, f.x)), radd(rmul(q, a.y), rmul(P.s2, f.y)));
-    }
+    const R q = rmul(P.s1, m.ks);
+    const cx<R> a = c[idx], f = Ff[idx];
+    r = mk<R>(radd(rmul(q, a.x), rmul(P.s2, f.x)), radd(rmul(q, a.y), rmul(P.s2, f.y)));
   }
   out[idx] = r;
 }
 
-// out = i k in (dir 0: kx, 1: ky), no truncation
-template <class R>
-__global__ void k_spec_mul_ik(const AdjPar<R> P, const cx<R>* __restrict__ in, cx<R>* __restrict__ out, int dir) {
-  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  ModeIdx<R> m;
-  if (!mode_of(P, idx, m)) return;
-  out[idx] = mul_ik(in[idx], dir == 0 ? m.kx : m.ky);
-}
-
-// f(c) = c (1-c)(1-2c) in place
-template <class R> __global__ void k_adj_bulk(R* __restrict__ x, size_t nn) {
+// f(c) = c (1-c)(1-2c)
+template <class R> __global__ void k_adj_bulk(const R* __restrict__ x, R* __restrict__ y, size_t nn) {
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
     const R a = x[k];
-    x[k] = rmul(rmul(a, rsub((R)1, a)), rsub((R)1, rmul((R)2, a)));
+    y[k] = rmul(rmul(a, rsub((R)1, a)), rsub((R)1, rmul((R)2, a)));
   }
 }
 
 // ---------------------------------------------------------------------------
 // adjoint of the spectral tail of nonlin() (nonlin.c:74-101, 232-253,
-// surface_tension.c:98-111, curl.c): from N_bar, the spectra whose F^T
-// (= n^2 ifft(X / w)) gives the physical adjoints A_bar, B_bar, Fx_bar, Fy_bar.
-// op: 0 A_bar = -Nw_bar, 1 B_bar = -Nc_bar, 2 Fx_bar = conj(-i ky) Nw_bar,
-//     3 Fy_bar = conj(i kx) Nw_bar.  Output scaled by n^2 / w_j (ifft then
-// divides by n^2).
+// surface_tension.c:98-111, curl.c): from N_bar, the four spectra whose F^T
+// (= n^2 ifft(X / w)) gives the physical adjoints, as one batch:
+//   0 A_bar = -Nw_bar, 1 B_bar = -Nc_bar, 2 Fx_bar = conj(-i ky) Nw_bar,
+//   3 Fy_bar = conj(i kx) Nw_bar,
+// each scaled by n^2 / w_j (the inverse transform divides by n^2).
 // ---------------------------------------------------------------------------
 template <class R>
-__global__ void k_adj_tail(int op, const AdjPar<R> P, const cx<R>* __restrict__ nw, const cx<R>* __restrict__ nc,
-                           cx<R>* __restrict__ out) {
+__global__ void k_adj_tail4(const AdjPar<R> P, const cx<R>* __restrict__ nw, const cx<R>* __restrict__ nc,
+                            cx<R>* __restrict__ out, size_t ncx) {
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
   if (!mode_of(P, idx, m)) return;
   const R sc = (R)((double)P.n * (double)P.n) / m.wj;
-  cx<R> r;
-  if (op == 0) r = cscale(nw[idx], (R)-1);
-  else if (op == 1) r = cscale(nc[idx], (R)-1);
-  else if (op == 2) r = mul_ik(nw[idx], m.ky);    // conj(-i ky) = i ky
-  else r = mul_mik(nw[idx], m.kx);                // conj(i kx) = -i kx
-  out[idx] = cscale(r, sc);
+  const cx<R> a = nw[idx], b = nc[idx];
+  out[idx] = cscale(a, -sc);
+  out[ncx + idx] = cscale(b, -sc);
+  out[2 * ncx + idx] = cscale(mul_ik(a, m.ky), sc);   // conj(-i ky) = i ky
+  out[3 * ncx + idx] = cscale(mul_mik(a, m.kx), sc);  // conj(i kx) = -i kx
 }
 
-// lambda_bar, sigma_bar from N_c = -F[B] - lambda s2 k^2 F[f] (nonlin.c:240,251)
-template <class R>
-__global__ void k_adj_param_nc(const AdjPar<R> P, const cx<R>* __restrict__ nc, const cx<R>* __restrict__ Ff,
-                               double* acc) {
-  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  ModeIdx<R> m;
-  double dl = 0.0, ds = 0.0;
-  if (mode_of(P, idx, m)) {
-    const double d = -(double)m.ks * rdot(nc[idx], Ff[idx]);
-    dl = (double)P.s2 * d;
-    ds = (double)P.lam * P.ds2 * d;
-  }
-  block_acc3(0.0, dl, ds, acc);
-}
-
-// mu_bar_hat = T[(w_j / n^2) dfft(mu_bar)]; c_bar += s1 k^2 mu_bar_hat;
-// the spectrum of F[f]'s adjoint s2 mu_bar_hat - lambda s2 k^2 Nc_bar, scaled
-// n^2 / w_j for F^T; sigma_bar from the mu terms.
+// mu_bar_hat = T[(w_j / n^2) dfft(mu_bar)]; c_bar += s1 k^2 mu_bar_hat; the
+// spectrum of F[f]'s adjoint, s2 mu_bar_hat - lambda s2 k^2 Nc_bar, scaled
+// n^2 / w_j for F^T; lambda_bar and sigma_bar from the mu terms and from
+// N_c = -F[B] - lambda s2 k^2 F[f] (nonlin.c:240, 251).
 template <class R>
 __global__ void k_adj_mu(const AdjPar<R> P, const cx<R>* __restrict__ mub_hat_raw, const cx<R>* __restrict__ c,
                          const cx<R>* __restrict__ Ff, const cx<R>* __restrict__ nc, cx<R>* __restrict__ gc,
                          cx<R>* __restrict__ fbar_spec, double* acc) {
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
-  double ds = 0.0;
+  double dl = 0.0, ds = 0.0;
   if (mode_of(P, idx, m)) {
     const R n2 = (R)((double)P.n * (double)P.n);
     cx<R> mb = czero<R>();
@@ -194,14 +186,17 @@ __global__ void k_adj_mu(const AdjPar<R> P, const cx<R>* __restrict__ mub_hat_ra
     const cx<R> g = gc[idx];
     const R q = rmul(P.s1, m.ks);
     gc[idx] = mk<R>(g.x + q * mb.x, g.y + q * mb.y);
-    const cx<R> a = c[idx], f = Ff[idx];
-    ds = rdot(mb, mk<R>((R)(P.ds1 * (double)m.ks) * a.x + (R)P.ds2 * f.x, (R)(P.ds1 * (double)m.ks) * a.y + (R)P.ds2 * f.y));
+    const cx<R> a = c[idx], f = Ff[idx], nb = nc[idx];
+    const R d1 = (R)(P.ds1 * (double)m.ks);
+    ds = rdot(mb, mk<R>(d1 * a.x + (R)P.ds2 * f.x, d1 * a.y + (R)P.ds2 * f.y));
+    const double dn = -(double)m.ks * rdot(nb, f);
+    dl = (double)P.s2 * dn;
+    ds += (double)P.lam * P.ds2 * dn;
     const R ql = rmul(rmul(P.lam, P.s2), m.ks);
-    const cx<R> nb = nc[idx];
     const cx<R> fb = mk<R>(P.s2 * mb.x - ql * nb.x, P.s2 * mb.y - ql * nb.y);
     fbar_spec[idx] = cscale(fb, n2 / m.wj);
   }
-  block_acc3(0.0, 0.0, ds, acc);
+  block_acc3(0.0, dl, ds, acc);
 }
 
 // physical adjoints of the products (nonlin.c:62, 207; surface_tension.c:87-88):
@@ -213,7 +208,7 @@ __global__ void k_adj_mubar(const R* __restrict__ fxb, const R* __restrict__ fyb
     mub[k] = fxb[k] * cxp[k] + fyb[k] * cyp[k];
 }
 
-// in place: (Ab, Bb, Fxb, Fyb, fb) -> (u_bar, v_bar, wx_bar, wy_bar, ct_bar, cx_bar, cy_bar)
+// (Ab, Bb, Fxb, Fyb, fb) -> (u_bar, v_bar, wx_bar, wy_bar, ct_bar, cx_bar, cy_bar)
 //   u_bar = Ab wx + Bb cx, v_bar = Ab wy + Bb cy, wx_bar = Ab u, wy_bar = Ab v,
 //   cx_bar = Bb u + Fxb mu, cy_bar = Bb v + Fyb mu, ct_bar = fb f'(ct)
 template <class R> struct PhysFields {
@@ -239,30 +234,31 @@ __global__ void k_adj_products(const PhysFields<R> F, const PhysAdj<R> A, size_t
 }
 
 // accumulation of C^T(x_bar) = (w_j / n^2) dfft(x_bar) through the multipliers
-// of the forward fields into (gw, gc):
+// of the forward fields into (gw, gc), for the batch of seven x_bar spectra
+// (field k at xb + k ncx, order u, v, wx, wy, ct, cx, cy):
 //   u = T[i ky psi], v = T[-i kx psi], psi = w / k^2; wx = T[i kx w], wy = T[i ky w];
 //   ct = T[c], cx = T[i kx c], cy = T[i ky c]
 template <class R>
-__global__ void k_adj_acc(int op, const AdjPar<R> P, const cx<R>* __restrict__ xb_hat, cx<R>* __restrict__ gw,
-                          cx<R>* __restrict__ gc) {
+__global__ void k_adj_acc7(const AdjPar<R> P, const cx<R>* __restrict__ xb, cx<R>* __restrict__ gw,
+                           cx<R>* __restrict__ gc, size_t ncx) {
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
   if (!mode_of(P, idx, m) || !m.in) return;
-  const R n2 = (R)((double)P.n * (double)P.n);
-  const cx<R> x = cscale(xb_hat[idx], m.wj / n2);
-  cx<R> d;
-  if (op <= FOP_V) {
-    if (!(m.ks > (R)1e-12)) return;
-    const cx<R> pb = op == FOP_U ? mul_mik(x, m.ky) : mul_mik(x, -m.kx);
-    d = mk<R>(rdiv(pb.x, m.ks), rdiv(pb.y, m.ks));
-  } else if (op == FOP_WX) d = mul_mik(x, m.kx);
-  else if (op == FOP_WY) d = mul_mik(x, m.ky);
-  else if (op == FOP_CT) d = x;
-  else if (op == FOP_CX) d = mul_mik(x, m.kx);
-  else d = mul_mik(x, m.ky);
-  cx<R>* g = op <= FOP_WY ? gw : gc;
-  const cx<R> o = g[idx];
-  g[idx] = mk<R>(o.x + d.x, o.y + d.y);
+  const R sc = m.wj / (R)((double)P.n * (double)P.n);
+  cx<R> x[FOP_N];
+#pragma unroll
+  for (int k = 0; k < FOP_N; k++) x[k] = cscale(xb[k * ncx + idx], sc);
+  // psi_bar = conj(i ky) u_bar + conj(-i kx) v_bar, w_bar += psi_bar / k^2
+  cx<R> dw = czero<R>();
+  if (m.ks > (R)1e-12) {
+    const cx<R> a = mul_mik(x[FOP_U], m.ky), b = mul_mik(x[FOP_V], -m.kx);
+    dw = mk<R>(rdiv(a.x + b.x, m.ks), rdiv(a.y + b.y, m.ks));
+  }
+  const cx<R> ax = mul_mik(x[FOP_WX], m.kx), ay = mul_mik(x[FOP_WY], m.ky);
+  const cx<R> bx = mul_mik(x[FOP_CX], m.kx), by = mul_mik(x[FOP_CY], m.ky);
+  const cx<R> ow = gw[idx], oc = gc[idx];
+  gw[idx] = mk<R>(ow.x + dw.x + ax.x + ay.x, ow.y + dw.y + ax.y + ay.y);
+  gc[idx] = mk<R>(oc.x + x[FOP_CT].x + bx.x + by.x, oc.y + x[FOP_CT].y + bx.y + by.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -347,17 +343,30 @@ __global__ void k_adj_loss(const R* __restrict__ c, const R* __restrict__ cxp, c
   block_acc3(sj, 0.0, ssg, acc);
 }
 
-// (gw, gc) of the loss: gc = (w_j/n^2)(dfft(cb) - i kx dfft(cxb) - i ky dfft(cyb))
+// the untruncated c, i kx c, i ky c (free_energy.c) as one batch
 template <class R>
-__global__ void k_adj_loss_acc(int op, const AdjPar<R> P, const cx<R>* __restrict__ xb_hat, cx<R>* __restrict__ gc) {
+__global__ void k_adj_loss_prep3(const AdjPar<R> P, const cx<R>* __restrict__ c, cx<R>* __restrict__ out, size_t ncx) {
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
   if (!mode_of(P, idx, m)) return;
-  const R n2 = (R)((double)P.n * (double)P.n);
-  const cx<R> x = cscale(xb_hat[idx], m.wj / n2);
-  cx<R> d = op == 0 ? x : (op == 1 ? mul_mik(x, m.kx) : mul_mik(x, m.ky));
-  const cx<R> o = op == 0 ? czero<R>() : gc[idx];
-  gc[idx] = mk<R>(o.x + d.x, o.y + d.y);
+  const cx<R> a = c[idx];
+  out[idx] = a;
+  out[ncx + idx] = mul_ik(a, m.kx);
+  out[2 * ncx + idx] = mul_ik(a, m.ky);
+}
+
+// gc = (w_j/n^2)(dfft(cb) - i kx dfft(cxb) - i ky dfft(cyb)) from the batch of three; gw = 0
+template <class R>
+__global__ void k_adj_loss_acc3(const AdjPar<R> P, const cx<R>* __restrict__ xb, cx<R>* __restrict__ gc,
+                                cx<R>* __restrict__ gw, size_t ncx) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  if (!mode_of(P, idx, m)) return;
+  const R sc = m.wj / (R)((double)P.n * (double)P.n);
+  const cx<R> a = cscale(xb[idx], sc);
+  const cx<R> b = mul_mik(cscale(xb[ncx + idx], sc), m.kx), d = mul_mik(cscale(xb[2 * ncx + idx], sc), m.ky);
+  gc[idx] = mk<R>(a.x + b.x + d.x, a.y + b.y + d.y);
+  gw[idx] = czero<R>();
 }
 
 }  // namespace chns

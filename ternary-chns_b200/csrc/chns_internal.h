@@ -29,6 +29,10 @@ struct Launchers {
   int (*to_fftw)(chns_ctx* c, const void* s, double* dst);
   // free energy and kinetic energy reductions (double results in c->red)
   int (*diag)(chns_ctx* c);
+  // nb transforms at once: field b at real + b rs (R elements) and s + b ss
+  // (complex elements); scratch holds nb n x (n/2+1) complex fields
+  int (*dfftb)(chns_ctx* c, const void* real, size_t rs, void* s, size_t ss, int nb, void* scratch);
+  int (*ifftb)(chns_ctx* c, const void* s, size_t ss, void* real, size_t rs, int nb, void* scratch);
 };
 
 const Launchers* launchers_f64(int logn);
@@ -46,6 +50,7 @@ struct chns_ctx {
   // device memory
   void* state[3];
   void* saved[3];
+  void* nstar[3];   // when set, stage 2 also stores N(u*) there (adjoint recording)
   void* nw;
   void* g[12];
   void* h[7];

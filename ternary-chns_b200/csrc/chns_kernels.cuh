@@ -67,6 +67,9 @@ template <class R> struct Bufs {
   cx<R>* sw;
   cx<R>* s1;
   cx<R>* s2;
+  cx<R>* xw;   // stage 2: N(u*) of w, c1, c2 stored here when not null
+  cx<R>* x1;
+  cx<R>* x2;
   cx<R>* nw;
   cx<R>* g[NG];
   cx<R>* h[NH];
@@ -617,6 +620,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
   for (int fld = 0; fld < (MODEL == MODEL_TERNARY ? 2 : 1); fld++) {
     cx<R>* cst = fld == 0 ? B.c1 : B.c2;
     cx<R>* csv = fld == 0 ? B.s1 : B.s2;
+    cx<R>* cx_out = fld == 0 ? B.x1 : B.x2;
     // F[f(c)] (binary) or F[mu^F_i] (ternary)
     if (MODEL == MODEL_BINARY) load_row<N>(f, B.h[HF], row, live, t);
     else load_row_pair<N>(f, B.h[HF], row, fld, live, t);
@@ -670,6 +674,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
       if (STAGE == 2) sv = live ? csv[idx] : czero<R>();
       c[m] = etd<STAGE>(c[m], nl, &sv, e, z1, z2);
       if (STAGE == 1 && live) csv[idx] = sv;
+      if (STAGE == 2 && cx_out && live) cx_out[idx] = nl;
       if (F32 && row == 0 && t == 0 && m == 0) {
         double* st = P.k0 + 2 * (1 + fld);
         double* sd = P.k0 + 2 * (4 + fld);
@@ -735,6 +740,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
     const R e = cf[0 * cstride + am], z1 = cf[1 * cstride + am], z2 = cf[2 * cstride + am];
     cx<R> sv;
     if (STAGE == 2) sv = live ? B.sw[idx] : czero<R>();
+    if (STAGE == 2 && B.xw && live) B.xw[idx] = a[m];
     b[m] = etd<STAGE>(b[m], a[m], &sv, e, z1, z2);
     if (STAGE == 1 && live) B.sw[idx] = sv;
     if (F32 && row == 0 && t == 0 && m == 0) {
@@ -788,11 +794,14 @@ __global__ void k_s_to_fftw(const cx<R>* __restrict__ src, double2* __restrict__
   }
 }
 
-// real field (n x n, R, row-major, i = x) -> H layout (plain): y-r2c of x-row pairs
+// real field (n x n, R, row-major, i = x) -> H layout (plain): y-r2c of x-row pairs.
+// Batched over blockIdx.y: field b reads x + b xs and writes H + b hs.
 template <int N, class R, int GPC>
 __global__ void __launch_bounds__(GPC * (N / 16)) k_row_r2c_plain(const R* __restrict__ x, cx<R>* __restrict__ H,
-                                                                  const cx<R>* __restrict__ tw) {
+                                                                  const cx<R>* __restrict__ tw, size_t xs, size_t hs) {
   constexpr int NT = N / 16;
+  x += blockIdx.y * xs;
+  H += blockIdx.y * hs;
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), tw, t);
@@ -810,11 +819,14 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_row_r2c_plain(const R* __res
   row_r2c_store<N>(v, H, N, i0, live, t, sh, TW);
 }
 
-// S/H layout row j': x transform (DIR), optional scale
+// S/H layout row j': x transform (DIR), optional scale; batched over blockIdx.y
 template <int N, class R, int GPC, int DIR>
 __global__ void __launch_bounds__(GPC * (N / 16)) k_col_plain(const cx<R>* __restrict__ src, cx<R>* __restrict__ dst,
-                                                              int nrows, R scale, const cx<R>* __restrict__ tw) {
+                                                              int nrows, R scale, const cx<R>* __restrict__ tw,
+                                                              size_t ss, size_t ds) {
   constexpr int NT = N / 16;
+  src += blockIdx.y * ss;
+  dst += blockIdx.y * ds;
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), tw, t);
@@ -830,11 +842,13 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_col_plain(const cx<R>* __res
   store_row<N>(v, dst, row, live, t);
 }
 
-// plain layout (rows 0..n/2) -> real field: y-c2r of x-row pairs
+// plain layout (rows 0..n/2) -> real field: y-c2r of x-row pairs; batched over blockIdx.y
 template <int N, class R, int GPC>
 __global__ void __launch_bounds__(GPC * (N / 16)) k_row_c2r_plain(const cx<R>* __restrict__ G, R* __restrict__ x,
-                                                                  const cx<R>* __restrict__ tw) {
+                                                                  const cx<R>* __restrict__ tw, size_t gs, size_t xs) {
   constexpr int NT = N / 16;
+  G += blockIdx.y * gs;
+  x += blockIdx.y * xs;
   constexpr int JT = N / 2;
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;

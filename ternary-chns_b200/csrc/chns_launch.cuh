@@ -67,6 +67,9 @@ template <class R> Bufs<R> make_bufs(const chns_ctx* c) {
   B.sw = (cx<R>*)c->saved[0];
   B.s1 = (cx<R>*)c->saved[1];
   B.s2 = (cx<R>*)c->saved[2];
+  B.xw = (cx<R>*)c->nstar[0];
+  B.x1 = (cx<R>*)c->nstar[1];
+  B.x2 = (cx<R>*)c->nstar[2];
   B.nw = (cx<R>*)c->nw;
   for (int k = 0; k < NG; k++) B.g[k] = (cx<R>*)c->g[k];
   for (int k = 0; k < NH; k++) B.h[k] = (cx<R>*)c->h[k];
@@ -222,30 +225,45 @@ template <int N, class R> int truncate_impl(chns_ctx* c, void* s) {
   return 1;
 }
 
-template <int N, class R> int dfft_impl(chns_ctx* c, const void* real, void* s) {
+// batched plain transforms: nb fields at strides (in elements of their type);
+// scratch holds nb H-layout fields of n x (n/2+1) complex
+template <int N, class R> int dfftb_impl(chns_ctx* c, const void* real, size_t rs, void* s, size_t ss, int nb,
+                                         void* scratch) {
   using S = Sizes<N, R>;
+  constexpr size_t HS = (size_t)N * (N / 2 + 1);
   auto k1 = k_row_r2c_plain<N, R, S::GPC>;
   set_smem(k1, S::FFT_SMEM);
-  k1<<<S::grid_rows(N / 2), S::THREADS, S::FFT_SMEM, c->stream>>>((const R*)real, (cx<R>*)c->h[HAB],
-                                                                   (const cx<R>*)c->tw);
+  k1<<<dim3(S::grid_rows(N / 2), nb), S::THREADS, S::FFT_SMEM, c->stream>>>((const R*)real, (cx<R>*)scratch,
+                                                                             (const cx<R>*)c->tw, rs, HS);
   auto k2 = k_col_plain<N, R, S::GPC, -1>;
   set_smem(k2, S::FFT_SMEM);
-  k2<<<S::grid_rows(N / 2 + 1), S::THREADS, S::FFT_SMEM, c->stream>>>(
-      (const cx<R>*)c->h[HAB], (cx<R>*)s, N / 2 + 1, (R)1, (const cx<R>*)c->tw);
+  k2<<<dim3(S::grid_rows(N / 2 + 1), nb), S::THREADS, S::FFT_SMEM, c->stream>>>(
+      (const cx<R>*)scratch, (cx<R>*)s, N / 2 + 1, (R)1, (const cx<R>*)c->tw, HS, ss);
   return 2;
 }
 
-template <int N, class R> int ifft_impl(chns_ctx* c, const void* s, void* real) {
+template <int N, class R> int ifftb_impl(chns_ctx* c, const void* s, size_t ss, void* real, size_t rs, int nb,
+                                         void* scratch) {
   using S = Sizes<N, R>;
+  constexpr size_t HS = (size_t)N * (N / 2 + 1);
   auto k1 = k_col_plain<N, R, S::GPC, +1>;
   set_smem(k1, S::FFT_SMEM);
-  k1<<<S::grid_rows(N / 2 + 1), S::THREADS, S::FFT_SMEM, c->stream>>>(
-      (const cx<R>*)s, (cx<R>*)c->h[HF], N / 2 + 1, (R)(1.0 / ((double)N * (double)N)), (const cx<R>*)c->tw);
+  k1<<<dim3(S::grid_rows(N / 2 + 1), nb), S::THREADS, S::FFT_SMEM, c->stream>>>(
+      (const cx<R>*)s, (cx<R>*)scratch, N / 2 + 1, (R)(1.0 / ((double)N * (double)N)), (const cx<R>*)c->tw, ss, HS);
   auto k2 = k_row_c2r_plain<N, R, S::GPC>;
   const size_t sm2 = S::TW + RowSmem<N, R, S::GPC>::bytes(N / 2, 0);
   set_smem(k2, sm2);
-  k2<<<S::grid_rows(N / 2), S::THREADS, sm2, c->stream>>>((const cx<R>*)c->h[HF], (R*)real, (const cx<R>*)c->tw);
+  k2<<<dim3(S::grid_rows(N / 2), nb), S::THREADS, sm2, c->stream>>>((const cx<R>*)scratch, (R*)real,
+                                                                     (const cx<R>*)c->tw, HS, rs);
   return 2;
+}
+
+template <int N, class R> int dfft_impl(chns_ctx* c, const void* real, void* s) {
+  return dfftb_impl<N, R>(c, real, 0, s, 0, 1, c->h[HAB]);
+}
+
+template <int N, class R> int ifft_impl(chns_ctx* c, const void* s, void* real) {
+  return ifftb_impl<N, R>(c, s, 0, real, 0, 1, c->h[HF]);
 }
 
 template <int N, class R> int from_fftw_impl(chns_ctx* c, const double* src, void* s) {
@@ -297,8 +315,9 @@ template <int N, class R> int diag_impl(chns_ctx* c) {
 }
 
 template <int N, class R> const Launchers* make_launchers() {
-  static const Launchers L = {stage_impl<N, R>, truncate_impl<N, R>, dfft_impl<N, R>, ifft_impl<N, R>,
-                              from_fftw_impl<N, R>, to_fftw_impl<N, R>, diag_impl<N, R>};
+  static const Launchers L = {stage_impl<N, R>,     truncate_impl<N, R>, dfft_impl<N, R>,
+                              ifft_impl<N, R>,      from_fftw_impl<N, R>, to_fftw_impl<N, R>,
+                              diag_impl<N, R>,      dfftb_impl<N, R>,     ifftb_impl<N, R>};
   return &L;
 }
 

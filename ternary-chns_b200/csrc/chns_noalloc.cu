@@ -98,8 +98,8 @@ template <int N> int run(const double* real, double* spec, const DeviceSetup* s,
     cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
     cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   }
-  k1<<<(N / 2 + GPC - 1) / GPC, THREADS, SMEM, st>>>(real, h, tw);
-  k2<<<(N / 2 + 1 + GPC - 1) / GPC, THREADS, SMEM, st>>>(h, sl, N / 2 + 1, 1.0, tw);
+  k1<<<(N / 2 + GPC - 1) / GPC, THREADS, SMEM, st>>>(real, h, tw, 0, 0);
+  k2<<<(N / 2 + 1 + GPC - 1) / GPC, THREADS, SMEM, st>>>(h, sl, N / 2 + 1, 1.0, tw, 0, 0);
   dim3 grid((N / 2 + 1 + 31) / 32, (N + 31) / 32);
   chns::k_s_to_fftw<double><<<grid, dim3(32, 8), 0, st>>>(sl, (double2*)spec, N);
   return cudaGetLastError() == cudaSuccess ? CHNS_OK : CHNS_ERR_CUDA;
