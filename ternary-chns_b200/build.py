@@ -37,12 +37,12 @@ def _headers():
         [os.path.join(ROOT, "include", "chns.h")]
 
 
-def _compile(src: str, verbose: bool) -> str:
-    obj = os.path.join(BUILD, os.path.basename(src).replace(".cu", ".o"))
+def _compile(src: str, verbose: bool, build_dir: str = BUILD, defines: tuple = ()) -> str:
+    obj = os.path.join(build_dir, os.path.basename(src).replace(".cu", ".o"))
     deps = [src] + _headers()
     if os.path.isfile(obj) and all(os.path.getmtime(d) <= os.path.getmtime(obj) for d in deps):
         return obj
-    cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, *[f"-D{d}" for d in defines], "-c", src, "-o", obj]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -54,21 +54,24 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
-def build(verbose: bool = False, jobs: int | None = None) -> str:
-    os.makedirs(BUILD, exist_ok=True)
-    os.makedirs(OUTDIR, exist_ok=True)
+def build(verbose: bool = False, jobs: int | None = None, defines: tuple = (), build_dir: str = BUILD,
+          lib: str = LIB) -> str:
+    """Compiles and links the library; `defines` (NAME=VALUE) and the build and
+    output paths are for variant builds such as the autotuner's."""
+    os.makedirs(build_dir, exist_ok=True)
+    os.makedirs(os.path.dirname(lib), exist_ok=True)
     srcs = _sources()
     with cf.ThreadPoolExecutor(max_workers=jobs or min(len(srcs), os.cpu_count() or 4)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
-    if os.path.isfile(LIB) and all(os.path.getmtime(o) <= os.path.getmtime(LIB) for o in objs):
-        return LIB
-    tmp = LIB + ".tmp"
+        objs = list(ex.map(lambda s: _compile(s, verbose, build_dir, tuple(defines)), srcs))
+    if os.path.isfile(lib) and all(os.path.getmtime(o) <= os.path.getmtime(lib) for o in objs):
+        return lib
+    tmp = lib + ".tmp"
     cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":

@@ -4,16 +4,25 @@
 
 #include "chns_internal.h"
 #include "chns_kernels.cuh"
+#include "chns_tuned.h"
 #include "chns_diag.cuh"
 
 namespace chns {
 
-// groups (transforms) per CTA: 256 threads for N >= 256, fewer for tiny grids
-template <int N> constexpr int gpc_of() {
+// groups (transforms of one row) per CTA: the tuned threads per CTA of
+// chns_tuned.h (or CHNS_CTA_THREADS for an autotuner build) over n/16 threads per
+// transform, at least 1 and at most n/16
+template <int N, class R> constexpr int gpc_of() {
   constexpr int nt = N / 16;
-  constexpr int a = 256 / nt;
-  constexpr int b = N / 16;
-  return a < b ? (a < 1 ? 1 : a) : (b < 1 ? 1 : b);
+  constexpr int lg = N >= 4096 ? 7 : N >= 2048 ? 6 : N >= 1024 ? 5 : N >= 512 ? 4 : N >= 256 ? 3 : N >= 128 ? 2
+                   : N >= 64 ? 1 : 0;
+#ifdef CHNS_CTA_THREADS
+  constexpr int threads = CHNS_CTA_THREADS;
+#else
+  constexpr int threads = sizeof(R) == 4 ? kCtaThreadsF32[lg] : kCtaThreadsF64[lg];
+#endif
+  constexpr int a = threads / nt;
+  return a < 1 ? 1 : (a > nt ? nt : a);
 }
 
 template <class R> Par<R> make_par(const chns_ctx* c) {
@@ -81,7 +90,7 @@ template <class K> static void set_smem(K kern, size_t bytes) {
 }
 
 template <int N, class R> struct Sizes {
-  static constexpr int GPC = gpc_of<N>();
+  static constexpr int GPC = gpc_of<N, R>();
   static constexpr int NT = N / 16;
   static constexpr int THREADS = GPC * NT;
   static constexpr size_t TW = tw_smem_per_thread<N, R>() * THREADS;  // precomputed twiddles
