@@ -69,10 +69,15 @@ void dcoef_dc(double c, double h, double* o) {
 //   spec: NSPEC S-layout fields in one allocation (slot k at k ncx complex)
 //   phys: NPHYS real n x n fields in one allocation
 //   bscr: scratch of the batched transforms (7 fields)
-//   seg:  per step of the current segment, 8 fields: u_n, u*, N(u_n), N(u*)
+//   seg:  per step of a segment, 8 fields: u_n, u*, N(u_n), N(u*); two
+//         segments' worth when memory allows, so that the recompute of one
+//         segment (side stream) overlaps the reversal of the next
 struct chns_adj {
-  int cap_states;
+  int cap_states;   // slots allocated (ckpt or 2 ckpt)
+  int seg_len;      // ckpt the slots were laid out for
   void* seg;
+  cudaStream_t side;
+  cudaEvent_t ev_sweep, ev_ready[2], ev_free[2];
   void** ckpt;
   double** ckptk0;
   int nckpt_cap;
@@ -230,12 +235,28 @@ int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
     if (cudaMemcpy(a->dcoef, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
       return CHNS_ERR_CUDA;
   }
-  if (seglen > a->cap_states) {
+  if (!a->side) {
+    if (cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking) != cudaSuccess) return CHNS_ERR_CUDA;
+    ACK(cudaEventCreateWithFlags(&a->ev_sweep, cudaEventDisableTiming));
+    for (int b = 0; b < 2; b++) {
+      ACK(cudaEventCreateWithFlags(&a->ev_ready[b], cudaEventDisableTiming));
+      ACK(cudaEventCreateWithFlags(&a->ev_free[b], cudaEventDisableTiming));
+    }
+  }
+  if (seglen != a->seg_len || a->cap_states < seglen) {
+    // two segments of slots if they fit, else one
     if (a->seg) cudaFree(a->seg);
     a->seg = nullptr;
     a->cap_states = 0;
-    if (cudaMalloc(&a->seg, SLOT_FIELDS * fbytes * seglen) != cudaSuccess) return CHNS_ERR_NOMEM;
-    a->cap_states = seglen;
+    a->seg_len = 0;
+    if (cudaMalloc(&a->seg, SLOT_FIELDS * fbytes * 2 * (size_t)seglen) == cudaSuccess) {
+      a->cap_states = 2 * seglen;
+    } else {
+      cudaGetLastError();
+      if (cudaMalloc(&a->seg, SLOT_FIELDS * fbytes * (size_t)seglen) != cudaSuccess) return CHNS_ERR_NOMEM;
+      a->cap_states = seglen;
+    }
+    a->seg_len = seglen;
   }
   if (nckpt > a->nckpt_cap) {
     for (int k = 0; k < a->nckpt_cap; k++) {
@@ -296,10 +317,11 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
   char* segbase = (char*)a->seg;
   const size_t slot = SLOT_FIELDS * bytes;
   const int nlast = (nseg - 1) * ckpt;
+  const size_t lastbuf = a->cap_states >= 2 * ckpt ? (size_t)((nseg - 1) % 2) * ckpt : 0;
   if ((rc = snapshot_save(c, a->ckpt[nseg], a->ckptk0[nseg]))) return rc;
   for (int n = 0; n < nsteps; n++) {
     if (n % ckpt == 0 && (rc = snapshot_save(c, a->ckpt[n / ckpt], a->ckptk0[n / ckpt]))) return rc;
-    rc = n >= nlast ? record_step(c, segbase + (size_t)(n - nlast) * slot, bytes) : chns_step(c, 1);
+    rc = n >= nlast ? record_step(c, segbase + (lastbuf + n - nlast) * slot, bytes) : chns_step(c, 1);
     if (rc) return rc;
   }
   // loss at the final state and its gradient (free_energy.c:3-157: c and grad c untruncated)
@@ -329,22 +351,46 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
     }
     cudaGetLastError();
   }
-  // reverse sweep: each segment but the last is recomputed from its checkpoint,
-  // recording its steps, then its steps are reversed
-  for (int s = nseg - 1; s >= 0; s--) {
-    const int n0 = s * ckpt, len = (n0 + ckpt <= nsteps) ? ckpt : nsteps - n0;
-    if (s != nseg - 1) {
-      if ((rc = snapshot_load(c, a->ckpt[s], a->ckptk0[s]))) return rc;
-      for (int k = 0; k < len; k++)
-        if ((rc = record_step(c, segbase + (size_t)k * slot, bytes))) return rc;
-    }
+  // reverse sweep: each segment but the last is recomputed from its checkpoint
+  // on the side stream, recording its steps into segment buffer s % nbuf, then
+  // its steps are reversed on the context stream.  With two buffers the
+  // recompute of segment s-1 runs while segment s is reversed.
+  const int nbuf = a->cap_states >= 2 * ckpt ? 2 : 1;
+  cudaStream_t side = a->side;
+  ACK(cudaEventRecord(a->ev_sweep, st));
+  ACK(cudaStreamWaitEvent(side, a->ev_sweep, 0));
+  auto recompute = [&](int s) -> int {
+    const int b = s % nbuf, len = (s * ckpt + ckpt <= nsteps) ? ckpt : nsteps - s * ckpt;
+    if (s + nbuf <= nseg - 1) ACK(cudaStreamWaitEvent(side, a->ev_free[b], 0));
+    c->stream = side;
+    int r = snapshot_load(c, a->ckpt[s], a->ckptk0[s]);
+    for (int k = 0; k < len && !r; k++) r = record_step(c, segbase + ((size_t)b * ckpt + k) * slot, bytes);
+    c->stream = st;
+    if (r) return r;
+    ACK(cudaEventRecord(a->ev_ready[b], side));
+    return CHNS_OK;
+  };
+  auto reverse = [&](int s) -> int {
+    const int b = s % nbuf, len = (s * ckpt + ckpt <= nsteps) ? ckpt : nsteps - s * ckpt;
+    if (s != nseg - 1) ACK(cudaStreamWaitEvent(st, a->ev_ready[b], 0));
     for (int k = len - 1; k >= 0; k--) {
-      ACK(cudaMemcpyAsync(A.S(CUW), segbase + (size_t)k * slot, slot, cudaMemcpyDeviceToDevice, st));
+      ACK(cudaMemcpyAsync(A.S(CUW), segbase + ((size_t)b * ckpt + k) * slot, slot, cudaMemcpyDeviceToDevice, st));
       if (a->rev) {
         ACK(cudaGraphLaunch(a->rev, st));
       } else {
         A.reverse_step(coef, dcoef);
       }
+    }
+    ACK(cudaEventRecord(a->ev_free[b], st));
+    return CHNS_OK;
+  };
+  for (int s = nseg - 1; s >= 0; s--) {
+    if (nbuf == 2) {
+      if (s > 0 && (rc = recompute(s - 1))) return rc;
+      if ((rc = reverse(s))) return rc;
+    } else {
+      if ((rc = reverse(s))) return rc;
+      if (s > 0 && (rc = recompute(s - 1))) return rc;
     }
   }
   ACK(cudaGetLastError());
@@ -379,6 +425,15 @@ void chns_adj_free(chns_ctx* c) {
   chns_adj* a = c->adj;
   if (!a) return;
   if (a->rev) cudaGraphExecDestroy(a->rev);
+  if (a->side) {
+    cudaStreamSynchronize(a->side);
+    cudaStreamDestroy(a->side);
+    cudaEventDestroy(a->ev_sweep);
+    for (int b = 0; b < 2; b++) {
+      cudaEventDestroy(a->ev_ready[b]);
+      cudaEventDestroy(a->ev_free[b]);
+    }
+  }
   if (a->spec) cudaFree(a->spec);
   if (a->phys) cudaFree(a->phys);
   if (a->bscr) cudaFree(a->bscr);

@@ -136,3 +136,24 @@ def test_autograd_function_wrapper(setup):
     fd = (forward_loss(C, p, [w0, c0 + h * d]) - forward_loss(C, p, [w0, c0 - h * d])) / (2 * h)
     ad = float(torch.sum(grad * torch.from_numpy(d.view(np.float64).reshape(d.shape + (2,)))))
     assert abs(ad - fd) <= 1e-6 * abs(fd)
+
+
+def test_checkpoint_interval_does_not_change_gradients(setup):
+    """Every checkpoint interval (one segment, several, one step per segment)
+    reverses the same trajectory: results agree to round-off."""
+    C, g, p = setup
+    w0, c0 = g["init"]
+    out = {}
+    with C.Context(p) as c:
+        c.set_state(w0, c0)
+        for k in (1, 3, 5, 12, 40):
+            out[k] = c.adjoint(STEPS, k)
+        # the state is unchanged by the adjoint
+        w1, c1 = c.get_state()
+    assert np.array_equal(w1, w0) and np.array_equal(c1, c0)
+    J0, gw0, gc0, gp0 = out[STEPS]
+    for k, (J, gw, gc, gp) in out.items():
+        assert abs(J - J0) <= 1e-14 * abs(J0), k
+        assert np.linalg.norm(gc - gc0) <= 1e-13 * np.linalg.norm(gc0), k
+        assert np.linalg.norm(gw - gw0) <= 1e-13 * max(np.linalg.norm(gw0), 1e-300), k
+        assert np.allclose(gp, gp0, rtol=1e-12, atol=0), k
