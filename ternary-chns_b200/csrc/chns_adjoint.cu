@@ -76,8 +76,9 @@ struct chns_adj {
   int cap_states;   // slots allocated (ckpt or 2 ckpt)
   int seg_len;      // ckpt the slots were laid out for
   void* seg;
-  cudaStream_t side;
-  cudaEvent_t ev_sweep, ev_ready[2], ev_free[2];
+  cudaStream_t side;  // segment recompute
+  cudaStream_t fork;  // parallel branch of the captured reverse step
+  cudaEvent_t ev_sweep, ev_ready[2], ev_free[2], ev_fork, ev_join;
   void** ckpt;
   double** ckptk0;
   int nckpt_cap;
@@ -93,20 +94,24 @@ struct chns_adj {
 
 namespace {
 
-// spectral slots
+// Two field sets (0: the state u*, 1: the state u_n of a reversed step), each
+// with its own spectral batch, scratch and F[f(c_t)] and its own physical
+// forward fields, so that the forward fields at u_n are computed on a branch
+// parallel to the transposed right-hand side at u*.
+constexpr int SSET = 9;                      // spectral fields per set
+enum { SB = 0, SXo = 7, SFFo = 8 };           // batch of 7, scratch, F[f]
 enum {
-  SB0 = 0,               // batch of 7 (SB0 .. SB0+6)
-  SFF = 7, SX, SY,       // F[f(c_t)], scratch
-  SNBW, SNBC,            // N*_bar
-  SNBAW, SNBAC,          // N(u_n)_bar
-  SGW, SGC,              // running gradient (w_bar, c_bar)
+  SY = 2 * SSET,                             // scratch (f_bar spectrum)
+  SNBW, SNBC,                                // N*_bar
+  SNBAW, SNBAC,                              // N(u_n)_bar
+  SGW, SGC,                                  // running gradient (w_bar, c_bar)
   // current step, in the segment slot layout: u_n, u*, N(u_n), N(u*)
   CUW, CUC, CSW, CSC, CNW, CNC, CXW, CXC,
   NSPEC
 };
-// physical slots
-enum { PU = 0, PV, PWX, PWY, PCT, PCX, PCY, PMU, PFB, PAB, PBB, PFXB, PFYB, PUB, PVB, PWXB, PWYB, PCTB, PCXB, PCYB,
-       NPHYS };
+constexpr int PSET = 9;                                    // physical fields per set
+enum { PU = 0, PV, PWX, PWY, PCT, PCX, PCY, PMU, PFT };     // forward fields, f(c_t)
+enum { PFB = 2 * PSET, PAB, PBB, PFXB, PFYB, PUB, PVB, PWXB, PWYB, PCTB, PCXB, PCYB, NPHYS };
 constexpr int SLOT_FIELDS = 8;
 
 template <class R> struct Adj {
@@ -119,49 +124,79 @@ template <class R> struct Adj {
 
   cx<R>* S(int k) const { return (cx<R>*)a->spec + (size_t)k * ncx; }
   R* F(int k) const { return (R*)a->phys + (size_t)k * nn; }
+  cx<R>* SS(int set, int k) const { return S(set * SSET + k); }
+  R* FS(int set, int k) const { return F(set * PSET + k); }
+  void* scratch(int set) const { return (char*)a->bscr + (size_t)set * FOP_N * ncx * sizeof(cx<R>); }
 
-  void ifft(const cx<R>* s, R* x, int nb) { c->L->ifftb(c, s, ncx, x, nn, nb, a->bscr); }
-  void dfft(const R* x, cx<R>* s, int nb) { c->L->dfftb(c, x, nn, s, ncx, nb, a->bscr); }
+  // batched transforms on stream s with the scratch of a field set
+  void ifft(cudaStream_t s, int set, const cx<R>* in, R* x, int nb) {
+    c->stream = s;
+    c->L->ifftb(c, in, ncx, x, nn, nb, scratch(set));
+    c->stream = st;
+  }
+  void dfft(cudaStream_t s, int set, const R* x, cx<R>* out, int nb) {
+    c->stream = s;
+    c->L->dfftb(c, x, nn, out, ncx, nb, scratch(set));
+    c->stream = st;
+  }
 
-  // (gw, gc) += J_N(w, cc)^T (nbw, nbc); parameter partials into acc[4..6]
-  void vjp(const cx<R>* w, const cx<R>* cc, const cx<R>* nbw, const cx<R>* nbc, cx<R>* gw, cx<R>* gc) {
+  // forward fields of the right-hand side at (w, cc) into field set `set`
+  void fields(cudaStream_t s, int set, const cx<R>* w, const cx<R>* cc) {
+    k_adj_fwd_prep7<R><<<blocks_s, 256, 0, s>>>(P, w, cc, SS(set, SB), ncx);
+    ifft(s, set, SS(set, SB), FS(set, PU), FOP_N);
+    k_adj_bulk<R><<<blocks_p, 256, 0, s>>>(FS(set, PCT), FS(set, PFT), nn);
+    dfft(s, set, FS(set, PFT), SS(set, SFFo), 1);
+    k_adj_mu_prep<R><<<blocks_s, 256, 0, s>>>(P, cc, SS(set, SFFo), SS(set, SXo));
+    ifft(s, set, SS(set, SXo), FS(set, PMU), 1);
+  }
+
+  // (gw, gc) += J_N(state)^T (nbw, nbc) with the forward fields of set `set`
+  // (c_hat of the state: cc); parameter partials into acc[4..6].  Scratch of set 0.
+  void transpose_rhs(int set, const cx<R>* cc, const cx<R>* nbw, const cx<R>* nbc, cx<R>* gw, cx<R>* gc) {
     double* pacc = a->acc + 4;
-    // forward fields at the state
-    k_adj_fwd_prep7<R><<<blocks_s, 256, 0, st>>>(P, w, cc, S(SB0), ncx);
-    ifft(S(SB0), F(PU), FOP_N);
-    k_adj_bulk<R><<<blocks_p, 256, 0, st>>>(F(PCT), F(PFB), nn);
-    dfft(F(PFB), S(SFF), 1);
-    k_adj_mu_prep<R><<<blocks_s, 256, 0, st>>>(P, cc, S(SFF), S(SX));
-    ifft(S(SX), F(PMU), 1);
     // transposed spectral tail -> A_bar, B_bar, Fx_bar, Fy_bar
-    k_adj_tail4<R><<<blocks_s, 256, 0, st>>>(P, nbw, nbc, S(SB0), ncx);
-    ifft(S(SB0), F(PAB), 4);
+    k_adj_tail4<R><<<blocks_s, 256, 0, st>>>(P, nbw, nbc, SS(0, SB), ncx);
+    ifft(st, 0, SS(0, SB), F(PAB), 4);
     // mu_bar -> c_bar (s1 k^2), f_bar, lambda and sigma partials
-    k_adj_mubar<R><<<blocks_p, 256, 0, st>>>(F(PFXB), F(PFYB), F(PCX), F(PCY), F(PUB), nn);
-    dfft(F(PUB), S(SX), 1);
-    k_adj_mu<R><<<blocks_s, 256, 0, st>>>(P, S(SX), cc, S(SFF), nbc, gc, S(SY), pacc);
-    ifft(S(SY), F(PFB), 1);
+    k_adj_mubar<R><<<blocks_p, 256, 0, st>>>(F(PFXB), F(PFYB), FS(set, PCX), FS(set, PCY), F(PUB), nn);
+    dfft(st, 0, F(PUB), SS(0, SXo), 1);
+    k_adj_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(0, SXo), cc, SS(set, SFFo), nbc, gc, S(SY), pacc);
+    ifft(st, 0, S(SY), F(PFB), 1);
     // products, then C^T of the seven forward fields
-    PhysFields<R> pf{F(PU), F(PV), F(PWX), F(PWY), F(PCT), F(PCX), F(PCY), F(PMU)};
+    PhysFields<R> pf{FS(set, PU), FS(set, PV), FS(set, PWX), FS(set, PWY), FS(set, PCT), FS(set, PCX),
+                     FS(set, PCY), FS(set, PMU)};
     PhysAdj<R> pa{F(PAB), F(PBB), F(PFXB), F(PFYB), F(PFB), F(PUB), F(PVB), F(PWXB), F(PWYB), F(PCTB), F(PCXB),
                   F(PCYB)};
     k_adj_products<R><<<blocks_p, 256, 0, st>>>(pf, pa, nn);
-    dfft(F(PUB), S(SB0), FOP_N);
-    k_adj_acc7<R><<<blocks_s, 256, 0, st>>>(P, S(SB0), gw, gc, ncx);
+    dfft(st, 0, F(PUB), SS(0, SB), FOP_N);
+    k_adj_acc7<R><<<blocks_s, 256, 0, st>>>(P, SS(0, SB), gw, gc, ncx);
   }
 
   // one reversed step from the current-step slots (CUW..CXC): the transposed
-  // stage 2, right-hand side at u*, stage 1 and right-hand side at u_n
-  void reverse_step(const R* coef, const double* dcoef) {
+  // stage 2, right-hand side at u*, stage 1 and right-hand side at u_n.  With a
+  // fork stream the forward fields at u_n are built on a parallel branch.
+  void reverse_step(const R* coef, const double* dcoef, cudaStream_t fork) {
     double* pacc = a->acc + 4;
     cx<R>* gw = S(SGW);
     cx<R>* gc = S(SGC);
+    if (fork) {
+      cudaEventRecord(a->ev_fork, st);
+      cudaStreamWaitEvent(fork, a->ev_fork, 0);
+      fields(fork, 1, S(CUW), S(CUC));
+      cudaEventRecord(a->ev_join, fork);
+    }
     k_adj_etd2<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(CXW), S(CXC), S(CNW), S(CNC), S(SNBW),
                                             S(SNBC), S(SNBAW), S(SNBAC), pacc);
-    vjp(S(CSW), S(CSC), S(SNBW), S(SNBC), gw, gc);
+    fields(st, 0, S(CSW), S(CSC));
+    transpose_rhs(0, S(CSC), S(SNBW), S(SNBC), gw, gc);
     k_adj_etd1<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(CUW), S(CUC), S(CNW), S(CNC), S(SNBAW),
                                             S(SNBAC), pacc);
-    vjp(S(CUW), S(CUC), S(SNBAW), S(SNBAC), gw, gc);
+    if (fork) {
+      cudaStreamWaitEvent(st, a->ev_join, 0);
+    } else {
+      fields(st, 1, S(CUW), S(CUC));
+    }
+    transpose_rhs(1, S(CUC), S(SNBAW), S(SNBAC), gw, gc);
   }
 };
 
@@ -212,7 +247,7 @@ int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
   if (!a->dcoef) {
     if (cudaMalloc(&a->spec, NSPEC * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMalloc(&a->phys, NPHYS * nn * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
-    if (cudaMalloc(&a->bscr, FOP_N * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->bscr, 2 * FOP_N * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMalloc((void**)&a->acc, 8 * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
     // derivative tables of the ETD coefficients: d/dnu (w), d/dlambda, d/dsigma (c)
     const int nr = c->nr;
@@ -237,7 +272,10 @@ int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
   }
   if (!a->side) {
     if (cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking) != cudaSuccess) return CHNS_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&a->fork, cudaStreamNonBlocking) != cudaSuccess) return CHNS_ERR_CUDA;
     ACK(cudaEventCreateWithFlags(&a->ev_sweep, cudaEventDisableTiming));
+    ACK(cudaEventCreateWithFlags(&a->ev_fork, cudaEventDisableTiming));
+    ACK(cudaEventCreateWithFlags(&a->ev_join, cudaEventDisableTiming));
     for (int b = 0; b < 2; b++) {
       ACK(cudaEventCreateWithFlags(&a->ev_ready[b], cudaEventDisableTiming));
       ACK(cudaEventCreateWithFlags(&a->ev_free[b], cudaEventDisableTiming));
@@ -326,24 +364,24 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
   }
   // loss at the final state and its gradient (free_energy.c:3-157: c and grad c untruncated)
   {
-    k_adj_loss_prep3<R><<<A.blocks_s, 256, 0, st>>>(A.P, (const cx<R>*)c->state[1], A.S(SB0), A.ncx);
-    A.ifft(A.S(SB0), A.F(PCT), 3);
+    k_adj_loss_prep3<R><<<A.blocks_s, 256, 0, st>>>(A.P, (const cx<R>*)c->state[1], A.SS(0, SB), A.ncx);
+    A.ifft(st, 0, A.SS(0, SB), A.FS(0, PCT), 3);
     const double inv = 1.0 / ((double)c->n * (double)c->n);
     const double kb = lw[0] * 12.0 * (p.sigma / p.epsilon) * inv;
     const double kg = (lw[1] * 0.75 * p.sigma * p.epsilon + 4.0 * lw[2]) * inv;
     const double dkb = lw[0] * 12.0 / p.epsilon * inv;
     const double dkg = lw[1] * 0.75 * p.epsilon * inv;
-    k_adj_loss<R><<<A.blocks_p, 256, 0, st>>>(A.F(PCT), A.F(PCX), A.F(PCY), A.F(PUB), A.F(PVB), A.F(PWXB), A.nn, kb,
-                                              kg, dkb, dkg, a->acc);
-    A.dfft(A.F(PUB), A.S(SB0), 3);
-    k_adj_loss_acc3<R><<<A.blocks_s, 256, 0, st>>>(A.P, A.S(SB0), A.S(SGC), A.S(SGW), A.ncx);
+    k_adj_loss<R><<<A.blocks_p, 256, 0, st>>>(A.FS(0, PCT), A.FS(0, PCX), A.FS(0, PCY), A.F(PUB), A.F(PVB),
+                                              A.F(PWXB), A.nn, kb, kg, dkb, dkg, a->acc);
+    A.dfft(st, 0, A.F(PUB), A.SS(0, SB), 3);
+    k_adj_loss_acc3<R><<<A.blocks_s, 256, 0, st>>>(A.P, A.SS(0, SB), A.S(SGC), A.S(SGW), A.ncx);
   }
   // the reversed step as a CUDA graph on its fixed buffers (eager if capture fails)
   if (!a->rev && !a->rev_tried) {
     a->rev_tried = true;
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      A.reverse_step(coef, dcoef);
+      A.reverse_step(coef, dcoef, a->fork);
       if (cudaStreamEndCapture(st, &g) == cudaSuccess && g) {
         if (cudaGraphInstantiate(&a->rev, g, 0) != cudaSuccess) a->rev = nullptr;
         cudaGraphDestroy(g);
@@ -378,7 +416,7 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
       if (a->rev) {
         ACK(cudaGraphLaunch(a->rev, st));
       } else {
-        A.reverse_step(coef, dcoef);
+        A.reverse_step(coef, dcoef, nullptr);
       }
     }
     ACK(cudaEventRecord(a->ev_free[b], st));
@@ -428,7 +466,10 @@ void chns_adj_free(chns_ctx* c) {
   if (a->side) {
     cudaStreamSynchronize(a->side);
     cudaStreamDestroy(a->side);
+    cudaStreamDestroy(a->fork);
     cudaEventDestroy(a->ev_sweep);
+    cudaEventDestroy(a->ev_fork);
+    cudaEventDestroy(a->ev_join);
     for (int b = 0; b < 2; b++) {
       cudaEventDestroy(a->ev_ready[b]);
       cudaEventDestroy(a->ev_free[b]);
