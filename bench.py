@@ -15,6 +15,13 @@ k = 0 modes in FP64.  A "step" is one full ETD2RK step (both stages).
   roofline : the dominant kernel's algorithmic bytes / its CUDA-event time
   cpu_baseline : the reference's own etd2rk() (compiled here, oracle/_ref)
              timed on the host cores on a sample of the same workload
+  adjoint  : the discrete adjoint (chns_adjoint) of 200 binary steps at 512^2
+             (nu = 0.01, M = 0.005, sigma = 0.2, eps = 2 dx, spinodal noise;
+             dt = 1e-4: with eps = 2 dx the explicit bulk term grows as n^3 and
+             dt = 1e-3 diverges at 512^2), checkpoints every 20 steps: its time
+             over the forward time of the same 200 steps, in FP64 and FP32,
+             central differences along seeded directions, and a 4096^2 run of
+             1000 steps (dt = 1.5e-7 for the same reason) for the memory budget
 
 --impl reference times the reference's CPU implementation (oracle/_ref) on the
 same metric; multi-GPU runs are independent replicas (the step does not shard;
@@ -140,6 +147,104 @@ def read_profile_traffic(kernel: str, n: int):
     return None
 
 
+def adjoint_params(n: int, precision: int, dt: float) -> dict:
+    lx = 2 * math.pi
+    p = dict(model=1, precision=precision, nx=n, ny=n, lx=lx, ly=lx, dt=dt, nu=0.01, sigma=0.2,
+             epsilon=2.0 * (lx / n), coef_mode=1)
+    p["lambda"] = 0.005
+    return p
+
+
+def adjoint_leg(C, stream, big_steps: int):
+    """Cost of the discrete adjoint against the forward steps it reverses."""
+    import numpy as np
+    import torch
+
+    n, steps, ckpt = 512, 200, 20
+    rng = np.random.default_rng(2024)
+    noise = rng.uniform(-0.05, 0.05, (n, n))
+    phi = noise - noise.mean()
+    c_real = 0.5 * (1.0 + phi)
+    out = {"grid": n, "steps": steps, "ckpt": ckpt, "loss": "E_bulk + E_grad + <|grad phi|^2> at the final step"}
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    for prec, name in ((C.FP64, "fp64"), (C.FP32, "fp32")):
+        with C.Context(adjoint_params(n, prec, 1e-4)) as c:
+            c.L.chns_set_stream(c.handle, ctypes_stream(stream))
+            c.set_phase_real(c_real)
+            st0 = c.get_state()
+            c.adjoint(steps, ckpt)  # buffers and the reverse-step graph
+            c.step(10)
+            c.set_state(*st0)
+            c.synchronize()
+            ev0.record(stream)
+            c.step(steps)
+            ev1.record(stream)
+            ev1.synchronize()
+            t_fwd = ev0.elapsed_time(ev1)
+            c.set_state(*st0)
+            c.synchronize()
+            ev0.record(stream)
+            J, gw, gc, gp = c.adjoint(steps, ckpt)
+            ev1.record(stream)
+            ev1.synchronize()
+            t_adj = ev0.elapsed_time(ev1)
+            leg = {"forward_ms": round(t_fwd, 3), "adjoint_ms": round(t_adj, 3), "ratio": round(t_adj / t_fwd, 3),
+                   "J": J, "dJ_dnu": gp[0], "dJ_dM": gp[1], "dJ_dsigma": gp[2]}
+            if prec == C.FP64:
+                # central differences of J along seeded smooth directions of c_hat_0
+                errs = []
+                mx = np.minimum(np.arange(n), n - np.arange(n))
+                kk = np.sqrt(mx[:, None] ** 2 + np.arange(n // 2 + 1)[None, :] ** 2)
+                for k in range(2):
+                    d = np.fft.rfft2(np.random.default_rng(100 + k).standard_normal((n, n)))
+                    d *= np.exp(-kk / 8.0)
+                    d *= np.abs(st0[1]).ravel()[1:].max() / np.abs(d).max()
+                    d[0, 0] = 0.0
+                    h = 1e-6
+                    js = []
+                    for sgn in (1, -1):
+                        c.set_state(st0[0], st0[1] + sgn * h * d)
+                        js.append(c.adjoint(steps, ckpt)[0])
+                    fd = (js[0] - js[1]) / (2 * h)
+                    ad = float(np.sum(gc.real * d.real + gc.imag * d.imag))
+                    errs.append(abs(ad - fd) / abs(fd))
+                leg["fd_rel_err"] = errs
+                g64 = (gc, gp)
+            else:
+                leg["rel_diff_vs_fp64_dJ_dc"] = float(np.linalg.norm(gc - g64[0]) / np.linalg.norm(g64[0]))
+            out[name] = leg
+    if big_steps > 0:
+        nb = 4096
+        with C.Context(adjoint_params(nb, C.FP32, 1.5e-7)) as c:
+            c.L.chns_set_stream(c.handle, ctypes_stream(stream))
+            noise = np.random.default_rng(7).uniform(-0.05, 0.05, (nb, nb))
+            c.set_phase_real(0.5 * (1.0 + noise - noise.mean()))
+            st_big = c.get_state()
+            c.step(3)
+            c.set_state(*st_big)
+            c.synchronize()
+            ev0.record(stream)
+            c.step(big_steps)
+            ev1.record(stream)
+            ev1.synchronize()
+            t_fwd = ev0.elapsed_time(ev1) / 1e3
+            c.set_state(*st_big)
+            c.synchronize()
+            free0, total = torch.cuda.mem_get_info()
+            ev0.record(stream)
+            J = c.adjoint(big_steps, ckpt)[0]
+            ev1.record(stream)
+            ev1.synchronize()
+            free1, _ = torch.cuda.mem_get_info()
+            t_adj = ev0.elapsed_time(ev1) / 1e3
+            out["fp32_4096"] = {"steps": big_steps, "ckpt": ckpt, "forward_s": round(t_fwd, 3),
+                                "adjoint_s": round(t_adj, 3), "ratio": round(t_adj / t_fwd, 3),
+                                "adjoint_buffers_gb": round((free0 - free1) / 1e9, 2),
+                                "hbm_total_gb": round(total / 1e9, 1), "J_finite": bool(math.isfinite(J))}
+    return out
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -235,6 +340,8 @@ def run_gpu(args):
                "mean_c_rel_drift_fp32": float(mean_drift), "coefficients": "series/expm1 (FP64) in both"}
         del res
 
+    adj = adjoint_leg(C, stream, args.adjoint_big_steps) if args.adjoint and rank == 0 else None
+
     out = None
     if rank == 0:
         hbm, src = peaks()
@@ -265,6 +372,7 @@ def run_gpu(args):
             "fp64_steps_per_s": round(fp64_sps, 3),
             "fp32_over_fp64": round((value / world) / fp64_sps, 3),
             "fp32_vs_fp64": acc,
+            "adjoint": adj,
             "per_kernel_ms": prof["per_kernel_ms"],
             "gpu_launches": launches,
             "state_finite": bool(finite),
@@ -462,6 +570,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dt", type=float, default=DT_DEFAULT)
     ap.add_argument("--accuracy-steps", type=int, default=1000)
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
+    ap.add_argument("--adjoint-big-steps", type=int, default=1000,
+                    help="steps of the 4096^2 FP32 adjoint memory check (0: skip)")
     ap.add_argument("--profile-case", action="store_true",
                     help="only run --steps steps of the FP32 workload (for ncu captures); prints nothing")
     args = ap.parse_args()
