@@ -22,6 +22,12 @@ k = 0 modes in FP64.  A "step" is one full ETD2RK step (both stages).
              over the forward time of the same 200 steps, in FP64 and FP32,
              central differences along seeded directions, and a 4096^2 run of
              1000 steps (dt = 1.5e-7 for the same reason) for the memory budget
+  ensemble : 64 ternary runs (32 at 256^2, 24 at 512^2, 8 at 1024^2; own seeds
+             and sigma_ij ~ U[0.15, 0.35] with every gamma_i >= 0.1; nu = 0.01,
+             M = 0.005, eps = 2 dx; FP32)
+             advanced together by chns_ensemble_step against the same members
+             stepped one after another (wall clock with a synchronize on both
+             sides; dt per size so that every run stays finite)
 
 --impl reference times the reference's CPU implementation (oracle/_ref) on the
 same metric; multi-GPU runs are independent replicas (the step does not shard;
@@ -245,6 +251,72 @@ def adjoint_leg(C, stream, big_steps: int):
     return out
 
 
+# (grid, members, dt): the explicit chemical-potential term grows as n^3 / gamma_min
+ENSEMBLE_GROUPS = ((256, 32, 1e-4), (512, 24, 2.5e-5), (1024, 8, 3e-6))
+
+
+def draw_sigmas(rng):
+    """sigma_12, sigma_13, sigma_23 ~ U[0.15, 0.35], redrawn until every spreading
+    coefficient gamma_i (main.c:166-170) is >= 0.1: a draw with gamma_i near or
+    below 0 is an ill-posed (negative surface tension) run."""
+    while True:
+        s12, s13, s23 = rng.uniform(0.15, 0.35, 3)
+        if min(s12 + s13 - s23, s12 + s23 - s13, s13 + s23 - s12) >= 0.1:
+            return float(s12), float(s13), float(s23)
+
+
+def ensemble_members(seed: int = 3000):
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for n, count, dt in ENSEMBLE_GROUPS:
+        for _ in range(count):
+            lx = 2 * math.pi
+            s12, s13, s23 = draw_sigmas(rng)
+            p = dict(model=2, precision=1, nx=n, ny=n, lx=lx, ly=lx, dt=dt, nu=0.01, epsilon=2.0 * lx / n,
+                     sigma12=s12, sigma13=s13, sigma23=s23, coef_mode=1)
+            p["lambda"] = 0.005
+            ph = (1 / 3 + 0.02 * rng.uniform(-1, 1, (n, n)), 1 / 3 + 0.02 * rng.uniform(-1, 1, (n, n)))
+            out.append((p, ph))
+    return out
+
+
+def ensemble_leg(C, steps: int):
+    """Throughput of the 64-member ternary ensemble, together and one by one."""
+    import numpy as np
+
+    members = ensemble_members()
+    pts = sum(p["nx"] * p["ny"] for p, _ in members)
+    with C.Ensemble([p for p, _ in members]) as ens:
+        for m, (_, ph) in zip(ens.members, members):
+            m.set_phase_real(*ph)
+        ens.step(5)
+        ens.synchronize()
+        t0 = time.perf_counter()
+        ens.step(steps)
+        ens.synchronize()
+        t_ens = time.perf_counter() - t0
+        fin = [bool(np.all(np.isfinite(m.get_state()[1]))) for m in ens.members]
+        finite = {f"{n}^2": all(f for f, (p, _) in zip(fin, members) if p["nx"] == n) for n, _, _ in ENSEMBLE_GROUPS}
+        launches = sum(m.launches_per_step() for m in ens.members) * steps
+    t_one = 0.0
+    for p, ph in members:
+        with C.Context(p) as c:
+            c.set_phase_real(*ph)
+            c.step(5)
+            c.synchronize()
+            t0 = time.perf_counter()
+            c.step(steps)
+            c.synchronize()
+            t_one += time.perf_counter() - t0
+    return {"members": {f"{n}^2": k for n, k, _ in ENSEMBLE_GROUPS}, "model": "ternary", "precision": "fp32",
+            "steps": steps, "ensemble_s": round(t_ens, 4), "one_by_one_s": round(t_one, 4),
+            "speedup": round(t_one / t_ens, 3), "member_steps_per_s": round(len(members) * steps / t_ens, 1),
+            "grid_point_steps_per_s": round(pts * steps / t_ens, 1), "gpu_launches": launches,
+            "all_finite": finite}
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -341,6 +413,7 @@ def run_gpu(args):
         del res
 
     adj = adjoint_leg(C, stream, args.adjoint_big_steps) if args.adjoint and rank == 0 else None
+    ens = ensemble_leg(C, args.ensemble_steps) if args.ensemble_steps > 0 and rank == 0 else None
 
     out = None
     if rank == 0:
@@ -373,6 +446,7 @@ def run_gpu(args):
             "fp32_over_fp64": round((value / world) / fp64_sps, 3),
             "fp32_vs_fp64": acc,
             "adjoint": adj,
+            "ensemble": ens,
             "per_kernel_ms": prof["per_kernel_ms"],
             "gpu_launches": launches,
             "state_finite": bool(finite),
@@ -571,6 +645,7 @@ def main():
     ap.add_argument("--dt", type=float, default=DT_DEFAULT)
     ap.add_argument("--accuracy-steps", type=int, default=1000)
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
+    ap.add_argument("--ensemble-steps", type=int, default=500, help="steps of the ensemble leg (0: skip)")
     ap.add_argument("--adjoint-big-steps", type=int, default=1000,
                     help="steps of the 4096^2 FP32 adjoint memory check (0: skip)")
     ap.add_argument("--profile-case", action="store_true",

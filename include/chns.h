@@ -123,6 +123,27 @@ int chns_diagnostics(chns_ctx *ctx, double *out_fe, double *out_ke);
 int chns_adjoint(chns_ctx *ctx, int nsteps, int ckpt, const double *loss_w, double *J, double *g_w,
                  double *g_c, double *g_params, int where);
 
+/* Ensembles.  Many independent runs (realisations with their own seeds and
+ * parameters, any mix of models, grid sizes and precisions) advanced together:
+ * the reference runs one configuration per mpirun, so this has no counterpart
+ * there; each member is a full context (the reference's state and step), and
+ * chns_ensemble_step advances all of them with one CUDA graph launch per step in
+ * which every member's stage kernels form their own branch, so members that
+ * are too small to fill the GPU alone run side by side.  Member i's results are
+ * identical to chns_step on a lone context with the same parameters. */
+typedef struct chns_ensemble chns_ensemble;
+int chns_ensemble_create(const chns_params *members, int count, chns_ensemble **out);
+int chns_ensemble_destroy(chns_ensemble *ens);
+/* The context of member i (owned by the ensemble: use it for set_state,
+ * get_state, set_phase_real and diagnostics; do not destroy it or change its
+ * stream).  NULL if i is out of range. */
+chns_ctx *chns_ensemble_member(chns_ensemble *ens, int i);
+int chns_ensemble_size(const chns_ensemble *ens);
+/* nsteps ETD2RK steps of every member; stream-ordered after earlier work on
+ * each member's stream, and later work on member streams waits for it. */
+int chns_ensemble_step(chns_ensemble *ens, int nsteps);
+int chns_ensemble_synchronize(chns_ensemble *ens);
+
 /* Kernel launches of one step (known after the first chns_step). */
 int chns_launches_per_step(const chns_ctx *ctx);
 

@@ -77,6 +77,16 @@ def load_library(path: str = LIB_PATH):
     L.chns_profile_step.restype = ip
     L.chns_adjoint.argtypes = [vp, ip, ip, vp, vp, vp, vp, vp, ip]
     L.chns_adjoint.restype = ip
+    L.chns_ensemble_create.argtypes = [vp, ip, ctypes.POINTER(vp)]
+    L.chns_ensemble_create.restype = ip
+    L.chns_ensemble_destroy.argtypes = [vp]
+    L.chns_ensemble_member.argtypes = [vp, ip]
+    L.chns_ensemble_member.restype = vp
+    L.chns_ensemble_size.argtypes = [vp]
+    L.chns_ensemble_step.argtypes = [vp, ip]
+    L.chns_ensemble_step.restype = ip
+    L.chns_ensemble_synchronize.argtypes = [vp]
+    L.chns_ensemble_synchronize.restype = ip
     L.chns_dfft_noalloc.argtypes = [vp, vp, ip, vp]
     L.chns_dfft_noalloc.restype = ip
     L.chns_status_string.restype = ctypes.c_char_p
@@ -238,3 +248,66 @@ class Context:
 
     def launches_per_step(self) -> int:
         return self.L.chns_launches_per_step(self._h)
+
+
+class Member(Context):
+    """A member of an Ensemble: the Context calls on a context the ensemble owns."""
+
+    def __init__(self, ens: "Ensemble", index: int, params: dict):
+        self.L = ens.L
+        self.params = dict(params)
+        self._p = make_params(params)
+        h = self.L.chns_ensemble_member(ens._h, index)
+        if not h:
+            raise ChnsError(-1, "chns_ensemble_member")
+        self._h = ctypes.c_void_p(h)
+        self.model = self._p.model
+        self.nx, self.ny = self._p.nx, self._p.ny
+        self.shape = (self.nx, self.ny // 2 + 1)
+
+    def close(self):
+        self._h = None  # owned by the ensemble
+
+
+class Ensemble:
+    """Independent runs (any mix of models, sizes, precisions and parameters)
+    advanced together by chns_ensemble_step: one CUDA graph launch per step with
+    every member on its own branch.  ``members[i]`` behaves like a Context."""
+
+    def __init__(self, params_list):
+        self.L = load_library()
+        plist = list(params_list)
+        arr = (Params * len(plist))(*[make_params(p) for p in plist])
+        h = ctypes.c_void_p()
+        _check(self.L.chns_ensemble_create(ctypes.cast(arr, ctypes.c_void_p), len(plist), ctypes.byref(h)),
+               "chns_ensemble_create")
+        self._h = h
+        self.members = [Member(self, i, p) for i, p in enumerate(plist)]
+
+    def __len__(self):
+        return len(self.members)
+
+    def step(self, n: int = 1):
+        _check(self.L.chns_ensemble_step(self._h, int(n)), "chns_ensemble_step")
+
+    def synchronize(self):
+        _check(self.L.chns_ensemble_synchronize(self._h), "chns_ensemble_synchronize")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for m in self.members:
+                m._h = None
+            self.L.chns_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
