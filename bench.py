@@ -153,6 +153,21 @@ def read_profile_traffic(kernel: str, n: int):
     return None
 
 
+def replica_throughput(ms: float, steps: int, world: int, device: str):
+    """Whole-job steps/s of `world` independent replicas (one per rank and GPU, no
+    data-path collective): every rank ran `steps` steps in `ms` milliseconds; the
+    job takes as long as its slowest rank.  Returns (max ms over ranks, steps/s)."""
+    t_max = ms
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    return t_max, world * steps / (t_max / 1e3)
+
+
 def adjoint_params(n: int, precision: int, dt: float) -> dict:
     lx = 2 * math.pi
     p = dict(model=1, precision=precision, nx=n, ny=n, lx=lx, ly=lx, dt=dt, nu=0.01, sigma=0.2,
@@ -365,13 +380,8 @@ def run_gpu(args):
     torch.cuda.synchronize()
     barrier()
     ms = ev0.elapsed_time(ev1)
-    t_max = ms
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max, value = replica_throughput(ms, args.steps, world, "cuda")
     ms_per_step = t_max / args.steps
-    value = world * args.steps / (t_max / 1e3)
     launches = ctx.launches_per_step() * args.steps
     fe, ke, rc = ctx.diagnostics()
     finite = rc == 0
