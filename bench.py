@@ -153,6 +153,31 @@ def read_profile_traffic(kernel: str, n: int):
     return None
 
 
+def init_leg(C, n: int) -> dict:
+    """Wall time of init.c's initial conditions on the device at n^2 (each call
+    ends with a synchronize): binary drop, Taylor-Green vorticity, ternary noise
+    (host draws of the C library generator + device fields and transforms)."""
+    out = {"grid": n, "precision": "fp32"}
+    lx = 2 * math.pi
+    for model, key in ((1, "binary"), (2, "ternary")):
+        p = dict(model=model, precision=1, nx=n, ny=n, lx=lx, ly=lx, dt=1e-6, nu=0.01, epsilon=2 * lx / n,
+                 sigma=0.2, sigma12=0.2, sigma13=0.3, sigma23=0.25)
+        p["lambda"] = 0.005
+        with C.Context(p) as c:
+            c.init_vorticity(C.INIT_W_TAYLOR_GREEN, 1.0)  # first call: buffers and kernels warm
+            t0 = time.perf_counter()
+            c.init_vorticity(C.INIT_W_TAYLOR_GREEN, 1.0)
+            t1 = time.perf_counter()
+            c.init_phase(C.INIT_C_DROP if model == 1 else C.INIT_C_NOISE, 10)
+            t2 = time.perf_counter()
+        if model == 1:
+            out["taylor_green_ms"] = round((t1 - t0) * 1e3, 3)
+            out["drop_ms"] = round((t2 - t1) * 1e3, 3)
+        else:
+            out["ternary_noise_ms"] = round((t2 - t1) * 1e3, 3)
+    return out
+
+
 def replica_throughput(ms: float, steps: int, world: int, device: str):
     """Whole-job steps/s of `world` independent replicas (one per rank and GPU, no
     data-path collective): every rank ran `steps` steps in `ms` milliseconds; the
@@ -422,6 +447,7 @@ def run_gpu(args):
                "mean_c_rel_drift_fp32": float(mean_drift), "coefficients": "series/expm1 (FP64) in both"}
         del res
 
+    init = init_leg(C, n) if rank == 0 else None
     adj = adjoint_leg(C, stream, args.adjoint_big_steps) if args.adjoint and rank == 0 else None
     ens = ensemble_leg(C, args.ensemble_steps) if args.ensemble_steps > 0 and rank == 0 else None
 
@@ -455,6 +481,7 @@ def run_gpu(args):
             "fp64_steps_per_s": round(fp64_sps, 3),
             "fp32_over_fp64": round((value / world) / fp64_sps, 3),
             "fp32_vs_fp64": acc,
+            "init": init,
             "adjoint": adj,
             "ensemble": ens,
             "per_kernel_ms": prof["per_kernel_ms"],

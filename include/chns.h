@@ -110,6 +110,27 @@ int chns_ifft(chns_ctx *ctx, const double *spec, double *real, int where);
  * phase-1 mean, phase-2 mean}. */
 int chns_diagnostics(chns_ctx *ctx, double *out_fe, double *out_ke);
 
+/* The reference's initial conditions (init.c) computed on the device, each with
+ * the dfft and truncation init.c applies.  Vorticity (init.c:38-96):
+ *   CHNS_INIT_W_ZERO           omega = 0 (ZERO_INIT, INIT_READ_DATA)
+ *   CHNS_INIT_W_TAYLOR_GREEN   TG_INIT: u = amplitude (sin x cos y, -cos x sin y),
+ *                              omega_hat = I (kx uy_hat - ky ux_hat), truncated
+ * The reference's remaining branch (random-phase modes, init.c:98-180) draws from
+ * a time-seeded rand() and is not provided.  Phase fields (init.c:229-292):
+ *   CHNS_INIT_C_DROP    binary: c = (1 - tanh((r - pi/4.5) / (eps/2))) / 2, r the
+ *                       distance to the box centre
+ *   CHNS_INIT_C_NOISE   ternary: c_i = 1/4 + 0.001 rand()/RAND_MAX, two draws per
+ *                       point in row-major order after srand(seed) (the reference
+ *                       uses seed = 10 + 2 rank); the C library's generator, run
+ *                       on the host with a private state
+ * chns_init_phase leaves omega unchanged; the other fields are replaced. */
+#define CHNS_INIT_W_ZERO 0
+#define CHNS_INIT_W_TAYLOR_GREEN 1
+#define CHNS_INIT_C_DROP 0
+#define CHNS_INIT_C_NOISE 1
+int chns_init_vorticity(chns_ctx *ctx, int kind, double amplitude);
+int chns_init_phase(chns_ctx *ctx, int kind, unsigned int seed);
+
 /* Discrete adjoint of `nsteps` ETD2RK steps of the binary model (etd2rk.c with
  * nonlin.c / surface_tension.c transposed operation by operation) from the
  * current state.  Loss at the final state, with c and grad c untruncated as in

@@ -67,6 +67,10 @@ CONFIGS = {
     # no working forcing, so this is the unforced step; same cost per step)
     "bin4096": dict(model=1, n=4096, lx="(2.0*pi)", dt="(2e-6)", nu="(1e-3)", lam="(1e-3)",
                     sigma="(0.1)", eps="(2.0*dx)"),
+    # Taylor-Green initial vorticity (TG_INIT, init.c:38-65): pure NS at L = 2 pi, and
+    # binary with the reference defaults (L = 4 pi, eps = 3 dx), whose init also lays the drop
+    "nstg32": dict(model=0, n=32, lx="(2.0*pi)", dt="(1e-3)", nu="(0.01)", init="tg"),
+    "bintg64": dict(_BIN_DEF, n=64, init="tg"),
 }
 
 _SUBST = {  # macro name -> key in the config dict
@@ -89,7 +93,7 @@ def _gen_global_h(cfg: dict) -> str:
 
 
 def _gen_macro_h(cfg: dict) -> str:
-    lines = ["/* generated by oracle/build_ref.py */", "#define ZERO_INIT"]
+    lines = ["/* generated by oracle/build_ref.py */", "#define TG_INIT" if cfg.get("init") == "tg" else "#define ZERO_INIT"]
     if cfg["model"] == 1:
         lines.append("#define BINARY")
     elif cfg["model"] == 2:

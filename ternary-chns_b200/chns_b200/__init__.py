@@ -25,6 +25,8 @@ MODEL_NS, MODEL_BINARY, MODEL_TERNARY = 0, 1, 2
 FP64, FP32 = 0, 1
 COEF_REFERENCE, COEF_ACCURATE = 0, 1
 HOST, DEVICE = 0, 1
+INIT_W_ZERO, INIT_W_TAYLOR_GREEN = 0, 1
+INIT_C_DROP, INIT_C_NOISE = 0, 1
 
 STATUS = {0: "ok", -1: "bad argument", -2: "CUDA error", -3: "non-finite or blown-up state",
           -4: "device wait timed out", -5: "unsupported size or option", -6: "out of memory"}
@@ -77,6 +79,10 @@ def load_library(path: str = LIB_PATH):
     L.chns_profile_step.restype = ip
     L.chns_adjoint.argtypes = [vp, ip, ip, vp, vp, vp, vp, vp, ip]
     L.chns_adjoint.restype = ip
+    L.chns_init_vorticity.argtypes = [vp, ip, ctypes.c_double]
+    L.chns_init_vorticity.restype = ip
+    L.chns_init_phase.argtypes = [vp, ip, ctypes.c_uint]
+    L.chns_init_phase.restype = ip
     L.chns_ensemble_create.argtypes = [vp, ip, ctypes.POINTER(vp)]
     L.chns_ensemble_create.restype = ip
     L.chns_ensemble_destroy.argtypes = [vp]
@@ -198,6 +204,15 @@ class Context:
         a = np.ascontiguousarray(p1, np.float64)
         b = np.ascontiguousarray(p2, np.float64) if p2 is not None else None
         _check(self.L.chns_set_phase_real(self._h, _ptr(a), _ptr(b), HOST), "chns_set_phase_real")
+
+    def init_vorticity(self, kind: int = INIT_W_ZERO, amplitude: float = 1.0):
+        """init.c's vorticity on the device: zero or Taylor-Green (TG_INIT)."""
+        _check(self.L.chns_init_vorticity(self._h, int(kind), float(amplitude)), "chns_init_vorticity")
+
+    def init_phase(self, kind: int, seed: int = 10):
+        """init.c's phase fields on the device: the binary drop or the ternary noise
+        (the C library's rand() after srand(seed); the reference seeds 10 + 2 rank)."""
+        _check(self.L.chns_init_phase(self._h, int(kind), int(seed)), "chns_init_phase")
 
     def step(self, n: int = 1):
         _check(self.L.chns_step(self._h, int(n)), "chns_step")

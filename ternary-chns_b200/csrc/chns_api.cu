@@ -468,15 +468,30 @@ int chns_get_state(chns_ctx* c, double* w, double* c1, double* c2, int where) {
   return CHNS_OK;
 }
 
-static int upload_real(chns_ctx* c, const double* real, int where) {
+// c->realdbl (n x n doubles) in the context precision in c->realbuf
+int chns_realdbl_to_realbuf(chns_ctx* c) {
   const size_t nn = (size_t)c->n * c->n;
-  int rc = to_device(c, c->realdbl, real, nn * sizeof(double), where);
-  if (rc) return rc;
   if (c->f32) {
     k_real_d2r_f32<<<1024, 256, 0, c->stream>>>(c->realdbl, (float*)c->realbuf, nn);
   } else {
     CK(cudaMemcpyAsync(c->realbuf, c->realdbl, nn * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   }
+  return CHNS_OK;
+}
+
+// phase field f (0: c / c1, 1: c2) from the real field in c->realdbl: dfft and
+// truncation (init.c:221-225, 253-262); FP32 contexts take its k = 0 mode in double
+int chns_phase_from_realdbl(chns_ctx* c, int f) {
+  int rc = chns_realdbl_to_realbuf(c);
+  if (rc) return rc;
+  c->L->dfft(c, c->realbuf, c->state[1 + f]);
+  c->L->truncate(c, c->state[1 + f]);
+  if (c->f32) {
+    // the k = 0 mode in double comes from the same FP32 transform
+    c->L->to_fftw(c, c->state[1 + f], c->stage);
+    k_k0_set<<<1, 1, 0, c->stream>>>(c->k0, c->stage, 1 + f);
+  }
+  CK(cudaGetLastError());
   return CHNS_OK;
 }
 
@@ -488,15 +503,10 @@ int chns_set_phase_real(chns_ctx* c, const double* p1, const double* p2, int whe
   if (c->f32) CK(cudaMemsetAsync(c->k0, 0, 2 * sizeof(double), c->stream));
   const double* src[2] = {p1, p2};
   for (int f = 0; f < c->p.model; f++) {
-    int rc = upload_real(c, src[f], where);
+    const size_t nn = (size_t)c->n * c->n;
+    int rc = to_device(c, c->realdbl, src[f], nn * sizeof(double), where);
+    if (!rc) rc = chns_phase_from_realdbl(c, f);
     if (rc) return rc;
-    c->L->dfft(c, c->realbuf, c->state[1 + f]);
-    c->L->truncate(c, c->state[1 + f]);
-    if (c->f32) {
-      // the k = 0 mode in double comes from the same FP32 transform
-      c->L->to_fftw(c, c->state[1 + f], c->stage);
-      k_k0_set<<<1, 1, 0, c->stream>>>(c->k0, c->stage, 1 + f);
-    }
   }
   CK(cudaGetLastError());
   return chns_synchronize(c);
@@ -555,7 +565,8 @@ int chns_rhs(chns_ctx* c, double* nw, double* nc1, double* nc2, int where) {
 
 int chns_dfft(chns_ctx* c, const double* real, double* spec, int where) {
   if (!c || !real || !spec) return CHNS_ERR_ARG;
-  int rc = upload_real(c, real, where);
+  int rc = to_device(c, c->realdbl, real, (size_t)c->n * c->n * sizeof(double), where);
+  if (!rc) rc = chns_realdbl_to_realbuf(c);
   if (rc) return rc;
   c->L->dfft(c, c->realbuf, c->nw);
   return get_field(c, 0, c->nw, spec, where, -1);

@@ -8,6 +8,9 @@
 struct chns_ctx;
 struct chns_adj;
 void chns_adj_free(chns_ctx* c);
+// shared by chns_set_phase_real and the initial conditions (chns_init.cu)
+extern "C" int chns_realdbl_to_realbuf(chns_ctx* c);
+extern "C" int chns_phase_from_realdbl(chns_ctx* c, int f);
 
 namespace chns {
 // intermediate buffers of a step: G slots (rows 0..jt) and H slots (rows

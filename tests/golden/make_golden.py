@@ -11,7 +11,7 @@ Small grids store full spectral states; the two full-size configurations
 (binary 256^2 x 1000 steps, ternary 512^2 x 2000 steps) store a fingerprint of
 the final state (see fingerprint()).
 
-Usage:  python tests/golden/make_golden.py [--full]
+Usage:  python tests/golden/make_golden.py [--full] [--init]  (--init: only init_ref.npz)
 """
 from __future__ import annotations
 
@@ -149,9 +149,30 @@ def make_full(O):
         print("wrote", name)
 
 
+# the reference's own init() (init.c) on configurations whose macros select each branch:
+# ZERO_INIT vorticity with the binary drop / ternary srand(10) noise, and TG_INIT
+INIT_CONFIGS = ["bin32", "ter32", "bindef64", "terdef64", "nstg32", "bintg64"]
+
+
+def make_init(O):
+    out = {}
+    for name in INIT_CONFIGS:
+        p = O.ref_config_params(name)
+        R = O.RefLib(name)  # ref_setup ends with the reference's init()
+        out[f"{name}_params"] = json.dumps(p)
+        for k, a in enumerate(R.get_state()):
+            out[f"{name}_state{k}"] = a
+    np.savez_compressed(os.path.join(HERE, "init_ref.npz"), **out)
+    print("wrote init_ref")
+
+
 if __name__ == "__main__":
     import oracle as O
     O.build_ref.build_all()
-    make_small(O)
+    if "--init" in sys.argv:
+        make_init(O)
+    else:
+        make_small(O)
+        make_init(O)
     if "--full" in sys.argv:
         make_full(O)
