@@ -40,6 +40,7 @@ extern "C" {
 #define CHNS_ERR_TIMEOUT (-4)     /* a bounded device wait ran out */
 #define CHNS_ERR_UNSUPPORTED (-5) /* size or option not supported */
 #define CHNS_ERR_NOMEM (-6)       /* device or host allocation failed */
+#define CHNS_ERR_IO (-7)          /* a file could not be read or written */
 
 enum { CHNS_MODEL_NS = 0, CHNS_MODEL_BINARY = 1, CHNS_MODEL_TERNARY = 2 };
 enum { CHNS_FP64 = 0, CHNS_FP32 = 1 };
@@ -130,6 +131,19 @@ int chns_diagnostics(chns_ctx *ctx, double *out_fe, double *out_ke);
 #define CHNS_INIT_C_NOISE 1
 int chns_init_vorticity(chns_ctx *ctx, int kind, double amplitude);
 int chns_init_phase(chns_ctx *ctx, int kind, unsigned int seed);
+
+/* Field files in the reference's format (write_array.c:18-46, read_array.c:12-40):
+ * raw FP64, nx x ny, row-major with x the slow index, no header.
+ * chns_write_fields writes the real-space fields of the current state as main.c's
+ * dumps do: <dir>/vort/wz.<index> and <dir>/phase_field/phi.<index> (binary) or
+ * phi1.<index> and phi2.<index> (ternary), creating the two folders.  truncate = 0
+ * is the serial dump (main.c:233-249, ifft of the state as it is), truncate = 1 the
+ * DUMP_REAL_MPI dump (main.c:334-356, truncation then ifft).
+ * chns_read_phase reads the phase file(s) of INIT_READ_DATA (init.c:221-225,
+ * 253-262: read, dfft, truncation; omega = 0), as chns_set_phase_real.
+ * A file that cannot be opened, written or fully read gives CHNS_ERR_IO. */
+int chns_write_fields(chns_ctx *ctx, const char *dir, int index, int truncate);
+int chns_read_phase(chns_ctx *ctx, const char *path1, const char *path2);
 
 /* Discrete adjoint of `nsteps` ETD2RK steps of the binary model (etd2rk.c with
  * nonlin.c / surface_tension.c transposed operation by operation) from the

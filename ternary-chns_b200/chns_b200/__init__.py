@@ -29,7 +29,8 @@ INIT_W_ZERO, INIT_W_TAYLOR_GREEN = 0, 1
 INIT_C_DROP, INIT_C_NOISE = 0, 1
 
 STATUS = {0: "ok", -1: "bad argument", -2: "CUDA error", -3: "non-finite or blown-up state",
-          -4: "device wait timed out", -5: "unsupported size or option", -6: "out of memory"}
+          -4: "device wait timed out", -5: "unsupported size or option", -6: "out of memory",
+          -7: "file could not be read or written"}
 
 
 class ChnsError(RuntimeError):
@@ -79,6 +80,10 @@ def load_library(path: str = LIB_PATH):
     L.chns_profile_step.restype = ip
     L.chns_adjoint.argtypes = [vp, ip, ip, vp, vp, vp, vp, vp, ip]
     L.chns_adjoint.restype = ip
+    L.chns_write_fields.argtypes = [vp, ctypes.c_char_p, ip, ip]
+    L.chns_write_fields.restype = ip
+    L.chns_read_phase.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p]
+    L.chns_read_phase.restype = ip
     L.chns_init_vorticity.argtypes = [vp, ip, ctypes.c_double]
     L.chns_init_vorticity.restype = ip
     L.chns_init_phase.argtypes = [vp, ip, ctypes.c_uint]
@@ -204,6 +209,17 @@ class Context:
         a = np.ascontiguousarray(p1, np.float64)
         b = np.ascontiguousarray(p2, np.float64) if p2 is not None else None
         _check(self.L.chns_set_phase_real(self._h, _ptr(a), _ptr(b), HOST), "chns_set_phase_real")
+
+    def write_fields(self, directory: str, index: int, truncate: bool = False):
+        """main.c's dumps: <directory>/vort/wz.<index>, phase_field/phi[1|2].<index>,
+        raw FP64 nx x ny (write_array.c); truncate=True as DUMP_REAL_MPI."""
+        _check(self.L.chns_write_fields(self._h, os.fsencode(directory), int(index), int(bool(truncate))),
+               "chns_write_fields")
+
+    def read_phase(self, path1: str, path2: str | None = None):
+        """INIT_READ_DATA: raw FP64 nx x ny phase file(s) (read_array.c), dfft, truncation."""
+        _check(self.L.chns_read_phase(self._h, os.fsencode(path1), os.fsencode(path2) if path2 else None),
+               "chns_read_phase")
 
     def init_vorticity(self, kind: int = INIT_W_ZERO, amplitude: float = 1.0):
         """init.c's vorticity on the device: zero or Taylor-Green (TG_INIT)."""

@@ -588,6 +588,26 @@ int chns_ifft(chns_ctx* c, const double* spec, double* real, int where) {
   return from_device(c, real, c->realdbl, nn * sizeof(double), where);
 }
 
+// real-space field f of the state (optionally truncated first) in c->realdbl
+int chns_field_to_realdbl(chns_ctx* c, int f, int truncate) {
+  const size_t nn = (size_t)c->n * c->n;
+  const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
+  const void* src = c->state[f];
+  if (truncate) {
+    CK(cudaMemcpyAsync(c->nw, c->state[f], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    c->L->truncate(c, c->nw);
+    src = c->nw;
+  }
+  c->L->ifft(c, src, c->realbuf);
+  if (c->f32) {
+    k_real_r2d_f32<<<1024, 256, 0, c->stream>>>((const float*)c->realbuf, c->realdbl, nn);
+  } else {
+    CK(cudaMemcpyAsync(c->realdbl, c->realbuf, nn * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  CK(cudaGetLastError());
+  return CHNS_OK;
+}
+
 int chns_diagnostics(chns_ctx* c, double* out_fe, double* out_ke) {
   if (!c) return CHNS_ERR_ARG;
   c->L->diag(c);
@@ -661,6 +681,7 @@ const char* chns_status_string(int s) {
     case CHNS_ERR_TIMEOUT: return "device wait timed out";
     case CHNS_ERR_UNSUPPORTED: return "unsupported size or option";
     case CHNS_ERR_NOMEM: return "out of memory";
+    case CHNS_ERR_IO: return "file could not be read or written";
   }
   return "unknown status";
 }

@@ -11,6 +11,8 @@ void chns_adj_free(chns_ctx* c);
 // shared by chns_set_phase_real and the initial conditions (chns_init.cu)
 extern "C" int chns_realdbl_to_realbuf(chns_ctx* c);
 extern "C" int chns_phase_from_realdbl(chns_ctx* c, int f);
+// real-space field f of the state (truncated first if asked) into c->realdbl
+extern "C" int chns_field_to_realdbl(chns_ctx* c, int f, int truncate);
 
 namespace chns {
 // intermediate buffers of a step: G slots (rows 0..jt) and H slots (rows
