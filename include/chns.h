@@ -111,6 +111,21 @@ int chns_ifft(chns_ctx *ctx, const double *spec, double *real, int where);
  * phase-1 mean, phase-2 mean}. */
 int chns_diagnostics(chns_ctx *ctx, double *out_fe, double *out_ke);
 
+/* Shell spectra of the current state (spectrum.c:3-194), without spectrum.c's side
+ * effect (it truncates the phase fields in place).  nshell = chns_spectrum_shells
+ * = round(nx/sqrt(2) + 1) (main.c:60); shell (int)(|k|/dk + 0.5), dk = 2 pi / lx.
+ * out receives ek and ensk (nshell each), then sph (binary) or sph1, sph2, sp12
+ * (ternary) (nshell each), then ekx and eky (nx/2 + 1 each: spectrum.c indexes
+ * them up to nx/2 although main.c:182-185 allocates only kxm / kym entries). */
+int chns_spectrum_shells(const chns_ctx *ctx);
+int chns_spectrum(chns_ctx *ctx, double *out);
+
+/* Interface perimeter (perimeter.c:3-271) of each phase field: out[5 f + 0..4] =
+ * count of cells whose +x or +y neighbour (periodic) lies on the other side of
+ * c = 0.5, count of cells with c >= 0.5, Sp_0 = 2 sqrt(pi count2 dx dy),
+ * Sp_t = count1 dx, def = Sp_t / Sp_0 - 1. */
+int chns_perimeter(chns_ctx *ctx, double *out);
+
 /* The reference's initial conditions (init.c) computed on the device, each with
  * the dfft and truncation init.c applies.  Vorticity (init.c:38-96):
  *   CHNS_INIT_W_ZERO           omega = 0 (ZERO_INIT, INIT_READ_DATA)

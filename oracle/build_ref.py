@@ -36,7 +36,7 @@ OUT = os.path.join(HERE, "_ref")
 REF_SOURCES = [
     "global.c", "etd2rk.c", "nonlin.c", "surface_tension.c", "chem_potential.c",
     "velocity.c", "curl.c", "functions.c", "fft.c", "init.c", "free_energy.c",
-    "kinetic_energy.c",
+    "kinetic_energy.c", "spectrum.c", "perimeter.c",
 ]
 
 # Configurations: model 0 = pure Navier-Stokes, 1 = BINARY, 2 = TERNARY.

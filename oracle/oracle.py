@@ -279,6 +279,34 @@ class RefLib:
         n = self._L.ref_kinetic_energy(out, 4)
         return list(out)[1:n]
 
+    def spectrum(self, workdir: str) -> dict:
+        """spectrum.c on the current state (state unchanged), run in `workdir`."""
+        L = self._L
+        L.ref_spectrum.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+        nshell = int(round(self.nx / math.sqrt(2.0) + 1.0))
+        nph = {0: 0, 1: 1, 2: 3}[self.model]
+        out = np.zeros((2 + nph) * nshell + (self.nx // 2 + 1) + (self.ny // 2 + 1))
+        n = L.ref_spectrum(os.fsencode(workdir), out.ctypes.data)
+        if n != nshell:
+            raise RuntimeError("ref_spectrum failed")
+        o = {"ek": out[:nshell], "ensk": out[nshell:2 * nshell]}
+        names = {1: ["sph"], 2: ["sph1", "sph2", "sp12"]}.get(self.model, [])
+        for k, nm in enumerate(names):
+            o[nm] = out[(2 + k) * nshell:(3 + k) * nshell]
+        b = (2 + nph) * nshell
+        o["ekx"] = out[b:b + self.nx // 2 + 1]
+        o["eky"] = out[b + self.nx // 2 + 1:]
+        return o
+
+    def perimeter(self) -> list:
+        """perimeter.c on the current state: (t, Sp_0, Sp_t, def) per phase field,
+        as printed with %g."""
+        L = self._L
+        L.ref_perimeter.argtypes = [ctypes.c_void_p]
+        out = np.zeros(8)
+        n = L.ref_perimeter(out.ctypes.data)
+        return [list(out[k:k + 4]) for k in range(0, n, 4)]
+
     def dfft(self, real):
         buf = np.zeros((self.nx, self.ny + 2))
         buf[:, : self.ny] = real

@@ -17,14 +17,19 @@
 #define _GNU_SOURCE
 #include "global.h"
 
+#include <math.h>
+#include <stdlib.h>
 #include <string.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #define API __attribute__((visibility("default")))
 
 void fftc_set_threads(int nthreads);
 
-static FILE *g_fe_stream, *g_fu_stream;
-static char *g_fe_buf, *g_fu_buf;
+static FILE *g_fe_stream, *g_fu_stream, *g_def_stream[2];
+static char *g_fe_buf, *g_fu_buf, *g_def_buf[2];
+static size_t g_def_len[2];
 static size_t g_fe_len, g_fu_len;
 
 API int ref_model(void)
@@ -150,6 +155,39 @@ API int ref_setup(int nthreads)
 #if defined BINARY || defined TERNARY
     g_fe_stream = open_memstream(&g_fe_buf, &g_fe_len);
     fe = g_fe_stream;
+#endif
+    /* spectrum() and perimeter() buffers (main.c:60-63, 104-127, 130-165, 182-185).
+     * main.c gives ekx / eky kxm / kym entries, but spectrum.c indexes them with
+     * (int)(|kx| / dk + 0.5) up to Nx/2, past the end; here they hold Nx/2 + 1. */
+    nshell = round(((double)Nx / sqrt(2.0)) + 1.0);
+    kxm = round(sqrt(kxmax * kxmax));
+    kym = round(sqrt(kymax * kymax));
+    ek = calloc(nshell, sizeof(double));
+    ensk = calloc(nshell, sizeof(double));
+    ekx = calloc((kxm > Nx / 2 + 1 ? kxm : Nx / 2 + 1), sizeof(double));
+    eky = calloc((kym > Ny / 2 + 1 ? kym : Ny / 2 + 1), sizeof(double));
+#ifdef BINARY
+    sph = calloc(nshell, sizeof(double));
+    ph = fftw_malloc((local_nx + 1) * (Ny + 2) * sizeof(double));
+    aph = fftw_malloc(Ny * sizeof(double));
+    bph = fftw_malloc(Ny * sizeof(double));
+    g_def_stream[0] = open_memstream(&g_def_buf[0], &g_def_len[0]);
+    fdef = g_def_stream[0];
+#endif
+#ifdef TERNARY
+    sph1 = calloc(nshell, sizeof(double));
+    sph2 = calloc(nshell, sizeof(double));
+    sp12 = calloc(nshell, sizeof(double));
+    ph1 = fftw_malloc((local_nx + 1) * (Ny + 2) * sizeof(double));
+    ph2 = fftw_malloc((local_nx + 1) * (Ny + 2) * sizeof(double));
+    aph1 = fftw_malloc(Ny * sizeof(double));
+    aph2 = fftw_malloc(Ny * sizeof(double));
+    bph1 = fftw_malloc(Ny * sizeof(double));
+    bph2 = fftw_malloc(Ny * sizeof(double));
+    g_def_stream[0] = open_memstream(&g_def_buf[0], &g_def_len[0]);
+    g_def_stream[1] = open_memstream(&g_def_buf[1], &g_def_len[1]);
+    fdef1 = g_def_stream[0];
+    fdef2 = g_def_stream[1];
 #endif
 
     kx = (double *)malloc(local_nx * sizeof(double));
@@ -302,6 +340,69 @@ API int ref_kinetic_energy(double *out, int nmax)
     kinetic_energy(cwz);
 #endif
     return last_line_values(g_fu_stream, &g_fu_buf, &g_fu_len, out, nmax);
+}
+
+/* spectrum() (spectrum.c:3-194) on the current state, run with `workdir` as the
+ * working directory (it writes spectra/spectrum.<ifile>, Xspectrum, Yspectrum
+ * there).  spectrum() truncates the phase fields in place; the state is restored
+ * afterwards.  out: ek, ensk, then sph (binary) or sph1, sph2, sp12 (ternary),
+ * nshell values each, then ekx and eky, Nx/2 + 1 values each.  Returns nshell. */
+API int ref_spectrum(const char *workdir, double *out)
+{
+    char here[4096];
+    const size_t nb = ncplx() * sizeof(fftw_complex);
+    double *keep = malloc(3 * nb);
+    if (!keep || !getcwd(here, sizeof(here)) || chdir(workdir) != 0) return -1;
+    mkdir("spectra", 0755);
+    memcpy(keep, cwz, nb);
+#ifdef BINARY
+    memcpy((char *)keep + nb, cphi, nb);
+    spectrum(cwz, cphi);
+    memcpy(cphi, (char *)keep + nb, nb);
+#elif defined TERNARY
+    memcpy((char *)keep + nb, cphi1, nb);
+    memcpy((char *)keep + 2 * nb, cphi2, nb);
+    spectrum(cwz, cphi1, cphi2);
+    memcpy(cphi1, (char *)keep + nb, nb);
+    memcpy(cphi2, (char *)keep + 2 * nb, nb);
+#else
+    spectrum(cwz);
+#endif
+    memcpy(cwz, keep, nb);
+    free(keep);
+    if (chdir(here) != 0) return -1;
+    double *o = out;
+    memcpy(o, ek, nshell * sizeof(double)); o += nshell;
+    memcpy(o, ensk, nshell * sizeof(double)); o += nshell;
+#ifdef BINARY
+    memcpy(o, sph, nshell * sizeof(double)); o += nshell;
+#elif defined TERNARY
+    memcpy(o, sph1, nshell * sizeof(double)); o += nshell;
+    memcpy(o, sph2, nshell * sizeof(double)); o += nshell;
+    memcpy(o, sp12, nshell * sizeof(double)); o += nshell;
+#endif
+    memcpy(o, ekx, (Nx / 2 + 1) * sizeof(double)); o += Nx / 2 + 1;
+    memcpy(o, eky, (Ny / 2 + 1) * sizeof(double));
+    return nshell;
+}
+
+/* perimeter() (perimeter.c:3-271) on the current state; out receives the values
+ * of the line(s) it printed (t, Sp_0, Sp_t, def; one line per phase field).
+ * Returns the number of values. */
+API int ref_perimeter(double *out)
+{
+#ifdef BINARY
+    perimeter(cphi);
+    return last_line_values(g_def_stream[0], &g_def_buf[0], &g_def_len[0], out, 4);
+#elif defined TERNARY
+    perimeter(cphi1, cphi2);
+    int a = last_line_values(g_def_stream[0], &g_def_buf[0], &g_def_len[0], out, 4);
+    int b = last_line_values(g_def_stream[1], &g_def_buf[1], &g_def_len[1], out + 4, 4);
+    return a + b;
+#else
+    (void)out;
+    return 0;
+#endif
 }
 
 /* Direct access to the reference's fft.c and functions.c on a caller buffer. */

@@ -80,6 +80,11 @@ def load_library(path: str = LIB_PATH):
     L.chns_profile_step.restype = ip
     L.chns_adjoint.argtypes = [vp, ip, ip, vp, vp, vp, vp, vp, ip]
     L.chns_adjoint.restype = ip
+    L.chns_spectrum_shells.argtypes = [vp]
+    L.chns_spectrum.argtypes = [vp, vp]
+    L.chns_spectrum.restype = ip
+    L.chns_perimeter.argtypes = [vp, vp]
+    L.chns_perimeter.restype = ip
     L.chns_write_fields.argtypes = [vp, ctypes.c_char_p, ip, ip]
     L.chns_write_fields.restype = ip
     L.chns_read_phase.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p]
@@ -209,6 +214,28 @@ class Context:
         a = np.ascontiguousarray(p1, np.float64)
         b = np.ascontiguousarray(p2, np.float64) if p2 is not None else None
         _check(self.L.chns_set_phase_real(self._h, _ptr(a), _ptr(b), HOST), "chns_set_phase_real")
+
+    def spectrum(self) -> dict:
+        """spectrum.c's shell spectra (ek, ensk, sph | sph1, sph2, sp12, ekx, eky);
+        the state is not modified."""
+        ns = self.L.chns_spectrum_shells(self._h)
+        nph = {0: 0, 1: 1, 2: 3}[self.model]
+        out = np.zeros((2 + nph) * ns + 2 * (self.nx // 2 + 1))
+        _check(self.L.chns_spectrum(self._h, _ptr(out)), "chns_spectrum")
+        o = {"ek": out[:ns], "ensk": out[ns:2 * ns]}
+        for k, nm in enumerate({1: ["sph"], 2: ["sph1", "sph2", "sp12"]}.get(self.model, [])):
+            o[nm] = out[(2 + k) * ns:(3 + k) * ns]
+        b = (2 + nph) * ns
+        o["ekx"] = out[b:b + self.nx // 2 + 1]
+        o["eky"] = out[b + self.nx // 2 + 1:]
+        return o
+
+    def perimeter(self) -> list:
+        """perimeter.c per phase field: dict(count1, count2, sp_0, sp_t, def)."""
+        out = np.zeros(10)
+        _check(self.L.chns_perimeter(self._h, _ptr(out)), "chns_perimeter")
+        keys = ("count1", "count2", "sp_0", "sp_t", "def")
+        return [dict(zip(keys, out[5 * f:5 * f + 5])) for f in range(self.model)]
 
     def write_fields(self, directory: str, index: int, truncate: bool = False):
         """main.c's dumps: <directory>/vort/wz.<index>, phase_field/phi[1|2].<index>,
