@@ -499,12 +499,33 @@ def run_gpu(args):
 
 
 def run_profile_case(args):
-    """The workload's FP32 context stepped --steps times, for an ncu capture."""
+    """A small, fixed piece of work for an ncu capture: "step" = the workload's FP32
+    context stepped --steps times; "adjoint" = one adjoint of --steps steps (K = 20)
+    at 512^2 FP64 after a warm-up call; "ensemble" = --steps ensemble steps of the
+    64-member ternary ensemble."""
     import torch
 
     import chns_b200 as C
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if args.profile_case == "adjoint":
+        import numpy as np
+
+        n = 512
+        noise = np.random.default_rng(2024).uniform(-0.05, 0.05, (n, n))
+        with C.Context(adjoint_params(n, C.FP64, 1e-4)) as c:
+            c.set_phase_real(0.5 * (1.0 + noise - noise.mean()))
+            c.adjoint(4, 20)
+            c.adjoint(args.steps, 20)
+        return
+    if args.profile_case == "ensemble":
+        members = ensemble_members()
+        with C.Ensemble([p for p, _ in members]) as ens:
+            for m, (_, ph) in zip(ens.members, members):
+                m.set_phase_real(*ph)
+            ens.step(args.steps)
+            ens.synchronize()
+        return
     n = args.n
     c0, w0 = initial_fields(n)
     with C.Context(workload_params(n, C.FP32, dt=args.dt)) as ctx:
@@ -685,8 +706,10 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=500, help="steps of the ensemble leg (0: skip)")
     ap.add_argument("--adjoint-big-steps", type=int, default=1000,
                     help="steps of the 4096^2 FP32 adjoint memory check (0: skip)")
-    ap.add_argument("--profile-case", action="store_true",
-                    help="only run --steps steps of the FP32 workload (for ncu captures); prints nothing")
+    ap.add_argument("--profile-case", nargs="?", const="step", default=None,
+                    choices=["step", "adjoint", "ensemble"],
+                    help="only run a small fixed case for ncu captures (step: --steps steps of the FP32 "
+                         "workload; adjoint; ensemble); prints nothing")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
