@@ -283,10 +283,13 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_inv(const Bufs<R> B, const Pa
   // outputs: 0 u, 1 v (velocity.c:12-42), 2 dx w, 3 dy w (nonlin.c:36-37); then per
   // phase field: c_t (surface_tension.c:20-22, nonlin.c:217, chem_potential.c:256-261),
   // dx c, dy c (surface_tension.c:57-58, nonlin.c:187-188, 272-273, 314-315).
-  // One loop with one inverse transform keeps the kernel small.
+  // One loop with one inverse transform keeps the kernel small.  The y derivative
+  // of c commutes with the x transform (ky is constant along the row), so dy c is
+  // i ky times the transformed c_t and gets no transform of its own.
   constexpr int NOUT = MODEL == MODEL_NS ? 4 : (MODEL == MODEL_BINARY ? 7 : 10);
 #pragma unroll 1
   for (int o = 0; o < NOUT; o++) {
+    if (o == 6 || o == 9) continue;  // dy c: stored with c_t
     if (o == 0 || o == 4 || o == 7) {
       const cx<R>* src = o == 0 ? B.w : (o == 4 ? B.c1 : B.c2);
 #pragma unroll
@@ -321,6 +324,9 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_inv(const Bufs<R> B, const Pa
     else if (q == 4) {
       if (MODEL == MODEL_BINARY) store_row<N>(v, B.g[GCT], row, live, t);
       else store_row_pair<N>(v, B.g[GCT], row, o < 7 ? 0 : 1, live, t);
+#pragma unroll
+      for (int m = 0; m < 16; m++) v[m] = mk<R>(-rmul(ky, v[m].y), rmul(ky, v[m].x));
+      store_row_pair<N>(v, B.g[o < 7 ? GD1 : GD2], row, 1, live, t);
     } else {
       store_row_pair<N>(v, B.g[o < 7 ? GD1 : GD2], row, q - 5, live, t);
     }
