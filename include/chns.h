@@ -106,6 +106,14 @@ int chns_rhs(chns_ctx *ctx, double *nw, double *nc1, double *nc2, int where);
 int chns_dfft(chns_ctx *ctx, const double *real, double *spec, int where);
 int chns_ifft(chns_ctx *ctx, const double *spec, double *real, int where);
 
+/* Failure detection: scans the state (and the FP32 k = 0 side channel) on the
+ * device for NaN or infinite values; CHNS_ERR_NONFINITE if there are any.  The
+ * reference has no such check (it aborts only through free_energy.c:151-154, which
+ * chns_diagnostics mirrors).  No call of this library waits on the device for
+ * another party (work is ordered by streams, events and graphs), so none can time
+ * out; CHNS_ERR_TIMEOUT is reserved. */
+int chns_check(chns_ctx *ctx);
+
 /* Free energy (free_energy.c:3-157) and kinetic energy (kinetic_energy.c:3-144)
  * of the current state: out_fe[2] = {bulk, gradient}; out_ke[3] = {<|u|^2/2>,
  * phase-1 mean, phase-2 mean}. */

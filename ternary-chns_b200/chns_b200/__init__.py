@@ -80,6 +80,8 @@ def load_library(path: str = LIB_PATH):
     L.chns_profile_step.restype = ip
     L.chns_adjoint.argtypes = [vp, ip, ip, vp, vp, vp, vp, vp, ip]
     L.chns_adjoint.restype = ip
+    L.chns_check.argtypes = [vp]
+    L.chns_check.restype = ip
     L.chns_spectrum_shells.argtypes = [vp]
     L.chns_spectrum.argtypes = [vp, vp]
     L.chns_spectrum.restype = ip
@@ -214,6 +216,10 @@ class Context:
         a = np.ascontiguousarray(p1, np.float64)
         b = np.ascontiguousarray(p2, np.float64) if p2 is not None else None
         _check(self.L.chns_set_phase_real(self._h, _ptr(a), _ptr(b), HOST), "chns_set_phase_real")
+
+    def check(self):
+        """Raises ChnsError (status -3) if the state holds NaN or infinite values."""
+        _check(self.L.chns_check(self._h), "chns_check")
 
     def spectrum(self) -> dict:
         """spectrum.c's shell spectra (ek, ensk, sph | sph1, sph2, sp12, ekx, eky);

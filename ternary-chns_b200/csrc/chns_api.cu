@@ -209,6 +209,14 @@ __global__ void k_k0_get(const double* k0, double* st, int slot) {
   st[1] = k0[2 * slot + 1];
 }
 
+// flag |= 1 when any of n reals is NaN or infinite
+template <class R> __global__ void k_nonfinite(const R* __restrict__ a, size_t n, unsigned int* flag) {
+  bool bad = false;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    bad |= !isfinite(a[i]);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
 int enqueue_step(chns_ctx* c) {
   int n1 = c->L->stage(c, 1);
   int n2 = c->L->stage(c, 2);
@@ -606,6 +614,25 @@ int chns_field_to_realdbl(chns_ctx* c, int f, int truncate) {
   }
   CK(cudaGetLastError());
   return CHNS_OK;
+}
+
+int chns_check(chns_ctx* c) {
+  if (!c) return CHNS_ERR_ARG;
+  unsigned int* flag = (unsigned int*)c->redscratch;
+  CK(cudaMemsetAsync(flag, 0, sizeof(unsigned int), c->stream));
+  const size_t nr = (size_t)c->n * c->nr * 2;  // reals per spectral field
+  for (int f = 0; f <= c->p.model; f++) {
+    if (c->f32)
+      k_nonfinite<float><<<1024, 256, 0, c->stream>>>((const float*)c->state[f], nr, flag);
+    else
+      k_nonfinite<double><<<1024, 256, 0, c->stream>>>((const double*)c->state[f], nr, flag);
+  }
+  if (c->f32) k_nonfinite<double><<<1, 32, 0, c->stream>>>(c->k0, 6, flag);
+  CK(cudaGetLastError());
+  unsigned int h = 0;
+  CK(cudaMemcpyAsync(&h, flag, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return h ? CHNS_ERR_NONFINITE : CHNS_OK;
 }
 
 int chns_diagnostics(chns_ctx* c, double* out_fe, double* out_ke) {

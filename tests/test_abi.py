@@ -67,5 +67,13 @@ def test_noalloc_rejects_sizes_before_touching_the_device(lib):
 
 
 def test_status_strings(lib):
-    for s in (0, -1, -2, -3, -4, -5, -6):
+    for s in (0, -1, -2, -3, -4, -5, -6, -7):
         assert lib.chns_status_string(s)
+    assert lib.chns_status_string(-7) != lib.chns_status_string(-99)
+
+
+def test_calls_reject_a_null_context_without_cuda(lib):
+    for fn in ("chns_step", "chns_check", "chns_synchronize", "chns_launches_per_step"):
+        f = getattr(lib, fn)
+        rc = f(None, 1) if fn == "chns_step" else f(None)
+        assert rc in (-1, 0) if fn == "chns_launches_per_step" else rc == -1, fn
