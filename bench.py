@@ -22,6 +22,9 @@ k = 0 modes in FP64.  A "step" is one full ETD2RK step (both stages).
              over the forward time of the same 200 steps, in FP64 and FP32,
              central differences along seeded directions, and a 4096^2 run of
              1000 steps (dt = 1.5e-7 for the same reason) for the memory budget
+  diagnostics / init : per-step diagnostics (free and kinetic energy, spectra,
+             perimeter) and init.c's initial conditions on the device at 4096^2,
+             beside the reference's own diagnostics on the host cores
   ensemble : 64 ternary runs (32 at 256^2, 24 at 512^2, 8 at 1024^2; own seeds
              and sigma_ij ~ U[0.15, 0.35] with every gamma_i >= 0.1; nu = 0.01,
              M = 0.005, eps = 2 dx; FP32)
@@ -178,6 +181,46 @@ def init_leg(C, n: int) -> dict:
     return out
 
 
+def diagnostics_leg(C, n: int, st0, cpu: bool) -> dict:
+    """Wall time (each call ends with a synchronize) of the per-step diagnostics at
+    n^2 on the bench state: free and kinetic energy (chns_diagnostics), spectra
+    (chns_spectrum), perimeter (chns_perimeter), FP32 and FP64 contexts; with
+    cpu=True also the reference's own free_energy(), kinetic_energy(), spectrum()
+    and perimeter() (oracle/_ref/bin<n>, oracle FFT on all host threads)."""
+    import tempfile
+
+    out = {"grid": n}
+    for prec, key in ((C.FP32, "gpu_fp32_ms"), (C.FP64, "gpu_fp64_ms")):
+        with C.Context(workload_params(n, prec)) as c:
+            c.set_state(*st0)
+            c.diagnostics(), c.spectrum(), c.perimeter()  # warm
+            t = {}
+            for nm, fn in (("energies", c.diagnostics), ("spectrum", c.spectrum), ("perimeter", c.perimeter)):
+                t0 = time.perf_counter()
+                fn()
+                t[nm] = round((time.perf_counter() - t0) * 1e3, 3)
+            out[key] = t
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        name = f"bin{n}"
+        if os.path.isfile(O.build_ref.lib_path(name)):
+            thr = os.cpu_count() or 1
+            R = O.RefLib(name, nthreads=thr)
+            R.set_state(*st0)
+            t = {}
+            work = tempfile.mkdtemp()
+            for nm, fn in (("free_energy", R.free_energy), ("kinetic_energy", R.kinetic_energy),
+                           ("spectrum", lambda: R.spectrum(work)), ("perimeter", R.perimeter)):
+                t0 = time.perf_counter()
+                fn()
+                t[nm] = round((time.perf_counter() - t0) * 1e3, 1)
+            out["reference_cpu_ms"] = t
+            out["reference_cores"] = thr
+    return out
+
+
 def replica_throughput(ms: float, steps: int, world: int, device: str):
     """Whole-job steps/s of `world` independent replicas (one per rank and GPU, no
     data-path collective): every rank ran `steps` steps in `ms` milliseconds; the
@@ -238,8 +281,10 @@ def adjoint_leg(C, stream, big_steps: int):
             leg = {"forward_ms": round(t_fwd, 3), "adjoint_ms": round(t_adj, 3), "ratio": round(t_adj / t_fwd, 3),
                    "J": J, "dJ_dnu": gp[0], "dJ_dM": gp[1], "dJ_dsigma": gp[2]}
             if prec == C.FP64:
-                # central differences of J along seeded smooth directions of c_hat_0
-                errs = []
+                # central differences of J along seeded smooth directions of c_hat_0, at
+                # h = 1e-6 and 1e-5 (J ~ 1.6e3: the rounding of J limits h = 1e-6 to
+                # ~eps J / (h |dJ|) relative; the O(h^2) error of 1e-5 is ~1e-10)
+                fds = []
                 mx = np.minimum(np.arange(n), n - np.arange(n))
                 kk = np.sqrt(mx[:, None] ** 2 + np.arange(n // 2 + 1)[None, :] ** 2)
                 for k in range(2):
@@ -247,15 +292,17 @@ def adjoint_leg(C, stream, big_steps: int):
                     d *= np.exp(-kk / 8.0)
                     d *= np.abs(st0[1]).ravel()[1:].max() / np.abs(d).max()
                     d[0, 0] = 0.0
-                    h = 1e-6
-                    js = []
-                    for sgn in (1, -1):
-                        c.set_state(st0[0], st0[1] + sgn * h * d)
-                        js.append(c.adjoint(steps, ckpt)[0])
-                    fd = (js[0] - js[1]) / (2 * h)
                     ad = float(np.sum(gc.real * d.real + gc.imag * d.imag))
-                    errs.append(abs(ad - fd) / abs(fd))
-                leg["fd_rel_err"] = errs
+                    row = {"adjoint": ad}
+                    for h in (1e-6, 1e-5):
+                        js = []
+                        for sgn in (1, -1):
+                            c.set_state(st0[0], st0[1] + sgn * h * d)
+                            js.append(c.adjoint(steps, ckpt)[0])
+                        fd = (js[0] - js[1]) / (2 * h)
+                        row[f"rel_err_h{h:g}"] = abs(ad - fd) / abs(fd)
+                    fds.append(row)
+                leg["fd"] = fds
                 g64 = (gc, gp)
             else:
                 leg["rel_diff_vs_fp64_dJ_dc"] = float(np.linalg.norm(gc - g64[0]) / np.linalg.norm(g64[0]))
@@ -448,6 +495,7 @@ def run_gpu(args):
         del res
 
     init = init_leg(C, n) if rank == 0 else None
+    diag = diagnostics_leg(C, n, st0, not args.no_cpu_baseline) if rank == 0 else None
     adj = adjoint_leg(C, stream, args.adjoint_big_steps) if args.adjoint and rank == 0 else None
     ens = ensemble_leg(C, args.ensemble_steps) if args.ensemble_steps > 0 and rank == 0 else None
 
@@ -482,6 +530,7 @@ def run_gpu(args):
             "fp32_over_fp64": round((value / world) / fp64_sps, 3),
             "fp32_vs_fp64": acc,
             "init": init,
+            "diagnostics": diag,
             "adjoint": adj,
             "ensemble": ens,
             "per_kernel_ms": prof["per_kernel_ms"],

@@ -113,6 +113,7 @@ constexpr int PSET = 9;                                    // physical fields pe
 enum { PU = 0, PV, PWX, PWY, PCT, PCX, PCY, PMU, PFT };     // forward fields, f(c_t)
 enum { PFB = 2 * PSET, PAB, PBB, PFXB, PFYB, PUB, PVB, PWXB, PWYB, PCTB, PCXB, PCYB, NPHYS };
 constexpr int SLOT_FIELDS = 8;
+constexpr int kLossBlocks = 1024;  // blocks of the loss reduction
 
 template <class R> struct Adj {
   chns_ctx* c;
@@ -248,7 +249,8 @@ int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
     if (cudaMalloc(&a->spec, NSPEC * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMalloc(&a->phys, NPHYS * nn * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMalloc(&a->bscr, 2 * FOP_N * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
-    if (cudaMalloc((void**)&a->acc, 8 * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
+    // 8 accumulators, then 3 per-block partials of each loss block
+    if (cudaMalloc((void**)&a->acc, (8 + 3 * kLossBlocks) * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
     // derivative tables of the ETD coefficients: d/dnu (w), d/dlambda, d/dsigma (c)
     const int nr = c->nr;
     const chns_params& p = c->p;
@@ -371,8 +373,9 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
     const double kg = (lw[1] * 0.75 * p.sigma * p.epsilon + 4.0 * lw[2]) * inv;
     const double dkb = lw[0] * 12.0 / p.epsilon * inv;
     const double dkg = lw[1] * 0.75 * p.epsilon * inv;
-    k_adj_loss<R><<<A.blocks_p, 256, 0, st>>>(A.FS(0, PCT), A.FS(0, PCX), A.FS(0, PCY), A.F(PUB), A.F(PVB),
-                                              A.F(PWXB), A.nn, kb, kg, dkb, dkg, a->acc);
+    k_adj_loss<R><<<kLossBlocks, 256, 0, st>>>(A.FS(0, PCT), A.FS(0, PCX), A.FS(0, PCY), A.F(PUB), A.F(PVB),
+                                               A.F(PWXB), A.nn, kb, kg, dkb, dkg, a->acc + 8);
+    k_sum_parts<<<1, 32, 0, st>>>(a->acc + 8, kLossBlocks, a->acc);
     A.dfft(st, 0, A.F(PUB), A.SS(0, SB), 3);
     k_adj_loss_acc3<R><<<A.blocks_s, 256, 0, st>>>(A.P, A.SS(0, SB), A.S(SGC), A.S(SGW), A.ncx);
   }

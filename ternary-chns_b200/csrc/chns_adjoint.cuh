@@ -58,6 +58,35 @@ template <class R> __device__ __forceinline__ double rdot(cx<R> a, cx<R> b) {
   return (double)a.x * (double)b.x + (double)a.y * (double)b.y;
 }
 
+// block sums of 3 doubles written to part[3 blockIdx.x + k] (no atomics: the
+// final sum in k_sum_parts has a fixed order, so the result is reproducible)
+__device__ __forceinline__ void block_part3(double a0, double a1, double a2, double* part) {
+  __shared__ double red[3][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, o);
+    a1 += __shfl_down_sync(0xffffffffu, a1, o);
+    a2 += __shfl_down_sync(0xffffffffu, a2, o);
+  }
+  if (lane == 0) { red[0][wid] = a0; red[1][wid] = a1; red[2][wid] = a2; }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[threadIdx.x][w];
+    part[3 * blockIdx.x + threadIdx.x] = s;
+  }
+}
+
+// acc[k] += sum over nblk blocks of part[3 b + k], k = 0..2, in a fixed order (one block of 32)
+__global__ void k_sum_parts(const double* __restrict__ part, int nblk, double* acc) {
+  if (threadIdx.x < 3) {
+    double s = 0.0;
+    for (int b = 0; b < nblk; b++) s += part[3 * b + threadIdx.x];
+    acc[threadIdx.x] += s;
+  }
+}
+
 // block sum of up to 3 doubles, added atomically to acc[0..2]
 __device__ __forceinline__ void block_acc3(double a0, double a1, double a2, double* acc) {
   __shared__ double red[3][32];
@@ -327,9 +356,9 @@ __global__ void k_adj_etd1(const AdjPar<R> P, const R* __restrict__ coef, const 
 template <class R>
 __global__ void k_adj_loss(const R* __restrict__ c, const R* __restrict__ cxp, const R* __restrict__ cyp,
                            R* __restrict__ cb, R* __restrict__ cxb, R* __restrict__ cyb, size_t nn, double kb,
-                           double kg, double dkb, double dkg, double* acc) {
+                           double kg, double dkb, double dkg, double* part) {
   // per point: J = kb c^2 (1-c)^2 + kg (cx^2 + cy^2), kb/kg include 1/n^2;
-  // acc[0] += J, acc[2] += d J / d sigma through kb, kg (dkb, dkg)
+  // per-block partials of J and of d J / d sigma through kb, kg (dkb, dkg)
   double sj = 0.0, ssg = 0.0;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
     const double a = c[k], x = cxp[k], y = cyp[k];
@@ -340,7 +369,7 @@ __global__ void k_adj_loss(const R* __restrict__ c, const R* __restrict__ cxp, c
     cxb[k] = (R)(kg * 2.0 * x);
     cyb[k] = (R)(kg * 2.0 * y);
   }
-  block_acc3(sj, 0.0, ssg, acc);
+  block_part3(sj, 0.0, ssg, part);
 }
 
 // the untruncated c, i kx c, i ky c (free_energy.c) as one batch

@@ -67,7 +67,7 @@ def test_adjoint_matches_finite_differences(setup):
         J, gw, gc, gpar = c.adjoint(STEPS, CKPT)
     assert abs(J - forward_loss(C, p, [w0, c0])) <= 1e-12 * abs(J)
     rng = np.random.default_rng(3)
-    for k in range(4):
+    for k in range(8):
         # smooth real perturbations of c and omega
         dc = np.fft.rfft2(rng.standard_normal((n, n)))
         dw = np.fft.rfft2(rng.standard_normal((n, n)))
