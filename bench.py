@@ -72,19 +72,15 @@ DT_DEFAULT = 2e-6
 
 
 def workload_params(n: int, precision: int, coef_mode: int = 1, dt: float = DT_DEFAULT) -> dict:
-    lx = 2 * math.pi
-    p = dict(model=1, precision=precision, nx=n, ny=n, lx=lx, ly=lx, dt=dt, nu=1e-3, sigma=0.1,
-             epsilon=2.0 * (lx / n), coef_mode=coef_mode, force_amp=1.0, force_k=4.0)
-    p["lambda"] = 1e-3
-    return p
+    from chns_b200 import configs
+
+    return configs.binary(n, dt, 1e-3, 1e-3, 0.1, precision, coef_mode, force_amp=1.0, force_k=4.0)
 
 
 def initial_fields(n: int):
-    from chns_b200 import fields
+    from chns_b200 import configs
 
-    lx = 2 * math.pi
-    c0 = fields.drops_binary(n, 42, ndrops=64, radius=0.3, lx=lx, epsilon=2.0 * (lx / n))
-    w0 = fields.random_vorticity_hat(n, 43, kmax=8.0, rms=0.1, lx=lx)
+    _, c0, w0 = configs.binary_kolmogorov(n)
     return c0, w0
 
 
@@ -237,11 +233,9 @@ def replica_throughput(ms: float, steps: int, world: int, device: str):
 
 
 def adjoint_params(n: int, precision: int, dt: float) -> dict:
-    lx = 2 * math.pi
-    p = dict(model=1, precision=precision, nx=n, ny=n, lx=lx, ly=lx, dt=dt, nu=0.01, sigma=0.2,
-             epsilon=2.0 * (lx / n), coef_mode=1)
-    p["lambda"] = 0.005
-    return p
+    from chns_b200 import configs
+
+    return configs.binary_adjoint(n, precision, dt)[0]
 
 
 def adjoint_leg(C, stream, big_steps: int):
@@ -249,11 +243,10 @@ def adjoint_leg(C, stream, big_steps: int):
     import numpy as np
     import torch
 
+    from chns_b200 import configs
+
     n, steps, ckpt = 512, 200, 20
-    rng = np.random.default_rng(2024)
-    noise = rng.uniform(-0.05, 0.05, (n, n))
-    phi = noise - noise.mean()
-    c_real = 0.5 * (1.0 + phi)
+    c_real = configs.binary_adjoint(n)[1]
     out = {"grid": n, "steps": steps, "ckpt": ckpt, "loss": "E_bulk + E_grad + <|grad phi|^2> at the final step"}
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -338,40 +331,16 @@ def adjoint_leg(C, stream, big_steps: int):
     return out
 
 
-# (grid, members, dt): the explicit chemical-potential term grows as n^3 / gamma_min
-ENSEMBLE_GROUPS = ((256, 32, 1e-4), (512, 24, 2.5e-5), (1024, 8, 3e-6))
-
-
-def draw_sigmas(rng):
-    """sigma_12, sigma_13, sigma_23 ~ U[0.15, 0.35], redrawn until every spreading
-    coefficient gamma_i (main.c:166-170) is >= 0.1: a draw with gamma_i near or
-    below 0 is an ill-posed (negative surface tension) run."""
-    while True:
-        s12, s13, s23 = rng.uniform(0.15, 0.35, 3)
-        if min(s12 + s13 - s23, s12 + s23 - s13, s13 + s23 - s12) >= 0.1:
-            return float(s12), float(s13), float(s23)
-
-
 def ensemble_members(seed: int = 3000):
-    import numpy as np
+    from chns_b200 import configs
 
-    rng = np.random.default_rng(seed)
-    out = []
-    for n, count, dt in ENSEMBLE_GROUPS:
-        for _ in range(count):
-            lx = 2 * math.pi
-            s12, s13, s23 = draw_sigmas(rng)
-            p = dict(model=2, precision=1, nx=n, ny=n, lx=lx, ly=lx, dt=dt, nu=0.01, epsilon=2.0 * lx / n,
-                     sigma12=s12, sigma13=s13, sigma23=s23, coef_mode=1)
-            p["lambda"] = 0.005
-            ph = (1 / 3 + 0.02 * rng.uniform(-1, 1, (n, n)), 1 / 3 + 0.02 * rng.uniform(-1, 1, (n, n)))
-            out.append((p, ph))
-    return out
+    return configs.ternary_ensemble(seed)
 
 
 def ensemble_leg(C, steps: int):
     """Throughput of the 64-member ternary ensemble, together and one by one."""
     import numpy as np
+    from chns_b200.configs import ENSEMBLE_GROUPS
 
     members = ensemble_members()
     pts = sum(p["nx"] * p["ny"] for p, _ in members)
@@ -558,12 +527,11 @@ def run_profile_case(args):
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     if args.profile_case == "adjoint":
-        import numpy as np
+        from chns_b200 import configs
 
-        n = 512
-        noise = np.random.default_rng(2024).uniform(-0.05, 0.05, (n, n))
-        with C.Context(adjoint_params(n, C.FP64, 1e-4)) as c:
-            c.set_phase_real(0.5 * (1.0 + noise - noise.mean()))
+        p, c_real = configs.binary_adjoint(512, C.FP64)
+        with C.Context(p) as c:
+            c.set_phase_real(c_real)
             c.adjoint(4, 20)
             c.adjoint(args.steps, 20)
         return

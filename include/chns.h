@@ -119,6 +119,16 @@ int chns_check(chns_ctx *ctx);
  * phase-1 mean, phase-2 mean}. */
 int chns_diagnostics(chns_ctx *ctx, double *out_fe, double *out_ke);
 
+/* Checkpoint / resume.  The reference cannot restart bit for bit (its dumps are
+ * real-space and truncated, main.c:332-359; INIT_READ_DATA reads only the phase
+ * fields).  chns_save writes the context's parameters and its spectral state
+ * (FFTW layout, FP64: FP32 states convert exactly and their k = 0 modes are kept in
+ * double) to `path`; chns_load reads such a file into a context created with the
+ * same parameters (else CHNS_ERR_ARG).  Steps after a load are bit-identical to the
+ * steps the saved context would have taken. */
+int chns_save(chns_ctx *ctx, const char *path);
+int chns_load(chns_ctx *ctx, const char *path);
+
 /* Shell spectra of the current state (spectrum.c:3-194), without spectrum.c's side
  * effect (it truncates the phase fields in place).  nshell = chns_spectrum_shells
  * = round(nx/sqrt(2) + 1) (main.c:60); shell (int)(|k|/dk + 0.5), dk = 2 pi / lx.

@@ -298,6 +298,17 @@ class RefLib:
         o["eky"] = out[b + self.nx // 2 + 1:]
         return o
 
+    def last_line(self, which: int) -> str:
+        """The last line the reference printed to a log (0 free_en_t.dat, 1 ken_t.dat,
+        2 gamma.dat / gamma1.dat, 3 gamma2.dat)."""
+        L = self._L
+        L.ref_last_line.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        buf = ctypes.create_string_buffer(4096)
+        n = L.ref_last_line(which, buf, 4096)
+        if n < 0:
+            raise RuntimeError("no line")
+        return buf.value.decode()
+
     def perimeter(self) -> list:
         """perimeter.c on the current state: (t, Sp_0, Sp_t, def) per phase field,
         as printed with %g."""

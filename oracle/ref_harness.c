@@ -405,6 +405,28 @@ API int ref_perimeter(double *out)
 #endif
 }
 
+/* The last line the reference printed to one of its logs (0 free_en_t.dat,
+ * 1 ken_t.dat, 2 gamma.dat / gamma1.dat, 3 gamma2.dat), without the newline.
+ * Returns its length, or -1. */
+API int ref_last_line(int which, char *out, int cap)
+{
+    FILE *s[4] = {g_fe_stream, g_fu_stream, g_def_stream[0], g_def_stream[1]};
+    char **b[4] = {&g_fe_buf, &g_fu_buf, &g_def_buf[0], &g_def_buf[1]};
+    size_t *l[4] = {&g_fe_len, &g_fu_len, &g_def_len[0], &g_def_len[1]};
+    if (which < 0 || which > 3 || !s[which]) return -1;
+    fflush(s[which]);
+    if (!*b[which] || *l[which] == 0) return -1;
+    char *end = *b[which] + *l[which];
+    while (end > *b[which] && end[-1] == '\n') end--;
+    char *line = end;
+    while (line > *b[which] && line[-1] != '\n') line--;
+    int n = (int)(end - line);
+    if (n >= cap) return -1;
+    memcpy(out, line, n);
+    out[n] = 0;
+    return n;
+}
+
 /* Direct access to the reference's fft.c and functions.c on a caller buffer. */
 API void ref_dfft(double *padded) { dfft(padded, (fftw_complex *)padded); }
 API void ref_ifft(double *padded) { ifft((fftw_complex *)padded, padded); }

@@ -87,6 +87,10 @@ def load_library(path: str = LIB_PATH):
     L.chns_spectrum.restype = ip
     L.chns_perimeter.argtypes = [vp, vp]
     L.chns_perimeter.restype = ip
+    L.chns_save.argtypes = [vp, ctypes.c_char_p]
+    L.chns_save.restype = ip
+    L.chns_load.argtypes = [vp, ctypes.c_char_p]
+    L.chns_load.restype = ip
     L.chns_write_fields.argtypes = [vp, ctypes.c_char_p, ip, ip]
     L.chns_write_fields.restype = ip
     L.chns_read_phase.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p]
@@ -242,6 +246,14 @@ class Context:
         _check(self.L.chns_perimeter(self._h, _ptr(out)), "chns_perimeter")
         keys = ("count1", "count2", "sp_0", "sp_t", "def")
         return [dict(zip(keys, out[5 * f:5 * f + 5])) for f in range(self.model)]
+
+    def save(self, path: str):
+        """Checkpoint: parameters and spectral state, for a bit-exact resume."""
+        _check(self.L.chns_save(self._h, os.fsencode(path)), "chns_save")
+
+    def load(self, path: str):
+        """Resume from a chns_save file written with the same parameters."""
+        _check(self.L.chns_load(self._h, os.fsencode(path)), "chns_load")
 
     def write_fields(self, directory: str, index: int, truncate: bool = False):
         """main.c's dumps: <directory>/vort/wz.<index>, phase_field/phi[1|2].<index>,

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <errno.h>
 #include <stdio.h>
+#include <string.h>
 #include <sys/stat.h>
 
 #include <string>
@@ -79,6 +80,82 @@ int chns_read_phase(chns_ctx* c, const char* path1, const char* path2) {
     if (rc) return rc;
   }
   return chns_set_phase_real(c, a.data(), b.empty() ? nullptr : b.data(), CHNS_HOST);
+}
+
+// checkpoint file: magic, the chns_params the context was created with (padding
+// zeroed), then the spectral fields (FFTW layout, FP64) of the model
+static const char kCkptMagic[8] = {'C', 'H', 'N', 'S', 'C', 'K', 'P', '1'};
+
+static chns_params canonical(const chns_params& a) {
+  chns_params q;
+  memset(&q, 0, sizeof(q));
+  q.model = a.model;
+  q.precision = a.precision;
+  q.nx = a.nx;
+  q.ny = a.ny;
+  q.lx = a.lx;
+  q.ly = a.ly;
+  q.dt = a.dt;
+  q.nu = a.nu;
+  q.lambda = a.lambda;
+  q.sigma = a.sigma;
+  q.epsilon = a.epsilon;
+  q.sigma12 = a.sigma12;
+  q.sigma13 = a.sigma13;
+  q.sigma23 = a.sigma23;
+  q.xlambda = a.xlambda;
+  q.dealias_div = a.dealias_div;
+  q.coef_mode = a.coef_mode;
+  q.force_amp = a.force_amp;
+  q.force_k = a.force_k;
+  return q;
+}
+
+int chns_save(chns_ctx* c, const char* path) {
+  if (!c || !path) return CHNS_ERR_ARG;
+  const size_t ncx = (size_t)c->n * c->nr;
+  std::vector<double> f[3];
+  for (int k = 0; k <= c->p.model; k++) f[k].resize(2 * ncx);
+  int rc = chns_get_state(c, f[0].data(), c->p.model >= 1 ? f[1].data() : nullptr,
+                          c->p.model == 2 ? f[2].data() : nullptr, CHNS_HOST);
+  if (rc) return rc;
+  FILE* fp = fopen(path, "wb");
+  if (!fp) return CHNS_ERR_IO;
+  const chns_params q = canonical(c->p);
+  bool ok = fwrite(kCkptMagic, 1, sizeof(kCkptMagic), fp) == sizeof(kCkptMagic) &&
+            fwrite(&q, sizeof(chns_params), 1, fp) == 1;
+  for (int k = 0; ok && k <= c->p.model; k++) ok = fwrite(f[k].data(), sizeof(double), f[k].size(), fp) == f[k].size();
+  ok = (fclose(fp) == 0) && ok;
+  return ok ? CHNS_OK : CHNS_ERR_IO;
+}
+
+int chns_load(chns_ctx* c, const char* path) {
+  if (!c || !path) return CHNS_ERR_ARG;
+  FILE* fp = fopen(path, "rb");
+  if (!fp) return CHNS_ERR_IO;
+  char magic[8];
+  chns_params p;
+  bool ok = fread(magic, 1, sizeof(magic), fp) == sizeof(magic) && memcmp(magic, kCkptMagic, sizeof(magic)) == 0 &&
+            fread(&p, sizeof(p), 1, fp) == 1;
+  if (!ok) {
+    fclose(fp);
+    return CHNS_ERR_IO;
+  }
+  const chns_params q = canonical(c->p), r = canonical(p);
+  if (memcmp(&q, &r, sizeof(q)) != 0) {  // another configuration
+    fclose(fp);
+    return CHNS_ERR_ARG;
+  }
+  const size_t ncx = (size_t)c->n * c->nr;
+  std::vector<double> f[3];
+  for (int k = 0; ok && k <= c->p.model; k++) {
+    f[k].resize(2 * ncx);
+    ok = fread(f[k].data(), sizeof(double), f[k].size(), fp) == f[k].size();
+  }
+  fclose(fp);
+  if (!ok) return CHNS_ERR_IO;
+  return chns_set_state(c, f[0].data(), c->p.model >= 1 ? f[1].data() : nullptr,
+                        c->p.model == 2 ? f[2].data() : nullptr, CHNS_HOST);
 }
 
 }  // extern "C"

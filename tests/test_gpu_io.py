@@ -70,3 +70,50 @@ def test_read_phase_equals_set_phase_real(chns, tmp_path):
         with pytest.raises(chns.ChnsError) as e:
             c1.read_phase(str(tmp_path / "missing.in"), str(tmp_path / "phi2.in"))
         assert e.value.status == -7
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("name", ["bin32", "ter32", "ns32"])
+def test_checkpoint_resume_is_bit_exact(chns, tmp_path, name, prec):
+    g = load_small(name)
+    p = dict(g["params"], precision=prec)
+    path = str(tmp_path / "run.ckpt")
+    with chns.Context(p) as a:
+        a.set_state(*g["init"])
+        a.step(7)
+        a.save(path)
+        a.step(9)
+        want = a.get_state()
+    with chns.Context(p) as b:
+        b.load(path)
+        b.step(9)
+        got = b.get_state()
+    for x, y in zip(got, want):
+        assert np.array_equal(x, y)
+    # a context with other parameters refuses the file
+    with chns.Context(dict(p, dt=p["dt"] * 2)) as c:
+        with pytest.raises(chns.ChnsError) as e:
+            c.load(path)
+        assert e.value.status == -1
+
+
+@pytest.mark.parametrize("name", ["bin32", "ter32", "ns32"])
+def test_logs_write_the_reference_files(chns, tmp_path, name):
+    from chns_b200 import logs
+
+    g = load_small(name)
+    p = g["params"]
+    with chns.Context(p) as c:
+        c.set_state(*g["init"])
+        lg = logs.Logs(c, str(tmp_path))
+        lg.record(0.0)
+        c.step(2)
+        lg.record(2 * p["dt"])
+    names = {0: ["ken_t.dat"], 1: ["free_en_t.dat", "ken_t.dat", "gamma.dat"],
+             2: ["free_en_t.dat", "ken_t.dat", "gamma1.dat", "gamma2.dat"]}[p["model"]]
+    for nm in names:
+        lines = open(tmp_path / "data" / nm).read().splitlines()
+        assert len(lines) == 2, nm
+    for i in (0, 1):
+        for stem in ("spectrum", "Xspectrum", "Yspectrum"):
+            assert (tmp_path / "spectra" / f"{stem}.{i}").stat().st_size > 0
