@@ -178,16 +178,19 @@ int chns_init_phase(chns_ctx *ctx, int kind, unsigned int seed);
 int chns_write_fields(chns_ctx *ctx, const char *dir, int index, int truncate);
 int chns_read_phase(chns_ctx *ctx, const char *path1, const char *path2);
 
-/* Discrete adjoint of `nsteps` ETD2RK steps of the binary model (etd2rk.c with
- * nonlin.c / surface_tension.c transposed operation by operation) from the
- * current state.  Loss at the final state, with c and grad c untruncated as in
- * free_energy.c:3-157:
- *   J = w[0] E_bulk + w[1] E_grad + w[2] <|grad phi|^2>,  phi = 2c - 1
- * (loss_w = NULL: all weights 1).  Outputs: *J; dJ/d(omega_hat_0), dJ/d(c_hat_0)
- * in FFTW layout (gradients with respect to the stored real and imaginary
- * parts; g_w / g_c may be NULL); g_params[3] = dJ/d(nu, lambda, sigma).  The
- * state is kept every `ckpt` steps and recomputed in between.  The state is
- * unchanged on return.  Other models return CHNS_ERR_UNSUPPORTED. */
+/* Discrete adjoint of `nsteps` ETD2RK steps (etd2rk.c with nonlin.c /
+ * surface_tension.c / chem_potential.c transposed operation by operation) from
+ * the current state.  Loss at the final state, with c and grad c untruncated as in
+ * free_energy.c:3-157 (loss_w = NULL: all weights 1):
+ *   binary  J = w[0] E_bulk + w[1] E_grad + w[2] <|grad phi|^2>,  phi = 2c - 1
+ *   ternary J = w[0] E_bulk + w[1] E_grad + w[2] <|grad c1|^2 + |grad c2|^2>
+ * Outputs: *J; dJ/d(omega_hat_0) in g_w and dJ/d(c_hat_0) (binary) or dJ/d(c1_hat_0)
+ * followed by dJ/d(c2_hat_0) (ternary) in g_c, FFTW layout (gradients with respect
+ * to the stored real and imaginary parts; g_w / g_c may be NULL); g_params =
+ * dJ/d(nu, lambda, sigma) (binary, 3 values) or dJ/d(nu, lambda, sigma_12,
+ * sigma_13, sigma_23) (ternary, 5 values).  The state is kept every `ckpt` steps
+ * and recomputed in between; it is unchanged on return.  Pure Navier-Stokes
+ * contexts return CHNS_ERR_UNSUPPORTED. */
 int chns_adjoint(chns_ctx *ctx, int nsteps, int ckpt, const double *loss_w, double *J, double *g_w,
                  double *g_c, double *g_params, int where);
 

@@ -309,18 +309,20 @@ class Context:
         return fe, ke, rc
 
     def adjoint(self, nsteps: int, ckpt: int = 20, loss_w=(1.0, 1.0, 1.0)):
-        """Discrete adjoint of `nsteps` binary ETD2RK steps from the current state.
-        Returns (J, dJ/d omega_hat_0, dJ/d c_hat_0, dJ/d(nu, lambda, sigma)); the
-        state is unchanged.  J = w0 E_bulk + w1 E_grad + w2 <|grad phi|^2> at the
-        final state (phi = 2c - 1)."""
+        """Discrete adjoint of `nsteps` ETD2RK steps from the current state (binary or
+        ternary).  Returns (J, dJ/d omega_hat_0, dJ/d c_hat_0, dJ/d params): for the
+        binary model dJ/d c_hat_0 is one array and the parameters are (nu, lambda,
+        sigma); for the ternary model it is a pair (c1, c2) and the parameters are
+        (nu, lambda, sigma_12, sigma_13, sigma_23).  The state is unchanged."""
         lw = np.ascontiguousarray(loss_w, np.float64)
         J = np.zeros(1)
         gw = np.empty(self.shape, np.complex128)
-        gc = np.empty(self.shape, np.complex128)
-        gp = np.zeros(3)
+        nc = max(self.model, 1)
+        gc = np.empty((nc,) + self.shape, np.complex128)
+        gp = np.zeros(3 if self.model == MODEL_BINARY else 5)
         _check(self.L.chns_adjoint(self._h, int(nsteps), int(ckpt), _ptr(lw), _ptr(J), _ptr(gw), _ptr(gc),
                                    _ptr(gp), HOST), "chns_adjoint")
-        return float(J[0]), gw, gc, gp
+        return float(J[0]), gw, (gc[0] if self.model == MODEL_BINARY else (gc[0], gc[1])), gp
 
     def launches_per_step(self) -> int:
         return self.L.chns_launches_per_step(self._h)

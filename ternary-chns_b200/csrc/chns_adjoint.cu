@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "chns_adjoint.cuh"
+#include "chns_adjoint_t.cuh"
 #include "chns_internal.h"
 
 namespace {
@@ -112,16 +113,74 @@ enum {
 constexpr int PSET = 9;                                    // physical fields per set
 enum { PU = 0, PV, PWX, PWY, PCT, PCX, PCY, PMU, PFT };     // forward fields, f(c_t)
 enum { PFB = 2 * PSET, PAB, PBB, PFXB, PFYB, PUB, PVB, PWXB, PWYB, PCTB, PCXB, PCYB, NPHYS };
-constexpr int SLOT_FIELDS = 8;
 constexpr int kLossBlocks = 1024;  // blocks of the loss reduction
+constexpr int kAcc = 32;           // accumulators; the loss reduction's per-block partials follow
 
 template <class R> struct Adj {
+  static constexpr int NF = 2, NSPEC_ = NSPEC, NPHYS_ = NPHYS, NBSCR = FOP_N, NDCOEF = 9;
   chns_ctx* c;
   chns_adj* a;
   AdjPar<R> P;
   cudaStream_t st;
   size_t ncx, nn;
   int blocks_s, blocks_p;
+
+  int cur0() const { return CUW; }
+  cx<R>* grad(int f) const { return S(SGW + f); }
+  void setup() {
+    const chns_params& p = c->p;
+    P.n = c->n;
+    P.jt = c->jt;
+    P.fx = c->fx;
+    P.fy = c->fy;
+    P.s1 = (R)(1.5 * p.sigma * p.epsilon);
+    P.s2 = (R)(24.0 * (p.sigma / p.epsilon));
+    P.lam = (R)p.lambda;
+    P.ds1 = 1.5 * p.epsilon;
+    P.ds2 = 24.0 / p.epsilon;
+    P.mrow = c->mrow;
+  }
+  // d/dnu of the w coefficients, d/dlambda and d/dsigma of the c coefficients
+  static void dcoef_tables(const chns_ctx* c, std::vector<double>& d) {
+    const int nr = c->nr;
+    const chns_params& p = c->p;
+    const size_t t = (size_t)nr * nr;
+    d.assign(NDCOEF * t, 0.0);
+    for (int j = 0; j < nr; j++)
+      for (int m = 0; m < nr; m++) {
+        const double kx = c->fx * m, ky = c->fy * j, ks = kx * kx + ky * ky, k4 = ks * ks;
+        double o[3];
+        dcoef_dc(-p.nu * ks, p.dt, o);
+        for (int q = 0; q < 3; q++) d[q * t + (size_t)j * nr + m] = -ks * o[q];
+        dcoef_dc(-1.5 * p.lambda * p.sigma * p.epsilon * k4, p.dt, o);
+        for (int q = 0; q < 3; q++) {
+          d[(3 + q) * t + (size_t)j * nr + m] = -1.5 * p.sigma * p.epsilon * k4 * o[q];
+          d[(6 + q) * t + (size_t)j * nr + m] = -1.5 * p.lambda * p.epsilon * k4 * o[q];
+        }
+      }
+  }
+  // loss at the final state and its gradient (free_energy.c:3-157: c and grad c untruncated)
+  void loss(const double* lw) {
+    const chns_params& p = c->p;
+    k_adj_loss_prep3<R><<<blocks_s, 256, 0, st>>>(P, (const cx<R>*)c->state[1], SS(0, SB), ncx);
+    ifft(st, 0, SS(0, SB), FS(0, PCT), 3);
+    const double inv = 1.0 / ((double)c->n * (double)c->n);
+    const double kb = lw[0] * 12.0 * (p.sigma / p.epsilon) * inv;
+    const double kg = (lw[1] * 0.75 * p.sigma * p.epsilon + 4.0 * lw[2]) * inv;
+    const double dkb = lw[0] * 12.0 / p.epsilon * inv;
+    const double dkg = lw[1] * 0.75 * p.epsilon * inv;
+    k_adj_loss<R><<<kLossBlocks, 256, 0, st>>>(FS(0, PCT), FS(0, PCX), FS(0, PCY), F(PUB), F(PVB), F(PWXB), nn, kb,
+                                               kg, dkb, dkg, a->acc + kAcc);
+    k_sum_parts<<<1, 32, 0, st>>>(a->acc + kAcc, kLossBlocks, a->acc);
+    dfft(st, 0, F(PUB), SS(0, SB), 3);
+    k_adj_loss_acc3<R><<<blocks_s, 256, 0, st>>>(P, SS(0, SB), S(SGC), S(SGW), ncx);
+  }
+  // h: the accumulators; g_par = dJ/d(nu, lambda, sigma)
+  void params(const double* h, double* g_par) const {
+    g_par[0] = h[4];
+    g_par[1] = h[5];
+    g_par[2] = h[6] + h[2];  // sigma: through the step and through the loss
+  }
 
   cx<R>* S(int k) const { return (cx<R>*)a->spec + (size_t)k * ncx; }
   R* F(int k) const { return (R*)a->phys + (size_t)k * nn; }
@@ -201,40 +260,232 @@ template <class R> struct Adj {
   }
 };
 
-// one forward step that also records u_n, u*, N(u_n) and N(u*) into a segment slot
-int record_step(chns_ctx* c, char* slot, size_t fbytes) {
+// ---------------------------------------------------------------------------
+// ternary model: state (w, c1, c2)
+// ---------------------------------------------------------------------------
+namespace tern {
+constexpr int SSET = 14;                       // spectral fields per set
+enum { SB = 0, SX = 10, SFF = 12 };             // batch of 10, mu_hat batch of 2, F[muF] batch of 2
+enum {
+  SYB = 2 * SSET,                              // F[muF]_bar spectra (2)
+  SNB = SYB + 2,                               // N*_bar (3)
+  SNA = SNB + 3,                               // N(u_n)_bar (3)
+  SG = SNA + 3,                                // running gradient (3)
+  CUR = SG + 3,                                // current step: u_n, u*, N(u_n), N(u*) (3 each)
+  NSPEC = CUR + 12
+};
+constexpr int PSET = 14;                       // physical fields per set
+enum { PF = 0, PMF = 10, PMU = 12 };            // ten forward fields, muF (2), mu (2)
+enum { PTAIL = 2 * PSET, PMUB = PTAIL + 5, PMFB = PMUB + 2, PXB = PMFB + 2, NPHYS = PXB + 10 };
+}  // namespace tern
+
+template <class R> struct AdjT3 {
+  static constexpr int NF = 3, NSPEC_ = tern::NSPEC, NPHYS_ = tern::NPHYS, NBSCR = T_N, NDCOEF = 6;
+  chns_ctx* c;
+  chns_adj* a;
+  AdjParT<R> P;
+  cudaStream_t st;
+  size_t ncx, nn;
+  int blocks_s, blocks_p;
+
+  cx<R>* S(int k) const { return (cx<R>*)a->spec + (size_t)k * ncx; }
+  R* F(int k) const { return (R*)a->phys + (size_t)k * nn; }
+  cx<R>* SS(int set, int k) const { return S(set * tern::SSET + k); }
+  R* FS(int set, int k) const { return F(set * tern::PSET + k); }
+  void* scratch(int set) const { return (char*)a->bscr + (size_t)set * T_N * ncx * sizeof(cx<R>); }
+  int cur0() const { return tern::CUR; }
+  cx<R>* grad(int f) const { return S(tern::SG + f); }
+  cx<R>* cu(int f) const { return S(tern::CUR + f); }      // u_n
+  cx<R>* cs(int f) const { return S(tern::CUR + 3 + f); }  // u*
+  cx<R>* cn(int f) const { return S(tern::CUR + 6 + f); }  // N(u_n)
+  cx<R>* cx_(int f) const { return S(tern::CUR + 9 + f); } // N(u*)
+
+  void ifft(cudaStream_t s, int set, const cx<R>* in, R* x, int nb) {
+    c->stream = s;
+    c->L->ifftb(c, in, ncx, x, nn, nb, scratch(set));
+    c->stream = st;
+  }
+  void dfft(cudaStream_t s, int set, const R* x, cx<R>* out, int nb) {
+    c->stream = s;
+    c->L->dfftb(c, x, nn, out, ncx, nb, scratch(set));
+    c->stream = st;
+  }
+
+  void setup() {
+    const chns_params& p = c->p;
+    P.n = c->n;
+    P.jt = c->jt;
+    P.fx = c->fx;
+    P.fy = c->fy;
+    P.mrow = c->mrow;
+    P.s1 = P.s2 = P.lam = (R)0;
+    P.ds1 = P.ds2 = 0.0;
+    const double g1 = c->gamma[0], g2 = c->gamma[1], g3 = c->gamma[2];
+    P.g1 = (R)g1;
+    P.g2 = (R)g2;
+    P.g3 = (R)g3;
+    P.kk = (R)(2.0 * c->del / p.epsilon);
+    P.xl6 = (R)(6.0 * p.xlambda);
+    P.mu1c = (R)(0.75 * g1 * p.epsilon);
+    P.mu2c = (R)(0.75 * g2 * p.epsilon);
+    P.lg1 = (R)(p.lambda / g1);
+    P.lg2 = (R)(p.lambda / g2);
+    P.w11 = (R)(1.0 + g3 / g1);
+    P.w12 = (R)(g3 / g2);
+    P.w21 = (R)(g3 / g1);
+    P.w22 = (R)(1.0 + g3 / g2);
+  }
+  // d/dnu of the w coefficients, d/dlambda of the c coefficients (-0.75 lambda eps k^4)
+  static void dcoef_tables(const chns_ctx* c, std::vector<double>& d) {
+    const int nr = c->nr;
+    const chns_params& p = c->p;
+    const size_t t = (size_t)nr * nr;
+    d.assign(NDCOEF * t, 0.0);
+    for (int j = 0; j < nr; j++)
+      for (int m = 0; m < nr; m++) {
+        const double kx = c->fx * m, ky = c->fy * j, ks = kx * kx + ky * ky, k4 = ks * ks;
+        double o[3];
+        dcoef_dc(-p.nu * ks, p.dt, o);
+        for (int q = 0; q < 3; q++) d[q * t + (size_t)j * nr + m] = -ks * o[q];
+        dcoef_dc(-0.75 * p.lambda * p.epsilon * k4, p.dt, o);
+        for (int q = 0; q < 3; q++) d[(3 + q) * t + (size_t)j * nr + m] = -0.75 * p.epsilon * k4 * o[q];
+      }
+  }
+
+  // forward fields of the right-hand side at (w, c1, c2) into field set `set`
+  void fields(cudaStream_t s, int set, const cx<R>* w, const cx<R>* c1, const cx<R>* c2) {
+    k_adj3_fwd_prep<R><<<blocks_s, 256, 0, s>>>(P, w, c1, c2, SS(set, tern::SB), ncx);
+    ifft(s, set, SS(set, tern::SB), FS(set, tern::PF), T_N);
+    k_adj3_bulk<R><<<blocks_p, 256, 0, s>>>(P, FS(set, tern::PF + T_C1), FS(set, tern::PF + T_C2),
+                                            FS(set, tern::PMF), nn);
+    dfft(s, set, FS(set, tern::PMF), SS(set, tern::SFF), 2);
+    k_adj3_mu_prep<R><<<blocks_s, 256, 0, s>>>(P, c1, c2, SS(set, tern::SFF), SS(set, tern::SX), ncx);
+    ifft(s, set, SS(set, tern::SX), FS(set, tern::PMU), 2);
+  }
+
+  // (gw, g1, g2) += J_N(state)^T (nw, n1, n2) with the forward fields of `set`;
+  // parameter sums into acc[8 + 2 ..]
+  void transpose_rhs(int set, const cx<R>* c1, const cx<R>* c2, const cx<R>* nw, const cx<R>* n1, const cx<R>* n2) {
+    double* pacc = a->acc + 8;
+    k_adj3_tail<R><<<blocks_s, 256, 0, st>>>(P, nw, n1, n2, SS(0, tern::SB), ncx);
+    ifft(st, 0, SS(0, tern::SB), F(tern::PTAIL), 5);
+    const int b = tern::PF;
+    PhysT<R> pf{FS(set, b + T_U),   FS(set, b + T_V),   FS(set, b + T_WX),  FS(set, b + T_WY),  FS(set, b + T_C1X),
+                FS(set, b + T_C1Y), FS(set, b + T_C2X), FS(set, b + T_C2Y), FS(set, tern::PMU), FS(set, tern::PMU + 1)};
+    AdjT5<R> at{F(tern::PTAIL), F(tern::PTAIL + 1), F(tern::PTAIL + 2), F(tern::PTAIL + 3), F(tern::PTAIL + 4)};
+    k_adj3_products<R><<<blocks_p, 256, 0, st>>>(P, pf, at, F(tern::PXB), F(tern::PMUB), nn, pacc + 2);
+    dfft(st, 0, F(tern::PMUB), SS(0, tern::SX), 2);
+    k_adj3_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(0, tern::SX), c1, c2, SS(set, tern::SFF), n1, n2, grad(1), grad(2),
+                                           S(tern::SYB), ncx, pacc + 6);
+    ifft(st, 0, S(tern::SYB), F(tern::PMFB), 2);
+    k_adj3_bulk_bar<R><<<blocks_p, 256, 0, st>>>(P, FS(set, b + T_C1), FS(set, b + T_C2), F(tern::PMFB),
+                                                 F(tern::PXB), nn, pacc + 10);
+    dfft(st, 0, F(tern::PXB), SS(0, tern::SB), T_N);
+    k_adj3_acc<R><<<blocks_s, 256, 0, st>>>(P, SS(0, tern::SB), grad(0), grad(1), grad(2), ncx);
+  }
+
+  void reverse_step(const R* coef, const double* dcoef, cudaStream_t fork) {
+    double* pacc = a->acc + 8;
+    if (fork) {
+      cudaEventRecord(a->ev_fork, st);
+      cudaStreamWaitEvent(fork, a->ev_fork, 0);
+      fields(fork, 1, cu(0), cu(1), cu(2));
+      cudaEventRecord(a->ev_join, fork);
+    }
+    CFields3<R> g{{grad(0), grad(1), grad(2)}};
+    CFields3<R> nst{{cx_(0), cx_(1), cx_(2)}}, nnn{{cn(0), cn(1), cn(2)}}, un{{cu(0), cu(1), cu(2)}};
+    Fields3<R> nbs{{S(tern::SNB), S(tern::SNB + 1), S(tern::SNB + 2)}};
+    Fields3<R> nba{{S(tern::SNA), S(tern::SNA + 1), S(tern::SNA + 2)}};
+    Fields3<R> gm{{grad(0), grad(1), grad(2)}};
+    k_adj3_etd2<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, g, nst, nnn, nbs, nba, pacc);
+    fields(st, 0, cs(0), cs(1), cs(2));
+    transpose_rhs(0, cs(1), cs(2), S(tern::SNB), S(tern::SNB + 1), S(tern::SNB + 2));
+    k_adj3_etd1<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gm, un, nnn, nba, pacc);
+    if (fork) {
+      cudaStreamWaitEvent(st, a->ev_join, 0);
+    } else {
+      fields(st, 1, cu(0), cu(1), cu(2));
+    }
+    transpose_rhs(1, cu(1), cu(2), S(tern::SNA), S(tern::SNA + 1), S(tern::SNA + 2));
+  }
+
+  // loss (free_energy.c ternary, untruncated c_i and gradients) and its gradient
+  void loss(const double* lw) {
+    const chns_params& p = c->p;
+    k_adj3_loss_prep<R><<<blocks_s, 256, 0, st>>>(P, (const cx<R>*)c->state[1], (const cx<R>*)c->state[2],
+                                                  SS(0, tern::SB), ncx);
+    ifft(st, 0, SS(0, tern::SB), FS(0, tern::PF), 6);
+    const double inv = 1.0 / ((double)c->n * (double)c->n);
+    const double kb = lw[0] * (6.0 / p.epsilon) * inv, kg = lw[1] * 0.375 * p.epsilon * inv, kp = lw[2] * inv;
+    k_adj3_loss<R><<<kLossBlocks, 256, 0, st>>>(P, FS(0, tern::PF), F(tern::PXB), nn, kb, kg, kp, a->acc + kAcc);
+    k_sum_partsn<4><<<1, 32, 0, st>>>(a->acc + kAcc, kLossBlocks, a->acc);
+    dfft(st, 0, F(tern::PXB), SS(0, tern::SB), 6);
+    k_adj3_loss_acc<R><<<blocks_s, 256, 0, st>>>(P, SS(0, tern::SB), grad(1), grad(2), grad(0), ncx);
+  }
+
+  // g_par = dJ/d(nu, lambda, sigma_12, sigma_13, sigma_23), chained through
+  // gamma_1 = s12 + s13 - s23, gamma_2 = s12 + s23 - s13, gamma_3 = s13 + s23 - s12
+  // (main.c:166-170) and Delta = 6 g1 g2 g3 / (g1 g2 + g1 g3 + g2 g3)
+  void params(const double* h, double* g_par) const {
+    const chns_params& p = c->p;
+    const double* q = h + 8;
+    const double g1 = c->gamma[0], g2 = c->gamma[1], g3 = c->gamma[2], eps = p.epsilon, lam = p.lambda;
+    double dg[3] = {h[1] + q[11], h[2] + q[12], h[3] + q[13]};
+    dg[0] += q[14] * (-1.0 / (g1 * g1));
+    dg[1] += q[15] * (-1.0 / (g2 * g2));
+    dg[2] += q[16] * (-1.0 / (g3 * g3));
+    // weights w11 = 1 + g3/g1, w12 = g3/g2, w21 = g3/g1, w22 = 1 + g3/g2
+    dg[0] += (q[2] + q[4]) * (-g3 / (g1 * g1));
+    dg[1] += (q[3] + q[5]) * (-g3 / (g2 * g2));
+    dg[2] += (q[2] + q[4]) / g1 + (q[3] + q[5]) / g2;
+    // 0.75 g_i eps k^2 c_i in mu_i; lambda / g_i in N_ci
+    dg[0] += q[6] * 0.75 * eps + q[8] * (-lam / (g1 * g1));
+    dg[1] += q[7] * 0.75 * eps + q[9] * (-lam / (g2 * g2));
+    // K = 2 Delta / eps
+    const double S = g1 * g2 + g1 * g3 + g2 * g3, P3 = g1 * g2 * g3;
+    const double dD[3] = {6.0 * (g2 * g3 * S - P3 * (g2 + g3)) / (S * S), 6.0 * (g1 * g3 * S - P3 * (g1 + g3)) / (S * S),
+                          6.0 * (g1 * g2 * S - P3 * (g1 + g2)) / (S * S)};
+    for (int k = 0; k < 3; k++) dg[k] += q[10] * (2.0 / eps) * dD[k];
+    g_par[0] = q[0];
+    g_par[1] = q[1] + q[8] / g1 + q[9] / g2;
+    g_par[2] = dg[0] + dg[1] - dg[2];
+    g_par[3] = dg[0] - dg[1] + dg[2];
+    g_par[4] = -dg[0] + dg[1] + dg[2];
+  }
+};
+
+// one forward step that also records u_n, u*, N(u_n) and N(u*) (nf fields each)
+// into a segment slot
+int record_step(chns_ctx* c, char* slot, size_t fbytes, int nf) {
   cudaStream_t st = c->stream;
-  ACK(cudaMemcpyAsync(slot, c->state[0], fbytes, cudaMemcpyDeviceToDevice, st));
-  ACK(cudaMemcpyAsync(slot + fbytes, c->state[1], fbytes, cudaMemcpyDeviceToDevice, st));
+  for (int f = 0; f < nf; f++) ACK(cudaMemcpyAsync(slot + f * fbytes, c->state[f], fbytes, cudaMemcpyDeviceToDevice, st));
   c->L->stage(c, 1);
-  ACK(cudaMemcpyAsync(slot + 2 * fbytes, c->state[0], fbytes, cudaMemcpyDeviceToDevice, st));
-  ACK(cudaMemcpyAsync(slot + 3 * fbytes, c->state[1], fbytes, cudaMemcpyDeviceToDevice, st));
-  ACK(cudaMemcpyAsync(slot + 4 * fbytes, c->saved[0], fbytes, cudaMemcpyDeviceToDevice, st));
-  ACK(cudaMemcpyAsync(slot + 5 * fbytes, c->saved[1], fbytes, cudaMemcpyDeviceToDevice, st));
-  c->nstar[0] = slot + 6 * fbytes;
-  c->nstar[1] = slot + 7 * fbytes;
+  for (int f = 0; f < nf; f++) {
+    ACK(cudaMemcpyAsync(slot + (nf + f) * fbytes, c->state[f], fbytes, cudaMemcpyDeviceToDevice, st));
+    ACK(cudaMemcpyAsync(slot + (2 * nf + f) * fbytes, c->saved[f], fbytes, cudaMemcpyDeviceToDevice, st));
+    c->nstar[f] = slot + (3 * nf + f) * fbytes;
+  }
   c->L->stage(c, 2);
-  c->nstar[0] = nullptr;
-  c->nstar[1] = nullptr;
+  for (int f = 0; f < 3; f++) c->nstar[f] = nullptr;
   return CHNS_OK;
 }
 
 int snapshot_save(chns_ctx* c, void* dst, double* dstk0) {
   const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
-  ACK(cudaMemcpyAsync(dst, c->state[0], bytes, cudaMemcpyDeviceToDevice, c->stream));
-  ACK(cudaMemcpyAsync((char*)dst + bytes, c->state[1], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  for (int f = 0; f <= c->p.model; f++)
+    ACK(cudaMemcpyAsync((char*)dst + f * bytes, c->state[f], bytes, cudaMemcpyDeviceToDevice, c->stream));
   ACK(cudaMemcpyAsync(dstk0, c->k0, 16 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   return CHNS_OK;
 }
 int snapshot_load(chns_ctx* c, const void* src, const double* srck0) {
   const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
-  ACK(cudaMemcpyAsync(c->state[0], src, bytes, cudaMemcpyDeviceToDevice, c->stream));
-  ACK(cudaMemcpyAsync(c->state[1], (const char*)src + bytes, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  for (int f = 0; f <= c->p.model; f++)
+    ACK(cudaMemcpyAsync(c->state[f], (const char*)src + f * bytes, bytes, cudaMemcpyDeviceToDevice, c->stream));
   ACK(cudaMemcpyAsync(c->k0, srck0, 16 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   return CHNS_OK;
 }
 
-int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
+template <class A> int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
   if (!c->adj) {
     c->adj = (chns_adj*)calloc(1, sizeof(chns_adj));
     if (!c->adj) return CHNS_ERR_NOMEM;
@@ -242,32 +493,16 @@ int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
   chns_adj* a = c->adj;
   const size_t ncx = (size_t)c->n * c->nr, nn = (size_t)c->n * c->n;
   const size_t fbytes = ncx * 2 * c->rsz;  // one S-layout field
-  const size_t snap = 2 * fbytes;
+  const size_t snap = (size_t)A::NF * fbytes;
   a->ncx = ncx;
   a->nn = nn;
   if (!a->dcoef) {
-    if (cudaMalloc(&a->spec, NSPEC * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
-    if (cudaMalloc(&a->phys, NPHYS * nn * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
-    if (cudaMalloc(&a->bscr, 2 * FOP_N * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
-    // 8 accumulators, then 3 per-block partials of each loss block
-    if (cudaMalloc((void**)&a->acc, (8 + 3 * kLossBlocks) * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
-    // derivative tables of the ETD coefficients: d/dnu (w), d/dlambda, d/dsigma (c)
-    const int nr = c->nr;
-    const chns_params& p = c->p;
-    std::vector<double> d(9 * (size_t)nr * nr);
-    const size_t t = (size_t)nr * nr;
-    for (int j = 0; j < nr; j++)
-      for (int m = 0; m < nr; m++) {
-        const double kx = c->fx * m, ky = c->fy * j, ks = kx * kx + ky * ky, k4 = ks * ks;
-        double o[3];
-        dcoef_dc(-p.nu * ks, p.dt, o);
-        for (int q = 0; q < 3; q++) d[q * t + (size_t)j * nr + m] = -ks * o[q];
-        dcoef_dc(-1.5 * p.lambda * p.sigma * p.epsilon * k4, p.dt, o);
-        for (int q = 0; q < 3; q++) {
-          d[(3 + q) * t + (size_t)j * nr + m] = -1.5 * p.sigma * p.epsilon * k4 * o[q];
-          d[(6 + q) * t + (size_t)j * nr + m] = -1.5 * p.lambda * p.epsilon * k4 * o[q];
-        }
-      }
+    if (cudaMalloc(&a->spec, A::NSPEC_ * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->phys, A::NPHYS_ * nn * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->bscr, 2 * (size_t)A::NBSCR * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc((void**)&a->acc, (kAcc + 4 * kLossBlocks) * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
+    std::vector<double> d;
+    A::dcoef_tables(c, d);
     if (cudaMalloc(&a->dcoef, d.size() * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMemcpy(a->dcoef, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
       return CHNS_ERR_CUDA;
@@ -289,11 +524,11 @@ int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
     a->seg = nullptr;
     a->cap_states = 0;
     a->seg_len = 0;
-    if (cudaMalloc(&a->seg, SLOT_FIELDS * fbytes * 2 * (size_t)seglen) == cudaSuccess) {
+    if (cudaMalloc(&a->seg, 4 * A::NF * fbytes * 2 * (size_t)seglen) == cudaSuccess) {
       a->cap_states = 2 * seglen;
     } else {
       cudaGetLastError();
-      if (cudaMalloc(&a->seg, SLOT_FIELDS * fbytes * (size_t)seglen) != cudaSuccess) return CHNS_ERR_NOMEM;
+      if (cudaMalloc(&a->seg, 4 * A::NF * fbytes * (size_t)seglen) != cudaSuccess) return CHNS_ERR_NOMEM;
       a->cap_states = seglen;
     }
     a->seg_len = seglen;
@@ -320,71 +555,47 @@ int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
   return CHNS_OK;
 }
 
-template <class R>
+template <class R, class A>
 int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J, double* g_w, double* g_c,
                  double* g_par, int where) {
   const int nseg = (nsteps + ckpt - 1) / ckpt;
-  int rc = adj_alloc(c, ckpt, nseg + 1);
+  int rc = adj_alloc<A>(c, ckpt, nseg + 1);
   if (rc) return rc;
   chns_adj* a = c->adj;
-  Adj<R> A;
-  A.c = c;
-  A.a = a;
-  A.st = c->stream;
-  A.ncx = a->ncx;
-  A.nn = a->nn;
-  A.blocks_s = (int)((A.ncx + 255) / 256);
-  A.blocks_p = 1024;
-  const chns_params& p = c->p;
-  A.P.n = c->n;
-  A.P.jt = c->jt;
-  A.P.fx = c->fx;
-  A.P.fy = c->fy;
-  A.P.s1 = (R)(1.5 * p.sigma * p.epsilon);
-  A.P.s2 = (R)(24.0 * (p.sigma / p.epsilon));
-  A.P.lam = (R)p.lambda;
-  A.P.ds1 = 1.5 * p.epsilon;
-  A.P.ds2 = 24.0 / p.epsilon;
-  A.P.mrow = c->mrow;
+  A ad;
+  ad.c = c;
+  ad.a = a;
+  ad.st = c->stream;
+  ad.ncx = a->ncx;
+  ad.nn = a->nn;
+  ad.blocks_s = (int)((ad.ncx + 255) / 256);
+  ad.blocks_p = 1024;
+  ad.setup();
   cudaStream_t st = c->stream;
-  const size_t bytes = A.ncx * sizeof(cx<R>);
+  const size_t bytes = ad.ncx * sizeof(cx<R>);
   const R* coef = (const R*)c->coef;
   const double* dcoef = (const double*)a->dcoef;
-  ACK(cudaMemsetAsync(a->acc, 0, 8 * sizeof(double), st));
+  ACK(cudaMemsetAsync(a->acc, 0, kAcc * sizeof(double), st));
 
   // forward sweep with checkpoints (checkpoint nseg keeps u_0 for restoring);
   // the last segment is recorded on the way
   char* segbase = (char*)a->seg;
-  const size_t slot = SLOT_FIELDS * bytes;
+  const size_t slot = 4 * (size_t)A::NF * bytes;
   const int nlast = (nseg - 1) * ckpt;
   const size_t lastbuf = a->cap_states >= 2 * ckpt ? (size_t)((nseg - 1) % 2) * ckpt : 0;
   if ((rc = snapshot_save(c, a->ckpt[nseg], a->ckptk0[nseg]))) return rc;
   for (int n = 0; n < nsteps; n++) {
     if (n % ckpt == 0 && (rc = snapshot_save(c, a->ckpt[n / ckpt], a->ckptk0[n / ckpt]))) return rc;
-    rc = n >= nlast ? record_step(c, segbase + (lastbuf + n - nlast) * slot, bytes) : chns_step(c, 1);
+    rc = n >= nlast ? record_step(c, segbase + (lastbuf + n - nlast) * slot, bytes, A::NF) : chns_step(c, 1);
     if (rc) return rc;
   }
-  // loss at the final state and its gradient (free_energy.c:3-157: c and grad c untruncated)
-  {
-    k_adj_loss_prep3<R><<<A.blocks_s, 256, 0, st>>>(A.P, (const cx<R>*)c->state[1], A.SS(0, SB), A.ncx);
-    A.ifft(st, 0, A.SS(0, SB), A.FS(0, PCT), 3);
-    const double inv = 1.0 / ((double)c->n * (double)c->n);
-    const double kb = lw[0] * 12.0 * (p.sigma / p.epsilon) * inv;
-    const double kg = (lw[1] * 0.75 * p.sigma * p.epsilon + 4.0 * lw[2]) * inv;
-    const double dkb = lw[0] * 12.0 / p.epsilon * inv;
-    const double dkg = lw[1] * 0.75 * p.epsilon * inv;
-    k_adj_loss<R><<<kLossBlocks, 256, 0, st>>>(A.FS(0, PCT), A.FS(0, PCX), A.FS(0, PCY), A.F(PUB), A.F(PVB),
-                                               A.F(PWXB), A.nn, kb, kg, dkb, dkg, a->acc + 8);
-    k_sum_parts<<<1, 32, 0, st>>>(a->acc + 8, kLossBlocks, a->acc);
-    A.dfft(st, 0, A.F(PUB), A.SS(0, SB), 3);
-    k_adj_loss_acc3<R><<<A.blocks_s, 256, 0, st>>>(A.P, A.SS(0, SB), A.S(SGC), A.S(SGW), A.ncx);
-  }
+  ad.loss(lw);
   // the reversed step as a CUDA graph on its fixed buffers (eager if capture fails)
   if (!a->rev && !a->rev_tried) {
     a->rev_tried = true;
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      A.reverse_step(coef, dcoef, a->fork);
+      ad.reverse_step(coef, dcoef, a->fork);
       if (cudaStreamEndCapture(st, &g) == cudaSuccess && g) {
         if (cudaGraphInstantiate(&a->rev, g, 0) != cudaSuccess) a->rev = nullptr;
         cudaGraphDestroy(g);
@@ -405,7 +616,8 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
     if (s + nbuf <= nseg - 1) ACK(cudaStreamWaitEvent(side, a->ev_free[b], 0));
     c->stream = side;
     int r = snapshot_load(c, a->ckpt[s], a->ckptk0[s]);
-    for (int k = 0; k < len && !r; k++) r = record_step(c, segbase + ((size_t)b * ckpt + k) * slot, bytes);
+    for (int k = 0; k < len && !r; k++)
+      r = record_step(c, segbase + ((size_t)b * ckpt + k) * slot, bytes, A::NF);
     c->stream = st;
     if (r) return r;
     ACK(cudaEventRecord(a->ev_ready[b], side));
@@ -415,11 +627,12 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
     const int b = s % nbuf, len = (s * ckpt + ckpt <= nsteps) ? ckpt : nsteps - s * ckpt;
     if (s != nseg - 1) ACK(cudaStreamWaitEvent(st, a->ev_ready[b], 0));
     for (int k = len - 1; k >= 0; k--) {
-      ACK(cudaMemcpyAsync(A.S(CUW), segbase + ((size_t)b * ckpt + k) * slot, slot, cudaMemcpyDeviceToDevice, st));
+      ACK(cudaMemcpyAsync(ad.S(ad.cur0()), segbase + ((size_t)b * ckpt + k) * slot, slot, cudaMemcpyDeviceToDevice,
+                          st));
       if (a->rev) {
         ACK(cudaGraphLaunch(a->rev, st));
       } else {
-        A.reverse_step(coef, dcoef, nullptr);
+        ad.reverse_step(coef, dcoef, nullptr);
       }
     }
     ACK(cudaEventRecord(a->ev_free[b], st));
@@ -437,24 +650,22 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
   ACK(cudaGetLastError());
   // restore u_0 and return the results
   if ((rc = snapshot_load(c, a->ckpt[nseg], a->ckptk0[nseg]))) return rc;
-  double h[8];
+  double h[kAcc];
   ACK(cudaMemcpyAsync(h, a->acc, sizeof(h), cudaMemcpyDeviceToHost, st));
   ACK(cudaStreamSynchronize(st));
   if (J) *J = h[0];
-  if (g_par) {
-    g_par[0] = h[4];
-    g_par[1] = h[5];
-    g_par[2] = h[6] + h[2];  // sigma: through the step and through the loss
-  }
+  if (g_par) ad.params(h, g_par);
   const size_t fb = 2 * (size_t)c->n * c->nr * sizeof(double);
   const cudaMemcpyKind kind = where == CHNS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   if (g_w) {
-    c->L->to_fftw(c, A.S(SGW), c->stage);
+    c->L->to_fftw(c, ad.grad(0), c->stage);
     ACK(cudaMemcpyAsync(g_w, c->stage, fb, kind, st));
   }
-  if (g_c) {
-    c->L->to_fftw(c, A.S(SGC), c->stage);
-    ACK(cudaMemcpyAsync(g_c, c->stage, fb, kind, st));
+  // g_c: dJ/dc_hat (binary) or dJ/dc1_hat followed by dJ/dc2_hat (ternary)
+  for (int f = 1; g_c && f < A::NF; f++) {
+    c->L->to_fftw(c, ad.grad(f), c->stage);
+    ACK(cudaMemcpyAsync((char*)g_c + (f - 1) * fb, c->stage, fb, kind, st));
+    ACK(cudaStreamSynchronize(st));  // the staging buffer is reused
   }
   ACK(cudaStreamSynchronize(st));
   return CHNS_OK;
@@ -497,9 +708,12 @@ void chns_adj_free(chns_ctx* c) {
 extern "C" int chns_adjoint(chns_ctx* c, int nsteps, int ckpt, const double* loss_w, double* J, double* g_w,
                             double* g_c, double* g_par, int where) {
   if (!c || nsteps < 1 || ckpt < 1) return CHNS_ERR_ARG;
-  if (c->p.model != CHNS_MODEL_BINARY) return CHNS_ERR_UNSUPPORTED;
+  if (c->p.model == CHNS_MODEL_NS) return CHNS_ERR_UNSUPPORTED;
   const double dflt[3] = {1.0, 1.0, 1.0};
   const double* lw = loss_w ? loss_w : dflt;
-  return c->f32 ? adjoint_impl<float>(c, nsteps, ckpt, lw, J, g_w, g_c, g_par, where)
-                : adjoint_impl<double>(c, nsteps, ckpt, lw, J, g_w, g_c, g_par, where);
+  if (c->p.model == CHNS_MODEL_BINARY)
+    return c->f32 ? adjoint_impl<float, Adj<float>>(c, nsteps, ckpt, lw, J, g_w, g_c, g_par, where)
+                  : adjoint_impl<double, Adj<double>>(c, nsteps, ckpt, lw, J, g_w, g_c, g_par, where);
+  return c->f32 ? adjoint_impl<float, AdjT3<float>>(c, nsteps, ckpt, lw, J, g_w, g_c, g_par, where)
+                : adjoint_impl<double, AdjT3<double>>(c, nsteps, ckpt, lw, J, g_w, g_c, g_par, where);
 }
