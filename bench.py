@@ -300,6 +300,33 @@ def adjoint_leg(C, stream, big_steps: int):
             else:
                 leg["rel_diff_vs_fp64_dJ_dc"] = float(np.linalg.norm(gc - g64[0]) / np.linalg.norm(g64[0]))
             out[name] = leg
+    # ternary: the spinodal setting at 512^2 (dt = 5e-5), same schedule
+    from chns_b200 import configs as _cf
+
+    pt, ph = _cf.ternary_spinodal(n, C.FP64)
+    for prec, name in ((C.FP64, "ternary_fp64"), (C.FP32, "ternary_fp32")):
+        with C.Context(dict(pt, precision=prec)) as c:
+            c.L.chns_set_stream(c.handle, ctypes_stream(stream))
+            c.set_phase_real(*ph)
+            st0 = c.get_state()
+            c.adjoint(steps, ckpt)
+            c.set_state(*st0)
+            c.synchronize()
+            ev0.record(stream)
+            c.step(steps)
+            ev1.record(stream)
+            ev1.synchronize()
+            t_fwd = ev0.elapsed_time(ev1)
+            c.set_state(*st0)
+            c.synchronize()
+            ev0.record(stream)
+            J, _, _, gp = c.adjoint(steps, ckpt)
+            ev1.record(stream)
+            ev1.synchronize()
+            t_adj = ev0.elapsed_time(ev1)
+            out[name] = {"forward_ms": round(t_fwd, 3), "adjoint_ms": round(t_adj, 3),
+                         "ratio": round(t_adj / t_fwd, 3), "J": J,
+                         "dJ_dparams": dict(zip(("nu", "M", "sigma12", "sigma13", "sigma23"), map(float, gp)))}
     if big_steps > 0:
         nb = 4096
         with C.Context(adjoint_params(nb, C.FP32, 1.5e-7)) as c:
