@@ -67,6 +67,8 @@ CONFIGS = {
     # no working forcing, so this is the unforced step; same cost per step)
     "bin4096": dict(model=1, n=4096, lx="(2.0*pi)", dt="(2e-6)", nu="(1e-3)", lam="(1e-3)",
                     sigma="(0.1)", eps="(2.0*dx)"),
+    # ternary at 1024^2 for a few-step parity check of the large-grid kernels
+    "ter1024": dict(_TER, n=1024, dt="(5e-6)"),
     # Taylor-Green initial vorticity (TG_INIT, init.c:38-65): pure NS at L = 2 pi, and
     # binary with the reference defaults (L = 4 pi, eps = 3 dx), whose init also lays the drop
     "nstg32": dict(model=0, n=32, lx="(2.0*pi)", dt="(1e-3)", nu="(0.01)", init="tg"),

@@ -11,7 +11,7 @@ Small grids store full spectral states; the two full-size configurations
 (binary 256^2 x 1000 steps, ternary 512^2 x 2000 steps) store a fingerprint of
 the final state (see fingerprint()).
 
-Usage:  python tests/golden/make_golden.py [--full] [--init]  (--init: only init_ref.npz)
+Usage:  python tests/golden/make_golden.py [--full] [--big] [--init]  (--init: only init_ref.npz)
 """
 from __future__ import annotations
 
@@ -43,6 +43,13 @@ FULL = [
     ("bin256", 1000, 100, None, 0.0, 0.0),
     # ternary spinodal run: 512^2, omega = 0, c_i = 1/3 + U(+-0.02), 2000 steps at dt = 5e-5
     ("ter512", 2000, 101, None, 0.0, 0.0),
+]
+
+# large grids, a few steps from spinodal noise plus random low-k vorticity: parity of
+# the 1024^2 / 4096^2 kernels (the same fingerprint as FULL)
+BIG = [
+    ("bin4096", 2, 102, 103, 8.0, 0.1),
+    ("ter1024", 3, 104, 105, 8.0, 0.1),
 ]
 
 NPROJ = 8
@@ -129,8 +136,8 @@ def make_small(O):
         print("wrote", name)
 
 
-def make_full(O):
-    for name, steps, ps, ws, kmax, rms in FULL:
+def make_full(O, cases=None):
+    for name, steps, ps, ws, kmax, rms in cases or FULL:
         p = O.ref_config_params(name)
         R = O.RefLib(name, nthreads=min(8, os.cpu_count() or 1))
         n = p["nx"]
@@ -176,3 +183,5 @@ if __name__ == "__main__":
         make_init(O)
     if "--full" in sys.argv:
         make_full(O)
+    if "--big" in sys.argv:
+        make_full(O, BIG)

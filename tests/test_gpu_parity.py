@@ -156,3 +156,24 @@ def test_kolmogorov_forcing_matches_oracle(chns):
         c.step(10)
         for a, b in zip(c.get_state(), o.get_state()):
             assert rel_l2(a, b) <= 1e-11
+
+
+@pytest.mark.parametrize("case", MG.BIG, ids=[c[0] for c in MG.BIG])
+def test_large_grids_match_reference(chns, case):
+    """The 4096^2 binary and 1024^2 ternary kernels against the reference's own
+    steps (compiled here) from spinodal noise plus random low-k vorticity:
+    fingerprint within 1e-11 after 2-3 steps."""
+    name, steps, ps, ws, kmax, rms = case
+    g = load_full(name)
+    p = g["params"]
+    assert g["steps"] == steps
+    p1, p2, w = MG.initial_state(p["model"], p["nx"], p["lx"], ps, ws, kmax, rms)
+    with _ctx(chns, p) as c:
+        MG.apply_initial(c, p["model"], p1, p2, w)
+        c.step(steps)
+        st = c.get_state()
+    for k, a in enumerate(st):
+        fp = MG.fingerprint(a)
+        ref = {key: g[f"final{k}_{key}"] for key in ("low", "proj", "norm")}
+        err = MG.fingerprint_rel_err(ref, fp)
+        assert err <= 1e-11, (name, k, err)
