@@ -490,10 +490,12 @@ def run_gpu(args):
                "mean_c_rel_drift_fp32": float(mean_drift), "coefficients": "series/expm1 (FP64) in both"}
         del res
 
-    init = init_leg(C, n) if rank == 0 else None
-    diag = diagnostics_leg(C, n, st0, not args.no_cpu_baseline) if rank == 0 else None
-    adj = adjoint_leg(C, stream, args.adjoint_big_steps) if args.adjoint and rank == 0 else None
-    ens = ensemble_leg(C, args.ensemble_steps) if args.ensemble_steps > 0 and rank == 0 else None
+    # single-GPU legs (the other ranks of a replica run would only wait for them)
+    solo = world == 1
+    init = init_leg(C, n) if solo else None
+    diag = diagnostics_leg(C, n, st0, not args.no_cpu_baseline) if solo else None
+    adj = adjoint_leg(C, stream, args.adjoint_big_steps) if args.adjoint and solo else None
+    ens = ensemble_leg(C, args.ensemble_steps) if args.ensemble_steps > 0 and solo else None
 
     out = None
     if rank == 0:
