@@ -677,7 +677,8 @@ def e2e_host_loop(ctx, stream, steps: int):
     wall = time.perf_counter() - t0
     bytes_ = 2 * shape[0] * shape[1] * 16
     return {"value": round(steps / wall, 3), "unit": "steps/s", "h2d_bytes_per_step": bytes_,
-            "d2h_bytes_per_step": bytes_, "note": "chns_set_state(host) + chns_step(1) + chns_get_state(host)"}
+            "d2h_bytes_per_step": bytes_, "note": "chns_set_state(host) + chns_step(1) + chns_get_state(host), page-locked host "
+                    "arrays (the drop-in etd2rk() page-locks the reference's arrays with chns_pin_host)"}
 
 
 def cpu_baseline(n: int, steps: int, threads: int | None = None):

@@ -80,6 +80,10 @@ def load_library(path: str = LIB_PATH):
     L.chns_profile_step.restype = ip
     L.chns_adjoint.argtypes = [vp, ip, ip, vp, vp, vp, vp, vp, ip]
     L.chns_adjoint.restype = ip
+    L.chns_pin_host.argtypes = [vp, vp, ctypes.c_size_t]
+    L.chns_pin_host.restype = ip
+    L.chns_unpin_host.argtypes = [vp, vp]
+    L.chns_unpin_host.restype = ip
     L.chns_check.argtypes = [vp]
     L.chns_check.restype = ip
     L.chns_spectrum_shells.argtypes = [vp]
@@ -220,6 +224,14 @@ class Context:
         a = np.ascontiguousarray(p1, np.float64)
         b = np.ascontiguousarray(p2, np.float64) if p2 is not None else None
         _check(self.L.chns_set_phase_real(self._h, _ptr(a), _ptr(b), HOST), "chns_set_phase_real")
+
+    def pin_host(self, a: np.ndarray):
+        """Page-locks a numpy array passed to set_state / get_state on every step
+        (until unpin_host or close; the array must stay alive until then)."""
+        _check(self.L.chns_pin_host(self._h, ctypes.c_void_p(a.ctypes.data), a.nbytes), "chns_pin_host")
+
+    def unpin_host(self, a: np.ndarray):
+        _check(self.L.chns_unpin_host(self._h, ctypes.c_void_p(a.ctypes.data)), "chns_unpin_host")
 
     def check(self):
         """Raises ChnsError (status -3) if the state holds NaN or infinite values."""

@@ -166,6 +166,8 @@ void free_all(chns_ctx* c) {
   for (void* q : c->h)
     if (q) cudaFree(q);
   if (c->hostpin) cudaFreeHost(c->hostpin);
+  for (int k = 0; k < c->npinned; k++) cudaHostUnregister(c->pinned[k]);
+  c->npinned = 0;
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   free(c);
 }
@@ -427,6 +429,38 @@ int chns_set_stream(chns_ctx* c, void* stream) {
     c->graph_ok = false;
   }
   return CHNS_OK;
+}
+
+int chns_pin_host(chns_ctx* c, void* ptr, size_t bytes) {
+  if (!c || !ptr || !bytes) return CHNS_ERR_ARG;
+  for (int k = 0; k < c->npinned; k++)
+    if (c->pinned[k] == ptr) return CHNS_OK;
+  const cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
+  if (e == cudaErrorHostMemoryAlreadyRegistered) {
+    cudaGetLastError();
+    return CHNS_OK;  // page-locked by someone else: nothing to undo later
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return CHNS_ERR_CUDA;
+  }
+  if (c->npinned == (int)(sizeof(c->pinned) / sizeof(c->pinned[0]))) {
+    cudaHostUnregister(ptr);
+    return CHNS_ERR_UNSUPPORTED;
+  }
+  c->pinned[c->npinned++] = ptr;
+  return CHNS_OK;
+}
+
+int chns_unpin_host(chns_ctx* c, void* ptr) {
+  if (!c || !ptr) return CHNS_ERR_ARG;
+  for (int k = 0; k < c->npinned; k++)
+    if (c->pinned[k] == ptr) {
+      cudaHostUnregister(ptr);
+      c->pinned[k] = c->pinned[--c->npinned];
+      return CHNS_OK;
+    }
+  return CHNS_ERR_ARG;
 }
 
 int chns_synchronize(chns_ctx* c) {

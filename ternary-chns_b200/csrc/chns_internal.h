@@ -81,6 +81,8 @@ struct chns_ctx {
   bool graph_ok;
   void* hostpin;    // pinned staging for host transfers
   size_t hostpin_bytes;
+  void* pinned[8];  // host arrays registered by chns_pin_host
+  int npinned;
   // discrete-adjoint buffers (allocated by the first chns_adjoint call)
   chns_adj* adj;
   // tracing: when prof_ev is set, every launch of a stage records an event

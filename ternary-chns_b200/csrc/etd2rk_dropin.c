@@ -82,6 +82,14 @@ static void dropin_init(void)
     if (rc != CHNS_OK) dropin_fail("chns_create", rc);
 }
 
+/* the state arrays are uploaded and read back on every call: page-lock them once
+ * (fftw_alloc_real(2 alloc_local) doubles each, main.c:75-163) */
+static void dropin_pin(void *a)
+{
+    if (a && chns_pin_host(dropin_ctx, a, 2 * (size_t)alloc_local * sizeof(double)) != CHNS_OK)
+        fprintf(stderr, "etd2rk (libchns_b200): could not page-lock a state array; transfers stay pageable\n");
+}
+
 void etd2rk(fftw_complex *cwz
 #ifdef BINARY
 , fftw_complex *cphi
@@ -92,6 +100,7 @@ void etd2rk(fftw_complex *cwz
 {
     double *c1 = NULL, *c2 = NULL;
     int rc;
+    int first = !dropin_ctx;
     if (!dropin_ctx) dropin_init();
 #ifdef BINARY
     c1 = (double *)cphi;
@@ -99,6 +108,11 @@ void etd2rk(fftw_complex *cwz
     c1 = (double *)cphi1;
     c2 = (double *)cphi2;
 #endif
+    if (first) {
+        dropin_pin(cwz);
+        dropin_pin(c1);
+        dropin_pin(c2);
+    }
     rc = chns_set_state(dropin_ctx, (const double *)cwz, c1, c2, CHNS_HOST);
     if (rc == CHNS_OK) rc = chns_step(dropin_ctx, 1);
     if (rc == CHNS_OK) rc = chns_get_state(dropin_ctx, (double *)cwz, c1, c2, CHNS_HOST);

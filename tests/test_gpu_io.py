@@ -3,6 +3,7 @@ nx x ny, x the slow index.  The dumps hold the reference's ifft of the state
 (restated by the oracle; FP64 relative L2 <= 1e-13), with DUMP_REAL_MPI's
 truncation when asked; reading a phase file equals chns_set_phase_real on the
 same array, bit for bit; unreadable files give CHNS_ERR_IO."""
+import ctypes
 import os
 
 import numpy as np
@@ -117,3 +118,25 @@ def test_logs_write_the_reference_files(chns, tmp_path, name):
     for i in (0, 1):
         for stem in ("spectrum", "Xspectrum", "Yspectrum"):
             assert (tmp_path / "spectra" / f"{stem}.{i}").stat().st_size > 0
+
+
+def test_pinned_host_arrays(chns):
+    g = load_small("ter32")
+    p = g["params"]
+    with chns.Context(p) as c:
+        bufs = [a.copy() for a in g["init"]]
+        for b in bufs:
+            c.pin_host(b)
+        c.pin_host(bufs[0])  # again: accepted
+        c.set_state(*bufs)
+        c.step(g["steps"])
+        out = [np.empty_like(b) for b in bufs]
+        for o in out:
+            c.pin_host(o)
+        c.L.chns_get_state(c.handle, *[ctypes.c_void_p(o.ctypes.data) for o in out], 0)
+        for o, ref in zip(out, g["final"]):
+            assert rel_l2(o, ref) <= 1e-11
+        for b in bufs + out:
+            c.unpin_host(b)
+        with pytest.raises(chns.ChnsError):
+            c.unpin_host(bufs[0])
