@@ -3,7 +3,6 @@ ternary-chns_b200/csrc/etd2rk_dropin.c (same signature, GPU step), driven like
 the reference (oracle/ref_harness.c), against the reference's golden vectors."""
 import os
 
-import numpy as np
 import pytest
 
 import oracle as O

@@ -4,7 +4,6 @@ nx x ny, x the slow index.  The dumps hold the reference's ifft of the state
 truncation when asked; reading a phase file equals chns_set_phase_real on the
 same array, bit for bit; unreadable files give CHNS_ERR_IO."""
 import ctypes
-import os
 
 import numpy as np
 import pytest
