@@ -247,30 +247,40 @@ def adjoint_leg(C, stream, big_steps: int):
 
     n, steps, ckpt = 512, 200, 20
     c_real = configs.binary_adjoint(n)[1]
-    out = {"grid": n, "steps": steps, "ckpt": ckpt, "loss": "E_bulk + E_grad + <|grad phi|^2> at the final step"}
+    out = {"grid": n, "steps": steps, "ckpt": ckpt, "loss": "E_bulk + E_grad + <|grad phi|^2> at the final step",
+           "timing": "median of 3 CUDA-event timings each"}
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    for prec, name in ((C.FP64, "fp64"), (C.FP32, "fp32")):
-        with C.Context(adjoint_params(n, prec, 1e-4)) as c:
-            c.L.chns_set_stream(c.handle, ctypes_stream(stream))
-            c.set_phase_real(c_real)
-            st0 = c.get_state()
-            c.adjoint(steps, ckpt)  # buffers and the reverse-step graph
-            c.step(10)
+    def timed_pair(c, st0):
+        """Median of 3 CUDA-event timings of `steps` forward steps and of the adjoint
+        of the same steps from st0 (after one untimed adjoint: buffers, graph)."""
+        c.adjoint(steps, ckpt)
+        c.step(10)
+        tf, ta = [], []
+        for _ in range(3):
             c.set_state(*st0)
             c.synchronize()
             ev0.record(stream)
             c.step(steps)
             ev1.record(stream)
             ev1.synchronize()
-            t_fwd = ev0.elapsed_time(ev1)
+            tf.append(ev0.elapsed_time(ev1))
+        for _ in range(3):
             c.set_state(*st0)
             c.synchronize()
             ev0.record(stream)
-            J, gw, gc, gp = c.adjoint(steps, ckpt)
+            res = c.adjoint(steps, ckpt)
             ev1.record(stream)
             ev1.synchronize()
-            t_adj = ev0.elapsed_time(ev1)
+            ta.append(ev0.elapsed_time(ev1))
+        return statistics.median(tf), statistics.median(ta), res
+
+    for prec, name in ((C.FP64, "fp64"), (C.FP32, "fp32")):
+        with C.Context(adjoint_params(n, prec, 1e-4)) as c:
+            c.L.chns_set_stream(c.handle, ctypes_stream(stream))
+            c.set_phase_real(c_real)
+            st0 = c.get_state()
+            t_fwd, t_adj, (J, gw, gc, gp) = timed_pair(c, st0)
             leg = {"forward_ms": round(t_fwd, 3), "adjoint_ms": round(t_adj, 3), "ratio": round(t_adj / t_fwd, 3),
                    "J": J, "dJ_dnu": gp[0], "dJ_dM": gp[1], "dJ_dsigma": gp[2]}
             if prec == C.FP64:
@@ -309,21 +319,7 @@ def adjoint_leg(C, stream, big_steps: int):
             c.L.chns_set_stream(c.handle, ctypes_stream(stream))
             c.set_phase_real(*ph)
             st0 = c.get_state()
-            c.adjoint(steps, ckpt)
-            c.set_state(*st0)
-            c.synchronize()
-            ev0.record(stream)
-            c.step(steps)
-            ev1.record(stream)
-            ev1.synchronize()
-            t_fwd = ev0.elapsed_time(ev1)
-            c.set_state(*st0)
-            c.synchronize()
-            ev0.record(stream)
-            J, _, _, gp = c.adjoint(steps, ckpt)
-            ev1.record(stream)
-            ev1.synchronize()
-            t_adj = ev0.elapsed_time(ev1)
+            t_fwd, t_adj, (J, _, _, gp) = timed_pair(c, st0)
             out[name] = {"forward_ms": round(t_fwd, 3), "adjoint_ms": round(t_adj, 3),
                          "ratio": round(t_adj / t_fwd, 3), "J": J,
                          "dJ_dparams": dict(zip(("nu", "M", "sigma12", "sigma13", "sigma23"), map(float, gp)))}
