@@ -116,15 +116,15 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   if (model == CHNS_MODEL_NS) {
     auto k = k_spec_inv<N, R, GPC, MODEL_NS>;
     set_smem(k, S::FFT_SMEM);
-    k<<<rows_inv, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    k<<<dim3(rows_inv, spec_inv_split<N>() ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
   } else if (model == CHNS_MODEL_BINARY) {
     auto k = k_spec_inv<N, R, GPC, MODEL_BINARY>;
     set_smem(k, S::FFT_SMEM);
-    k<<<rows_inv, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    k<<<dim3(rows_inv, spec_inv_split<N>() ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
   } else {
     auto k = k_spec_inv<N, R, GPC, MODEL_TERNARY>;
     set_smem(k, S::FFT_SMEM);
-    k<<<rows_inv, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    k<<<dim3(rows_inv, spec_inv_split<N>() ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
   }
   launches++;
   mark(c, KIND_SPEC_INV);
