@@ -1,7 +1,11 @@
-// chns_adjoint.cu -- discrete adjoint of n binary ETD2RK steps (chns_adjoint).
+// chns_adjoint.cu -- discrete adjoint of n ETD2RK steps (chns_adjoint), binary
+// and ternary models.
 //
-// Gradient of a final-time functional J(c_T) with respect to the initial spectral
-// state (omega_hat_0, c_hat_0) and to nu, lambda (the mobility M) and sigma.
+// Gradient of a final-time functional J with respect to the initial spectral
+// state (omega_hat_0 and c_hat_0, or c1_hat_0 and c2_hat_0) and to nu, lambda (the
+// mobility M) and sigma (binary) or sigma_12, sigma_13, sigma_23 (ternary).  The
+// schedule below is shared; Adj (binary) and AdjT3 (ternary) supply the buffers,
+// the transposed step and the loss.
 // Reverse sweep with two-level checkpointing: the forward pass keeps the state
 // every `ckpt` steps; each segment is recomputed forward from its checkpoint
 // (the last one is recorded during the forward pass), keeping per step u_n, the
