@@ -51,18 +51,58 @@ template <int DIR, class R> __device__ __forceinline__ cx<R> mul_i(cx<R> a) {
   return DIR < 0 ? mk<R>(a.y, -a.x) : mk<R>(-a.y, a.x);
 }
 
+// Butterfly adds.  In FP32 a complex add or subtract is one packed f32x2
+// instruction (sm_100a): two IEEE round-to-nearest adds, the results of the
+// scalar pair, in half the issue slots of the transforms' dominant operation.
+template <class R> __device__ __forceinline__ cx<R> badd(cx<R> a, cx<R> b) { return a + b; }
+template <class R> __device__ __forceinline__ cx<R> bsub(cx<R> a, cx<R> b) { return a - b; }
+__device__ __forceinline__ cxf badd(cxf a, cxf b) {
+  const float2 r = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+  return mk<float>(r.x, r.y);
+}
+__device__ __forceinline__ cxf bsub(cxf a, cxf b) {
+  cxf r;
+  asm("{\n\t.reg .b64 p, q, d;\n\tmov.b64 p, {%2, %3};\n\tmov.b64 q, {%4, %5};\n\t"
+      "sub.rn.f32x2 d, p, q;\n\tmov.b64 {%0, %1}, d;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
+// t1 + DIR i d and t1 - DIR i d: the swapped components of i d have no packed
+// form, so these stay scalar (and need no register moves)
+template <int DIR, class R> __device__ __forceinline__ void rot_pm(cx<R>& a, cx<R>& b, cx<R> t1, cx<R> d) {
+  if (DIR < 0) {
+    a = mk<R>(t1.x + d.y, t1.y - d.x);
+    b = mk<R>(t1.x - d.y, t1.y + d.x);
+  } else {
+    a = mk<R>(t1.x - d.y, t1.y + d.x);
+    b = mk<R>(t1.x + d.y, t1.y - d.x);
+  }
+}
+
 template <int DIR, class R> __device__ __forceinline__ void dft2(cx<R>& a0, cx<R>& a1) {
-  cx<R> t = a0 - a1;
-  a0 = a0 + a1;
+  cx<R> t = bsub(a0, a1);
+  a0 = badd(a0, a1);
   a1 = t;
 }
 
 template <int DIR, class R> __device__ __forceinline__ void dft4(cx<R>& a0, cx<R>& a1, cx<R>& a2, cx<R>& a3) {
-  cx<R> t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = mul_i<DIR>(a1 - a3);
-  a0 = t0 + t2;
-  a2 = t0 - t2;
-  a1 = t1 + t3;
-  a3 = t1 - t3;
+  const cx<R> t0 = badd(a0, a2), t1 = bsub(a0, a2), t2 = badd(a1, a3), d = bsub(a1, a3);
+  a0 = badd(t0, t2);
+  a2 = bsub(t0, t2);
+  rot_pm<DIR>(a1, a3, t1, d);
+}
+
+// dft4 whose third input enters multiplied by DIR i (the W16^4 twiddle of the
+// radix-16 and radix-8 stages), folded into the scalar adds
+template <int DIR, class R> __device__ __forceinline__ void dft4_i2(cx<R>& a0, cx<R>& a1, cx<R>& a2, cx<R>& a3) {
+  cx<R> t0, t1;
+  rot_pm<DIR>(t0, t1, a0, a2);  // a0 + DIR i a2, a0 - DIR i a2
+  const cx<R> t2 = badd(a1, a3), d = bsub(a1, a3);
+  a0 = badd(t0, t2);
+  a2 = bsub(t0, t2);
+  rot_pm<DIR>(a1, a3, t1, d);
 }
 
 // constants of the 16th roots of unity
@@ -113,10 +153,14 @@ template <int DIR, int RADIX, int STRIDE, class R> __device__ __forceinline__ vo
     dft4<DIR>(y[0], y[2], y[4], y[6]);
     dft4<DIR>(y[1], y[3], y[5], y[7]);
     y[3] = tw16<DIR, 2>(y[3]);
-    y[5] = tw16<DIR, 4>(y[5]);
     y[7] = tw16<DIR, 6>(y[7]);
-#pragma unroll
-    for (int k2 = 0; k2 < 4; k2++) dft2<DIR>(y[2 * k2], y[2 * k2 + 1]);
+    dft2<DIR>(y[0], y[1]);
+    dft2<DIR>(y[2], y[3]);
+    {
+      const cx<R> a = y[4], b = y[5];  // (a + DIR i b, a - DIR i b): the W16^4 twiddle folded in
+      rot_pm<DIR>(y[4], y[5], a, b);
+    }
+    dft2<DIR>(y[6], y[7]);
 #pragma unroll
     for (int k = 0; k < 8; k++) v[k * STRIDE] = y[(k / 4) + 2 * (k % 4)];
   } else {
@@ -131,13 +175,14 @@ template <int DIR, int RADIX, int STRIDE, class R> __device__ __forceinline__ vo
     y[9] = tw16<DIR, 2>(y[9]);
     y[13] = tw16<DIR, 3>(y[13]);
     y[6] = tw16<DIR, 2>(y[6]);
-    y[10] = tw16<DIR, 4>(y[10]);
     y[14] = tw16<DIR, 6>(y[14]);
     y[7] = tw16<DIR, 3>(y[7]);
     y[11] = tw16<DIR, 6>(y[11]);
     y[15] = tw16<DIR, 9>(y[15]);
-#pragma unroll
-    for (int k2 = 0; k2 < 4; k2++) dft4<DIR>(y[4 * k2], y[4 * k2 + 1], y[4 * k2 + 2], y[4 * k2 + 3]);
+    dft4<DIR>(y[0], y[1], y[2], y[3]);
+    dft4<DIR>(y[4], y[5], y[6], y[7]);
+    dft4_i2<DIR>(y[8], y[9], y[10], y[11]);  // y[10] carries the W16^4 twiddle
+    dft4<DIR>(y[12], y[13], y[14], y[15]);
 #pragma unroll
     for (int k = 0; k < 16; k++) v[k * STRIDE] = y[(k / 4) + 4 * (k % 4)];
   }
