@@ -457,6 +457,25 @@ def run_gpu(args):
     e2e = e2e_host_loop(ctx, stream, max(3, min(args.steps, 10)))
     ctx.close()
 
+    # ---------------- FP32 right-hand side with the state in double ----------------
+    s64 = None
+    if args.state64_steps > 0:
+        cs = C.Context(workload_params(n, C.FP32_STATE64, dt=args.dt))
+        cs.set_state(*st0)
+        L.chns_set_stream(cs.handle, ctypes_stream(stream))
+        cs.step(3)
+        cs.synchronize()
+        ev0.record(stream)
+        cs.step(args.state64_steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        s64_sps = args.state64_steps / (ev0.elapsed_time(ev1) / 1e3)
+        s64_prof = profile_kernels(cs, L, stream, reps=5)
+        cs.close()
+        s64 = {"steps_per_s": round(s64_sps, 3), "steps": args.state64_steps,
+               "per_kernel_ms": s64_prof["per_kernel_ms"],
+               "note": "CHNS_FP32_STATE64: the FP32 right-hand side with w, c and the ETD update in double"}
+
     # ---------------- FP64 plain step (reference coefficients) on the same workload ----------------
     ctx64 = C.Context(workload_params(n, C.FP64, coef_mode=0, dt=args.dt))
     ctx64.set_state(*st0)
@@ -475,15 +494,17 @@ def run_gpu(args):
     acc = None
     if args.accuracy_steps > 0:
         res = []
-        for prec in (C.FP64, C.FP32):
+        for prec in (C.FP64, C.FP32, C.FP32_STATE64):
             with C.Context(workload_params(n, prec, coef_mode=1, dt=args.dt)) as c:
                 c.set_state(*st0)
                 c.step(args.accuracy_steps)
                 res.append(c.get_state())
         err = [float(np.linalg.norm(b - a) / np.linalg.norm(a)) for a, b in zip(res[0], res[1])]
+        err64 = [float(np.linalg.norm(b - a) / np.linalg.norm(a)) for a, b in zip(res[0], res[2])]
         mean_drift = abs(res[1][1][0, 0] - st0[1][0, 0]) / abs(st0[1][0, 0])
         acc = {"steps": args.accuracy_steps, "rel_l2_w": err[0], "rel_l2_c": err[1],
-               "mean_c_rel_drift_fp32": float(mean_drift), "coefficients": "series/expm1 (FP64) in both"}
+               "mean_c_rel_drift_fp32": float(mean_drift), "coefficients": "series/expm1 (FP64) in all",
+               "state64": {"rel_l2_w": err64[0], "rel_l2_c": err64[1]}}
         del res
 
     # single-GPU legs (the other ranks of a replica run would only wait for them)
@@ -523,6 +544,7 @@ def run_gpu(args):
             "fp64_steps_per_s": round(fp64_sps, 3),
             "fp32_over_fp64": round((value / world) / fp64_sps, 3),
             "fp32_vs_fp64": acc,
+            "fp32_state64": s64,
             "init": init,
             "diagnostics": diag,
             "adjoint": adj,
@@ -608,7 +630,7 @@ def profile_kernels(ctx, L, stream, reps: int):
     per_launch = {k: per[k] / cnt[k] for k in per}
     n = ctx.nx
     jt = n // 4
-    cx = 8 if ctx.params.get("precision", 0) == 1 else 16
+    cx = 16 if ctx.params.get("precision", 0) == 0 else 8
     S = (n // 2 + 1) * n * cx
     G = (jt + 1) * n * cx
     disc = disc_modes(n) * cx
@@ -745,6 +767,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dt", type=float, default=DT_DEFAULT)
     ap.add_argument("--accuracy-steps", type=int, default=1000)
+    ap.add_argument("--state64-steps", type=int, default=200,
+                    help="steps of the FP32-with-double-state throughput leg (0: skip)")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
     ap.add_argument("--ensemble-steps", type=int, default=500, help="steps of the ensemble leg (0: skip)")
     ap.add_argument("--adjoint-big-steps", type=int, default=1000,

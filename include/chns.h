@@ -43,7 +43,16 @@ extern "C" {
 #define CHNS_ERR_IO (-7)          /* a file could not be read or written */
 
 enum { CHNS_MODEL_NS = 0, CHNS_MODEL_BINARY = 1, CHNS_MODEL_TERNARY = 2 };
-enum { CHNS_FP64 = 0, CHNS_FP32 = 1 };
+/* Arithmetic of a context.  FP64: every operation in double (the reference's
+ * arithmetic).  FP32: transforms and point-wise work in float, ETD coefficients
+ * computed in double, k = 0 modes kept in double.  FP32_STATE64: the FP32
+ * right-hand side, with the state (w, c_i) kept in double and the ETD update
+ * done in double with double coefficients; the float copy of the state that the
+ * right-hand side reads is rounded from it after every stage.  At small dt an
+ * FP32 state loses the low bits of every increment, and the spinodal modes
+ * amplify that rounding: FP32_STATE64 removes this error source for one more
+ * read and write of each evolved field per stage. */
+enum { CHNS_FP64 = 0, CHNS_FP32 = 1, CHNS_FP32_STATE64 = 2 };
 /* ETD phi-function coefficients: REFERENCE evaluates etd2rk.c's direct formulas
  * (etd2rk.c:88-206, with its small-|c| branches) on the host in double, so
  * the FP64 step reproduces the reference; ACCURATE uses expm1 and a series for
@@ -53,7 +62,7 @@ enum { CHNS_HOST = 0, CHNS_DEVICE = 1 };
 
 typedef struct chns_params {
     int model;          /* CHNS_MODEL_*: none / BINARY / TERNARY (macro.h) */
-    int precision;      /* CHNS_FP64 or CHNS_FP32 */
+    int precision;      /* CHNS_FP64, CHNS_FP32 or CHNS_FP32_STATE64 */
     int nx, ny;         /* Nx, Ny (global.h:23-24); nx == ny, power of two, 32..4096 */
     double lx, ly;      /* box (global.h:20-21) */
     double dt, nu;      /* dt, nu (global.h:30-31) */
@@ -199,7 +208,7 @@ int chns_read_phase(chns_ctx *ctx, const char *path1, const char *path2);
  * dJ/d(nu, lambda, sigma) (binary, 3 values) or dJ/d(nu, lambda, sigma_12,
  * sigma_13, sigma_23) (ternary, 5 values).  The state is kept every `ckpt` steps
  * and recomputed in between; it is unchanged on return.  Pure Navier-Stokes
- * contexts return CHNS_ERR_UNSUPPORTED. */
+ * contexts and CHNS_FP32_STATE64 contexts return CHNS_ERR_UNSUPPORTED. */
 int chns_adjoint(chns_ctx *ctx, int nsteps, int ckpt, const double *loss_w, double *J, double *g_w,
                  double *g_c, double *g_params, int where);
 

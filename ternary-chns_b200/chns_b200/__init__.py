@@ -22,7 +22,7 @@ PKG = os.path.dirname(HERE)
 LIB_PATH = os.path.join(PKG, "lib", "libchns_b200.so")
 
 MODEL_NS, MODEL_BINARY, MODEL_TERNARY = 0, 1, 2
-FP64, FP32 = 0, 1
+FP64, FP32, FP32_STATE64 = 0, 1, 2
 COEF_REFERENCE, COEF_ACCURATE = 0, 1
 HOST, DEVICE = 0, 1
 INIT_W_ZERO, INIT_W_TAYLOR_GREEN = 0, 1

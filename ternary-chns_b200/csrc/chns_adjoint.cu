@@ -713,6 +713,8 @@ extern "C" int chns_adjoint(chns_ctx* c, int nsteps, int ckpt, const double* los
                             double* g_c, double* g_par, int where) {
   if (!c || nsteps < 1 || ckpt < 1) return CHNS_ERR_ARG;
   if (c->p.model == CHNS_MODEL_NS) return CHNS_ERR_UNSUPPORTED;
+  // the checkpoints hold the float state; a double state would not be restored
+  if (c->st64) return CHNS_ERR_UNSUPPORTED;
   const double dflt[3] = {1.0, 1.0, 1.0};
   const double* lw = loss_w ? loss_w : dflt;
   if (c->p.model == CHNS_MODEL_BINARY)

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "chns_internal.h"
+#include "chns_kernels.cuh"
 
 namespace chns {
 #define CHNS_DECL(NN)                  \
@@ -137,7 +138,8 @@ void etd_coefs(const chns_params& p, double ksqr, double* o) {
 int validate(const chns_params* p) {
   if (!p) return CHNS_ERR_ARG;
   if (p->model < 0 || p->model > 2) return CHNS_ERR_ARG;
-  if (p->precision != CHNS_FP64 && p->precision != CHNS_FP32) return CHNS_ERR_ARG;
+  if (p->precision != CHNS_FP64 && p->precision != CHNS_FP32 && p->precision != CHNS_FP32_STATE64)
+    return CHNS_ERR_ARG;
   if (p->nx != p->ny) return CHNS_ERR_UNSUPPORTED;
   const int l = ilog2_exact(p->nx);
   if (l < 5 || l > 12) return CHNS_ERR_UNSUPPORTED;
@@ -158,7 +160,8 @@ void free_all(chns_ctx* c) {
   chns_adj_free(c);
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   void* ptrs[] = {c->state[0], c->state[1], c->state[2], c->saved[0], c->saved[1], c->saved[2], c->nw,
-                  c->coef, c->mrow, c->tw, c->k0, c->stage, c->realbuf, c->realdbl, c->red, c->redscratch};
+                  c->coef, c->mrow, c->tw, c->k0, c->stage, c->realbuf, c->realdbl, c->red, c->redscratch,
+                  c->state64[0], c->state64[1], c->state64[2], c->coef64};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (void* q : c->g)
@@ -280,7 +283,8 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
   const chns_params& p = c->p;
   c->n = p.nx;
   c->nr = p.nx / 2 + 1;
-  c->f32 = p.precision == CHNS_FP32;
+  c->f32 = p.precision != CHNS_FP64;
+  c->st64 = p.precision == CHNS_FP32_STATE64;
   c->rsz = c->f32 ? 4 : 8;
   const int logn = ilog2_exact(c->n);
   c->L = c->f32 ? chns::launchers_f32(logn) : chns::launchers_f64(logn);
@@ -371,12 +375,14 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
     if (f < nfields) {
       rc = dmalloc(&c->state[f], ncx * cxsz);
       if (rc == CHNS_OK) rc = dmalloc(&c->saved[f], ncx * cxsz);
+      if (rc == CHNS_OK && c->st64) rc = dmalloc(&c->state64[f], ncx * 2 * sizeof(double));
     }
   }
   if (rc == CHNS_OK) rc = dmalloc(&c->nw, ncx * cxsz);
   for (int k = 0; k < chns::kNumG && rc == CHNS_OK; k++) rc = dmalloc(&c->g[k], ngx * cxsz);
   for (int k = 0; k < chns::kNumH && rc == CHNS_OK; k++) rc = dmalloc(&c->h[k], nhx * cxsz);
   if (rc == CHNS_OK) rc = dmalloc(&c->coef, 6 * tsz * c->rsz);
+  if (rc == CHNS_OK && c->st64) rc = dmalloc(&c->coef64, 6 * tsz * sizeof(double));
   if (rc == CHNS_OK) rc = dmalloc((void**)&c->mrow, nr * sizeof(int));
   if (rc == CHNS_OK) rc = dmalloc(&c->tw, (size_t)n * cxsz);
   if (rc == CHNS_OK) rc = dmalloc((void**)&c->k0, 16 * sizeof(double));
@@ -396,6 +402,7 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
     std::vector<float> tf(twd.begin(), twd.end());
     e = cudaMemcpy(c->coef, cf.data(), cf.size() * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->tw, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && c->st64) e = cudaMemcpy(c->coef64, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice);
   } else {
     e = cudaMemcpy(c->coef, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->tw, twd.data(), twd.size() * 8, cudaMemcpyHostToDevice);
@@ -470,12 +477,31 @@ int chns_synchronize(chns_ctx* c) {
   return CHNS_OK;
 }
 
+// FFTW-layout double <-> S-layout double (the double state of CHNS_FP32_STATE64)
+static void fftw_to_s64(chns_ctx* c, const double* src, void* s) {
+  const dim3 grid((c->nr + 31) / 32, (c->n + 31) / 32);
+  chns::k_fftw_to_s<double><<<grid, dim3(32, 8), 0, c->stream>>>((const double2*)src, (chns::cxd*)s, c->n);
+}
+static void s64_to_fftw(chns_ctx* c, const void* s, double* dst) {
+  const dim3 grid((c->nr + 31) / 32, (c->n + 31) / 32);
+  chns::k_s_to_fftw<double><<<grid, dim3(32, 8), 0, c->stream>>>((const chns::cxd*)s, (double2*)dst, c->n);
+}
+
+__global__ void k_widen_state(const float2* __restrict__ a, double2* __restrict__ b, size_t n, const double* k0,
+                              int slot) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float2 v = a[i];
+    b[i] = i == 0 ? make_double2(k0[2 * slot], k0[2 * slot + 1]) : make_double2((double)v.x, (double)v.y);
+  }
+}
+
 static int set_field(chns_ctx* c, int f, const double* src, int where) {
   const size_t bytes = 2 * (size_t)c->n * c->nr * sizeof(double);
   int rc = to_device(c, c->stage, src, bytes, where);
   if (rc) return rc;
   c->L->from_fftw(c, c->stage, c->state[f]);
   if (c->f32) k_k0_set<<<1, 1, 0, c->stream>>>(c->k0, c->stage, f);
+  if (c->st64) fftw_to_s64(c, c->stage, c->state64[f]);
   CK(cudaGetLastError());
   return CHNS_OK;
 }
@@ -504,9 +530,24 @@ int chns_get_state(chns_ctx* c, double* w, double* c1, double* c2, int where) {
   double* dst[3] = {w, c1, c2};
   for (int f = 0; f <= c->p.model; f++) {
     if (!dst[f]) continue;
-    int rc = get_field(c, f, c->state[f], dst[f], where, f);
+    int rc;
+    if (c->st64) {
+      s64_to_fftw(c, c->state64[f], c->stage);
+      CK(cudaGetLastError());
+      rc = from_device(c, dst[f], c->stage, 2 * (size_t)c->n * c->nr * sizeof(double), where);
+    } else {
+      rc = get_field(c, f, c->state[f], dst[f], where, f);
+    }
     if (rc) return rc;
   }
+  return CHNS_OK;
+}
+
+int chns_state64_from_f32(chns_ctx* c, int f) {
+  if (!c->st64) return CHNS_OK;
+  const size_t ncx = (size_t)c->n * c->nr;
+  k_widen_state<<<1024, 256, 0, c->stream>>>((const float2*)c->state[f], (double2*)c->state64[f], ncx, c->k0, f);
+  CK(cudaGetLastError());
   return CHNS_OK;
 }
 
@@ -534,7 +575,7 @@ int chns_phase_from_realdbl(chns_ctx* c, int f) {
     k_k0_set<<<1, 1, 0, c->stream>>>(c->k0, c->stage, 1 + f);
   }
   CK(cudaGetLastError());
-  return CHNS_OK;
+  return chns_state64_from_f32(c, 1 + f);
 }
 
 int chns_set_phase_real(chns_ctx* c, const double* p1, const double* p2, int where) {
@@ -543,6 +584,7 @@ int chns_set_phase_real(chns_ctx* c, const double* p1, const double* p2, int whe
   const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
   CK(cudaMemsetAsync(c->state[0], 0, bytes, c->stream));  // init.c:78-87
   if (c->f32) CK(cudaMemsetAsync(c->k0, 0, 2 * sizeof(double), c->stream));
+  if (c->st64) CK(cudaMemsetAsync(c->state64[0], 0, 2 * bytes, c->stream));
   const double* src[2] = {p1, p2};
   for (int f = 0; f < c->p.model; f++) {
     const size_t nn = (size_t)c->n * c->n;
@@ -580,12 +622,19 @@ int chns_rhs(chns_ctx* c, double* nw, double* nc1, double* nc2, int where) {
   // a copy of the state and restore the state afterwards
   const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
   void* keep[3] = {nullptr, nullptr, nullptr};
+  void* keep64[3] = {nullptr, nullptr, nullptr};
   double k0keep[12];
   int rc = CHNS_OK;
   for (int f = 0; f <= c->p.model && rc == CHNS_OK; f++) {
     if (cudaMalloc(&keep[f], bytes) != cudaSuccess) rc = CHNS_ERR_NOMEM;
     else if (cudaMemcpyAsync(keep[f], c->state[f], bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
       rc = CHNS_ERR_CUDA;
+    if (rc == CHNS_OK && c->st64) {
+      if (cudaMalloc(&keep64[f], 2 * bytes) != cudaSuccess) rc = CHNS_ERR_NOMEM;
+      else if (cudaMemcpyAsync(keep64[f], c->state64[f], 2 * bytes, cudaMemcpyDeviceToDevice, c->stream) !=
+               cudaSuccess)
+        rc = CHNS_ERR_CUDA;
+    }
   }
   if (rc == CHNS_OK && c->f32 && cudaMemcpy(k0keep, c->k0, sizeof(k0keep), cudaMemcpyDeviceToHost) != cudaSuccess)
     rc = CHNS_ERR_CUDA;
@@ -598,6 +647,11 @@ int chns_rhs(chns_ctx* c, double* nw, double* nc1, double* nc2, int where) {
       cudaMemcpyAsync(c->state[f], keep[f], bytes, cudaMemcpyDeviceToDevice, c->stream);
       cudaStreamSynchronize(c->stream);
       cudaFree(keep[f]);
+    }
+    if (keep64[f]) {
+      cudaMemcpyAsync(c->state64[f], keep64[f], 2 * bytes, cudaMemcpyDeviceToDevice, c->stream);
+      cudaStreamSynchronize(c->stream);
+      cudaFree(keep64[f]);
     }
   }
   if (c->f32) cudaMemcpy(c->k0, k0keep, sizeof(k0keep), cudaMemcpyHostToDevice);

@@ -56,6 +56,7 @@ template <class R> struct Par {
   double k0coef[6];        // ETD coefficients at k = 0 (double)
   const int* mrow;         // [n/2+1] largest |m| kept by the truncation per row (-1: none)
   const R* coef;           // [6][n/2+1][n/2+1] ETD coefficients at (row, |m|)
+  const double* coef64;    // the same in double (FP32 contexts with a double state), else null
   const cx<R>* tw;         // tw[q] = exp(-2 pi i q / n)
   double* k0;              // FP32 only: k = 0 modes in double [w, c1, c2, sw, s1, s2] x (re, im)
 };
@@ -71,6 +72,7 @@ template <class R> struct Bufs {
   cx<R>* x1;
   cx<R>* x2;
   cx<R>* nw;
+  cxd* m[3];   // FP32 contexts with a double state: w, c1, c2 in double (else null)
   cx<R>* g[NG];
   cx<R>* h[NH];
 };
@@ -595,6 +597,28 @@ __device__ __forceinline__ void etd_k0(double* st, double* sv, double nx, double
   }
 }
 
+// ETD update of one mode of an FP32 context whose state is kept in double:
+// u (read from and written back to u64[idx]) and the update in double with the
+// double coefficients cf[0], cf[cs], cf[2 cs] (e, z1, z2); N and the saved N
+// stay float.  Returns the float rounding of the new u for the float copy.
+template <int STAGE, class R>
+__device__ __forceinline__ cx<R> etd64(cxd* __restrict__ u64, size_t idx, bool live, cx<R> nl, cx<R>* saved,
+                                       const double* __restrict__ cf, size_t cs) {
+  const cxd u = live ? u64[idx] : mk<double>(0.0, 0.0);
+  cxd r;
+  if (STAGE == 1) {
+    *saved = nl;
+    const double e = cf[0], z1 = cf[cs];
+    r = mk<double>(u.x * e + (double)nl.x * z1, u.y * e + (double)nl.y * z1);
+  } else {
+    const cx<R> s = *saved;
+    const double z2 = cf[2 * cs];
+    r = mk<double>(u.x + ((double)nl.x - (double)s.x) * z2, u.y + ((double)nl.y - (double)s.y) * z2);
+  }
+  if (live) u64[idx] = r;
+  return mk<R>((R)r.x, (R)r.y);
+}
+
 // ---------------------------------------------------------------------------
 // P3 (phase-field models): x forward transforms, N_w partial, mu and its x
 // inverse transform, N_c and the ETD update of c  (H -> S, G)
@@ -603,7 +627,8 @@ __device__ __forceinline__ void etd_k0(double* st, double* sv, double nx, double
 // ternary: chem_potential.c:319-320 (F[mu^F]), surface_tension.c:116-137,
 //          nonlin.c:300-377, etd2rk.c:117-130 / 191-206
 // ---------------------------------------------------------------------------
-template <int N, class R, int GPC, int MODEL, int STAGE>
+// S64: FP32 context whose state is kept in double (B.m, P.coef64)
+template <int N, class R, int GPC, int MODEL, int STAGE, bool S64>
 __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
@@ -636,6 +661,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
     cx<R>* cst = fld == 0 ? B.c1 : B.c2;
     cx<R>* csv = fld == 0 ? B.s1 : B.s2;
     cx<R>* cx_out = fld == 0 ? B.x1 : B.x2;
+    cxd* c64 = B.m[1 + fld];
     // F[f(c)] (binary) or F[mu^F_i] (ternary)
     if (MODEL == MODEL_BINARY) load_row<N>(f, B.h[HF], row, live, t);
     else load_row_pair<N>(f, B.h[HF], row, fld, live, t);
@@ -684,10 +710,14 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
         nl = mk<R>(rsub(-v[m].x, rmul(q, f[m].x)), rsub(-v[m].y, rmul(q, f[m].y)));
       }
       const size_t idx = (size_t)rowc * N + t + NT * m;
-      const R e = cf[3 * cstride + am], z1 = cf[4 * cstride + am], z2 = cf[5 * cstride + am];
       cx<R> sv;
       if (STAGE == 2) sv = live ? csv[idx] : czero<R>();
-      c[m] = etd<STAGE>(c[m], nl, &sv, e, z1, z2);
+      if (S64) {
+        c[m] = etd64<STAGE>(c64, idx, live, nl, &sv, P.coef64 + (size_t)rowc * NR + 3 * cstride + am, cstride);
+      } else {
+        const R e = cf[3 * cstride + am], z1 = cf[4 * cstride + am], z2 = cf[5 * cstride + am];
+        c[m] = etd<STAGE>(c[m], nl, &sv, e, z1, z2);
+      }
       if (STAGE == 1 && live) csv[idx] = sv;
       if (STAGE == 2 && cx_out && live) cx_out[idx] = nl;
       if (F32 && row == 0 && t == 0 && m == 0) {
@@ -695,6 +725,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
         double* sd = P.k0 + 2 * (4 + fld);
         etd_k0<STAGE>(st, sd, (double)nl.x, (double)nl.y, P.k0coef, 3);
         c[m] = mk<R>((R)st[0], (R)st[1]);
+        if (S64) c64[0] = mk<double>(st[0], st[1]);
       }
     }
     store_row<N>(c, cst, row, live, t);
@@ -707,7 +738,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
 // etd2rk.c:88-99 / 162-174.  Pure Navier-Stokes (CURL = false):
 // N_w = -F[u.grad w] (nonlin.c:74-101) from the plain field in HAB.
 // ---------------------------------------------------------------------------
-template <int N, class R, int GPC, bool CURL, int STAGE>
+template <int N, class R, int GPC, bool CURL, int STAGE, bool S64>
 __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
@@ -747,20 +778,25 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
     for (int m = 0; m < 16; m++) a[m] = mk<R>(a[m].x * (R)(-1), a[m].y * (R)(-1));
   }
   if (P.force_j >= 0 && row == P.force_j && t == 0) a[0].x = radd(a[0].x, P.force_hat);
-  load_row<N>(b, B.w, row, live, t);
+  if (!S64) load_row<N>(b, B.w, row, live, t);  // a double state is read by the update itself
 #pragma unroll
   for (int m = 0; m < 16; m++) {
     const int am = amask<N>(t, m);
     const size_t idx = (size_t)rowc * N + t + NT * m;
-    const R e = cf[0 * cstride + am], z1 = cf[1 * cstride + am], z2 = cf[2 * cstride + am];
     cx<R> sv;
     if (STAGE == 2) sv = live ? B.sw[idx] : czero<R>();
     if (STAGE == 2 && B.xw && live) B.xw[idx] = a[m];
-    b[m] = etd<STAGE>(b[m], a[m], &sv, e, z1, z2);
+    if (S64) {
+      b[m] = etd64<STAGE>(B.m[0], idx, live, a[m], &sv, P.coef64 + (size_t)rowc * NR + am, cstride);
+    } else {
+      const R e = cf[0 * cstride + am], z1 = cf[1 * cstride + am], z2 = cf[2 * cstride + am];
+      b[m] = etd<STAGE>(b[m], a[m], &sv, e, z1, z2);
+    }
     if (STAGE == 1 && live) B.sw[idx] = sv;
     if (F32 && row == 0 && t == 0 && m == 0) {
       etd_k0<STAGE>(P.k0 + 0, P.k0 + 6, (double)a[m].x, (double)a[m].y, P.k0coef, 0);
       b[m] = mk<R>((R)P.k0[0], (R)P.k0[1]);
+      if (S64) B.m[0][0] = mk<double>(P.k0[0], P.k0[1]);
     }
   }
   store_row<N>(b, B.w, row, live, t);

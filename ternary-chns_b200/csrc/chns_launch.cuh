@@ -63,6 +63,7 @@ template <class R> Par<R> make_par(const chns_ctx* c) {
   for (int k = 0; k < 6; k++) P.k0coef[k] = c->k0coef[k];
   P.mrow = c->mrow;
   P.coef = (const R*)c->coef;
+  P.coef64 = c->st64 ? (const double*)c->coef64 : nullptr;
   P.tw = (const cx<R>*)c->tw;
   P.k0 = c->k0;
   return P;
@@ -80,6 +81,7 @@ template <class R> Bufs<R> make_bufs(const chns_ctx* c) {
   B.x1 = (cx<R>*)c->nstar[1];
   B.x2 = (cx<R>*)c->nstar[2];
   B.nw = (cx<R>*)c->nw;
+  for (int f = 0; f < 3; f++) B.m[f] = c->st64 ? (cxd*)c->state64[f] : nullptr;
   for (int k = 0; k < NG; k++) B.g[k] = (cx<R>*)c->g[k];
   for (int k = 0; k < NH; k++) B.h[k] = (cx<R>*)c->h[k];
   return B;
@@ -111,6 +113,9 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   const int rows_all = S::grid_rows(N / 2 + 1);
   const int pairs = S::grid_rows(N / 2);
   int launches = 0;
+  // FP32 contexts with a double state run the P3 / P5 variants that update it
+  constexpr bool F32 = sizeof(R) == 4;
+  const bool s64 = F32 && c->st64;
 
   // P1: spectral fan-out and x inverse transforms
   if (model == CHNS_MODEL_NS) {
@@ -152,11 +157,11 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   if (model == CHNS_MODEL_NS) {
     // pure Navier-Stokes: N_w = -F[u.grad w], ETD of w
     if (stage == 1) {
-      auto k = k_spec_curl_w<N, R, GPC, false, 1>;
+      auto k = s64 ? k_spec_curl_w<N, R, GPC, false, 1, F32> : k_spec_curl_w<N, R, GPC, false, 1, false>;
       set_smem(k, S::FFT_SMEM);
       k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
     } else {
-      auto k = k_spec_curl_w<N, R, GPC, false, 2>;
+      auto k = s64 ? k_spec_curl_w<N, R, GPC, false, 2, F32> : k_spec_curl_w<N, R, GPC, false, 2, false>;
       set_smem(k, S::FFT_SMEM);
       k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
     }
@@ -167,21 +172,21 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   // P3: x forward transforms, mu, N_c, ETD of c
   if (model == CHNS_MODEL_BINARY) {
     if (stage == 1) {
-      auto k = k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1>;
+      auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1, F32> : k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1, false>;
       set_smem(k, S::FFT_SMEM);
       k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
     } else {
-      auto k = k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 2>;
+      auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 2, F32> : k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 2, false>;
       set_smem(k, S::FFT_SMEM);
       k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
     }
   } else {
     if (stage == 1) {
-      auto k = k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 1>;
+      auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 1, F32> : k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 1, false>;
       set_smem(k, S::FFT_SMEM);
       k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
     } else {
-      auto k = k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 2>;
+      auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 2, F32> : k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 2, false>;
       set_smem(k, S::FFT_SMEM);
       k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
     }
@@ -206,11 +211,11 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
 
   // P5: curl, N_w, ETD of w
   if (stage == 1) {
-    auto k = k_spec_curl_w<N, R, GPC, true, 1>;
+    auto k = s64 ? k_spec_curl_w<N, R, GPC, true, 1, F32> : k_spec_curl_w<N, R, GPC, true, 1, false>;
     set_smem(k, S::FFT_SMEM);
     k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
   } else {
-    auto k = k_spec_curl_w<N, R, GPC, true, 2>;
+    auto k = s64 ? k_spec_curl_w<N, R, GPC, true, 2, F32> : k_spec_curl_w<N, R, GPC, true, 2, false>;
     set_smem(k, S::FFT_SMEM);
     k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
   }
