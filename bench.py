@@ -474,7 +474,7 @@ def run_gpu(args):
         cs.close()
         s64 = {"steps_per_s": round(s64_sps, 3), "steps": args.state64_steps,
                "per_kernel_ms": s64_prof["per_kernel_ms"],
-               "note": "CHNS_FP32_STATE64: the FP32 right-hand side with w, c and the ETD update in double"}
+               "note": "CHNS_FP32_STATE64: the FP32 right-hand side, w and c as float pairs (hi + lo) inside the truncation disc, the ETD update in double"}
 
     # ---------------- FP64 plain step (reference coefficients) on the same workload ----------------
     ctx64 = C.Context(workload_params(n, C.FP64, coef_mode=0, dt=args.dt))
@@ -565,7 +565,7 @@ def run_gpu(args):
 
 def run_profile_case(args):
     """A small, fixed piece of work for an ncu capture: "step" = the workload's FP32
-    context stepped --steps times; "adjoint" = one adjoint of --steps steps (K = 20)
+    context stepped --steps times ("step_state64": the CHNS_FP32_STATE64 context); "adjoint" = one adjoint of --steps steps (K = 20)
     at 512^2 FP64 after a warm-up call; "ensemble" = --steps ensemble steps of the
     64-member ternary ensemble."""
     import torch
@@ -592,7 +592,8 @@ def run_profile_case(args):
         return
     n = args.n
     c0, w0 = initial_fields(n)
-    with C.Context(workload_params(n, C.FP32, dt=args.dt)) as ctx:
+    prec = C.FP32_STATE64 if args.profile_case == "step_state64" else C.FP32
+    with C.Context(workload_params(n, prec, dt=args.dt)) as ctx:
         ctx.set_phase_real(c0)
         st = ctx.get_state()
         st[0] = w0

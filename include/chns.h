@@ -46,12 +46,15 @@ enum { CHNS_MODEL_NS = 0, CHNS_MODEL_BINARY = 1, CHNS_MODEL_TERNARY = 2 };
 /* Arithmetic of a context.  FP64: every operation in double (the reference's
  * arithmetic).  FP32: transforms and point-wise work in float, ETD coefficients
  * computed in double, k = 0 modes kept in double.  FP32_STATE64: the FP32
- * right-hand side, with the state (w, c_i) kept in double and the ETD update
- * done in double with double coefficients; the float copy of the state that the
- * right-hand side reads is rounded from it after every stage.  At small dt an
- * FP32 state loses the low bits of every increment, and the spinodal modes
- * amplify that rounding: FP32_STATE64 removes this error source for one more
- * read and write of each evolved field per stage. */
+ * right-hand side, with the state (w, c_i) carried as a pair of floats hi + lo
+ * (48 significant bits) and the ETD update done in double (u + (u (e - 1) + N
+ * z1), e - 1 from expm1); the right-hand side reads hi, the float rounding of the
+ * state.  At small dt an FP32 state loses the low bits of every increment, and
+ * the spinodal modes amplify that rounding: FP32_STATE64 removes this error
+ * source for one more float read and write of the modes inside the truncation
+ * disc per stage (the modes outside it never reach a right-hand side, so they
+ * stay float).  chns_set_state / chns_get_state convert to and from the pair
+ * (relative rounding <= 2^-48 per element inside the disc, 2^-24 outside). */
 enum { CHNS_FP64 = 0, CHNS_FP32 = 1, CHNS_FP32_STATE64 = 2 };
 /* ETD phi-function coefficients: REFERENCE evaluates etd2rk.c's direct formulas
  * (etd2rk.c:88-206, with its small-|c| branches) on the host in double, so

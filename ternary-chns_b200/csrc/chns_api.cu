@@ -86,6 +86,15 @@ double phi2_z(double z) {
 
 // ETD coefficients of one wavenumber, etd2rk.c:88-97,102-111,117-127 (stage 1)
 // and :162-172,177-186,191-203 (stage 2), in the reference's operand order.
+// e - 1 of the vorticity (o[0]) and phase-field (o[1]) linear terms at k^2 = ksqr
+void etd_em1(const chns_params& p, double ksqr, double* o) {
+  o[0] = expm1(-p.nu * p.dt * ksqr);
+  double c = 0.0;
+  if (p.model == CHNS_MODEL_BINARY) c = -1.5 * p.lambda * p.sigma * p.epsilon * ksqr * ksqr;
+  else if (p.model == CHNS_MODEL_TERNARY) c = -0.75 * p.lambda * p.epsilon * ksqr * ksqr;
+  o[1] = expm1(p.dt * c);
+}
+
 void etd_coefs(const chns_params& p, double ksqr, double* o) {
   const double dt = p.dt, nu = p.nu;
   double c = -nu * ksqr;
@@ -161,7 +170,7 @@ void free_all(chns_ctx* c) {
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   void* ptrs[] = {c->state[0], c->state[1], c->state[2], c->saved[0], c->saved[1], c->saved[2], c->nw,
                   c->coef, c->mrow, c->tw, c->k0, c->stage, c->realbuf, c->realdbl, c->red, c->redscratch,
-                  c->state64[0], c->state64[1], c->state64[2], c->coef64};
+                  c->statelo[0], c->statelo[1], c->statelo[2]};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (void* q : c->g)
@@ -375,14 +384,13 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
     if (f < nfields) {
       rc = dmalloc(&c->state[f], ncx * cxsz);
       if (rc == CHNS_OK) rc = dmalloc(&c->saved[f], ncx * cxsz);
-      if (rc == CHNS_OK && c->st64) rc = dmalloc(&c->state64[f], ncx * 2 * sizeof(double));
+      if (rc == CHNS_OK && c->st64) rc = dmalloc(&c->statelo[f], ncx * cxsz);
     }
   }
   if (rc == CHNS_OK) rc = dmalloc(&c->nw, ncx * cxsz);
   for (int k = 0; k < chns::kNumG && rc == CHNS_OK; k++) rc = dmalloc(&c->g[k], ngx * cxsz);
   for (int k = 0; k < chns::kNumH && rc == CHNS_OK; k++) rc = dmalloc(&c->h[k], nhx * cxsz);
   if (rc == CHNS_OK) rc = dmalloc(&c->coef, 6 * tsz * c->rsz);
-  if (rc == CHNS_OK && c->st64) rc = dmalloc(&c->coef64, 6 * tsz * sizeof(double));
   if (rc == CHNS_OK) rc = dmalloc((void**)&c->mrow, nr * sizeof(int));
   if (rc == CHNS_OK) rc = dmalloc(&c->tw, (size_t)n * cxsz);
   if (rc == CHNS_OK) rc = dmalloc((void**)&c->k0, 16 * sizeof(double));
@@ -400,9 +408,19 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
   if (c->f32) {
     std::vector<float> cf(coef.begin(), coef.end());
     std::vector<float> tf(twd.begin(), twd.end());
+    if (c->st64) {
+      // a double-float state is advanced with e - 1 (slots 0 and 3) in place of e
+      for (int j = 0; j < nr; j++)
+        for (int m = 0; m < nr; m++) {
+          const double ks = (c->fx * m) * (c->fx * m) + (c->fy * j) * (c->fy * j);
+          double em1[2];
+          etd_em1(p, ks, em1);
+          cf[0 * tsz + (size_t)j * nr + m] = (float)em1[0];
+          cf[3 * tsz + (size_t)j * nr + m] = (float)em1[1];
+        }
+    }
     e = cudaMemcpy(c->coef, cf.data(), cf.size() * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->tw, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && c->st64) e = cudaMemcpy(c->coef64, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice);
   } else {
     e = cudaMemcpy(c->coef, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->tw, twd.data(), twd.size() * 8, cudaMemcpyHostToDevice);
@@ -477,31 +495,68 @@ int chns_synchronize(chns_ctx* c) {
   return CHNS_OK;
 }
 
-// FFTW-layout double <-> S-layout double (the double state of CHNS_FP32_STATE64)
-static void fftw_to_s64(chns_ctx* c, const double* src, void* s) {
-  const dim3 grid((c->nr + 31) / 32, (c->n + 31) / 32);
-  chns::k_fftw_to_s<double><<<grid, dim3(32, 8), 0, c->stream>>>((const double2*)src, (chns::cxd*)s, c->n);
-}
-static void s64_to_fftw(chns_ctx* c, const void* s, double* dst) {
-  const dim3 grid((c->nr + 31) / 32, (c->n + 31) / 32);
-  chns::k_s_to_fftw<double><<<grid, dim3(32, 8), 0, c->stream>>>((const chns::cxd*)s, (double2*)dst, c->n);
+// FFTW-layout double <-> S-layout double-float pair (hi = float rounding, lo =
+// float rounding of the rest): the state of CHNS_FP32_STATE64.  32 x 32 tiles
+// transposed through shared memory, as the plain layout conversions.
+__global__ void k_fftw_to_hilo(const double2* __restrict__ src, float2* __restrict__ hi, float2* __restrict__ lo,
+                               int n) {
+  __shared__ double2 tile[32][33];
+  const int nr = n / 2 + 1;
+  const int j0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int i = i0 + k, j = j0 + threadIdx.x;
+    if (i < n && j < nr) tile[k][threadIdx.x] = src[(size_t)i * nr + j];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int j = j0 + k, i = i0 + threadIdx.x;
+    if (i < n && j < nr) {
+      const double2 v = tile[threadIdx.x][k];
+      const float2 h = make_float2((float)v.x, (float)v.y);
+      hi[(size_t)j * n + i] = h;
+      lo[(size_t)j * n + i] = make_float2((float)(v.x - (double)h.x), (float)(v.y - (double)h.y));
+    }
+  }
 }
 
-__global__ void k_widen_state(const float2* __restrict__ a, double2* __restrict__ b, size_t n, const double* k0,
-                              int slot) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const float2 v = a[i];
-    b[i] = i == 0 ? make_double2(k0[2 * slot], k0[2 * slot + 1]) : make_double2((double)v.x, (double)v.y);
+__global__ void k_hilo_to_fftw(const float2* __restrict__ hi, const float2* __restrict__ lo, double2* __restrict__ dst,
+                               int n) {
+  __shared__ double2 tile[32][33];
+  const int nr = n / 2 + 1;
+  const int j0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int j = j0 + k, i = i0 + threadIdx.x;
+    if (i < n && j < nr) {
+      const float2 h = hi[(size_t)j * n + i], l = lo[(size_t)j * n + i];
+      tile[threadIdx.x][k] = make_double2((double)h.x + (double)l.x, (double)h.y + (double)l.y);
+    }
   }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int i = i0 + k, j = j0 + threadIdx.x;
+    if (i < n && j < nr) dst[(size_t)i * nr + j] = tile[k][threadIdx.x];
+  }
+}
+
+// low part of the k = 0 mode of field `slot` from its double value
+__global__ void k_lo_k0(const float2* __restrict__ hi, float2* __restrict__ lo, const double* k0, int slot) {
+  const float2 h = hi[0];
+  lo[0] = make_float2((float)(k0[2 * slot] - (double)h.x), (float)(k0[2 * slot + 1] - (double)h.y));
 }
 
 static int set_field(chns_ctx* c, int f, const double* src, int where) {
   const size_t bytes = 2 * (size_t)c->n * c->nr * sizeof(double);
   int rc = to_device(c, c->stage, src, bytes, where);
   if (rc) return rc;
-  c->L->from_fftw(c, c->stage, c->state[f]);
+  if (c->st64) {
+    const dim3 grid((c->nr + 31) / 32, (c->n + 31) / 32);
+    k_fftw_to_hilo<<<grid, dim3(32, 8), 0, c->stream>>>((const double2*)c->stage, (float2*)c->state[f],
+                                                         (float2*)c->statelo[f], c->n);
+    c->L->truncate(c, c->statelo[f]);  // low parts only inside the truncation disc
+  } else {
+    c->L->from_fftw(c, c->stage, c->state[f]);
+  }
   if (c->f32) k_k0_set<<<1, 1, 0, c->stream>>>(c->k0, c->stage, f);
-  if (c->st64) fftw_to_s64(c, c->stage, c->state64[f]);
   CK(cudaGetLastError());
   return CHNS_OK;
 }
@@ -532,7 +587,10 @@ int chns_get_state(chns_ctx* c, double* w, double* c1, double* c2, int where) {
     if (!dst[f]) continue;
     int rc;
     if (c->st64) {
-      s64_to_fftw(c, c->state64[f], c->stage);
+      const dim3 grid((c->nr + 31) / 32, (c->n + 31) / 32);
+      k_hilo_to_fftw<<<grid, dim3(32, 8), 0, c->stream>>>((const float2*)c->state[f], (const float2*)c->statelo[f],
+                                                          (double2*)c->stage, c->n);
+      k_k0_get<<<1, 1, 0, c->stream>>>(c->k0, c->stage, f);
       CK(cudaGetLastError());
       rc = from_device(c, dst[f], c->stage, 2 * (size_t)c->n * c->nr * sizeof(double), where);
     } else {
@@ -543,10 +601,11 @@ int chns_get_state(chns_ctx* c, double* w, double* c1, double* c2, int where) {
   return CHNS_OK;
 }
 
-int chns_state64_from_f32(chns_ctx* c, int f) {
+int chns_statelo_reset(chns_ctx* c, int f) {
   if (!c->st64) return CHNS_OK;
   const size_t ncx = (size_t)c->n * c->nr;
-  k_widen_state<<<1024, 256, 0, c->stream>>>((const float2*)c->state[f], (double2*)c->state64[f], ncx, c->k0, f);
+  CK(cudaMemsetAsync(c->statelo[f], 0, ncx * sizeof(float2), c->stream));
+  k_lo_k0<<<1, 1, 0, c->stream>>>((const float2*)c->state[f], (float2*)c->statelo[f], c->k0, f);
   CK(cudaGetLastError());
   return CHNS_OK;
 }
@@ -575,7 +634,7 @@ int chns_phase_from_realdbl(chns_ctx* c, int f) {
     k_k0_set<<<1, 1, 0, c->stream>>>(c->k0, c->stage, 1 + f);
   }
   CK(cudaGetLastError());
-  return chns_state64_from_f32(c, 1 + f);
+  return chns_statelo_reset(c, 1 + f);
 }
 
 int chns_set_phase_real(chns_ctx* c, const double* p1, const double* p2, int where) {
@@ -584,7 +643,7 @@ int chns_set_phase_real(chns_ctx* c, const double* p1, const double* p2, int whe
   const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
   CK(cudaMemsetAsync(c->state[0], 0, bytes, c->stream));  // init.c:78-87
   if (c->f32) CK(cudaMemsetAsync(c->k0, 0, 2 * sizeof(double), c->stream));
-  if (c->st64) CK(cudaMemsetAsync(c->state64[0], 0, 2 * bytes, c->stream));
+  if (c->st64) CK(cudaMemsetAsync(c->statelo[0], 0, bytes, c->stream));
   const double* src[2] = {p1, p2};
   for (int f = 0; f < c->p.model; f++) {
     const size_t nn = (size_t)c->n * c->n;
@@ -622,7 +681,7 @@ int chns_rhs(chns_ctx* c, double* nw, double* nc1, double* nc2, int where) {
   // a copy of the state and restore the state afterwards
   const size_t bytes = (size_t)c->n * c->nr * 2 * c->rsz;
   void* keep[3] = {nullptr, nullptr, nullptr};
-  void* keep64[3] = {nullptr, nullptr, nullptr};
+  void* keeplo[3] = {nullptr, nullptr, nullptr};
   double k0keep[12];
   int rc = CHNS_OK;
   for (int f = 0; f <= c->p.model && rc == CHNS_OK; f++) {
@@ -630,9 +689,8 @@ int chns_rhs(chns_ctx* c, double* nw, double* nc1, double* nc2, int where) {
     else if (cudaMemcpyAsync(keep[f], c->state[f], bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
       rc = CHNS_ERR_CUDA;
     if (rc == CHNS_OK && c->st64) {
-      if (cudaMalloc(&keep64[f], 2 * bytes) != cudaSuccess) rc = CHNS_ERR_NOMEM;
-      else if (cudaMemcpyAsync(keep64[f], c->state64[f], 2 * bytes, cudaMemcpyDeviceToDevice, c->stream) !=
-               cudaSuccess)
+      if (cudaMalloc(&keeplo[f], bytes) != cudaSuccess) rc = CHNS_ERR_NOMEM;
+      else if (cudaMemcpyAsync(keeplo[f], c->statelo[f], bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
         rc = CHNS_ERR_CUDA;
     }
   }
@@ -648,10 +706,10 @@ int chns_rhs(chns_ctx* c, double* nw, double* nc1, double* nc2, int where) {
       cudaStreamSynchronize(c->stream);
       cudaFree(keep[f]);
     }
-    if (keep64[f]) {
-      cudaMemcpyAsync(c->state64[f], keep64[f], 2 * bytes, cudaMemcpyDeviceToDevice, c->stream);
+    if (keeplo[f]) {
+      cudaMemcpyAsync(c->statelo[f], keeplo[f], bytes, cudaMemcpyDeviceToDevice, c->stream);
       cudaStreamSynchronize(c->stream);
-      cudaFree(keep64[f]);
+      cudaFree(keeplo[f]);
     }
   }
   if (c->f32) cudaMemcpy(c->k0, k0keep, sizeof(k0keep), cudaMemcpyHostToDevice);

@@ -110,7 +110,7 @@ int chns_init_vorticity(chns_ctx* c, int kind, double amplitude) {
     return CHNS_ERR_ARG;
   }
   if (c->f32) IK(cudaMemsetAsync(c->k0, 0, 2 * sizeof(double), c->stream));  // the mean vorticity is 0
-  if (int rc = chns_state64_from_f32(c, 0)) return rc;
+  if (int rc = chns_statelo_reset(c, 0)) return rc;
   IK(cudaGetLastError());
   return chns_synchronize(c);
 }

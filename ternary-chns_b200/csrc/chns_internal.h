@@ -13,9 +13,10 @@ extern "C" int chns_realdbl_to_realbuf(chns_ctx* c);
 extern "C" int chns_phase_from_realdbl(chns_ctx* c, int f);
 // real-space field f of the state (truncated first if asked) into c->realdbl
 extern "C" int chns_field_to_realdbl(chns_ctx* c, int f, int truncate);
-// CHNS_FP32_STATE64: the double state of field f from its float copy (k = 0 from
-// the double k = 0 modes), after anything but a step has written the float copy
-extern "C" int chns_state64_from_f32(chns_ctx* c, int f);
+// CHNS_FP32_STATE64: the low part of field f after anything but a step or
+// chns_set_state has written its float part (zero, and at k = 0 the rest of the
+// double k = 0 mode)
+extern "C" int chns_statelo_reset(chns_ctx* c, int f);
 
 namespace chns {
 // intermediate buffers of a step: G slots (rows 0..jt) and H slots (rows
@@ -52,14 +53,13 @@ struct chns_ctx {
   chns_params p;
   int n, nr, jt;
   bool f32;
-  bool st64;   // FP32 context with the state in double (CHNS_FP32_STATE64)
+  bool st64;   // FP32 context with a double-float state (CHNS_FP32_STATE64)
   size_t rsz;  // bytes per real scalar (4 or 8)
   cudaStream_t stream;
   bool own_stream;
   // device memory
   void* state[3];
-  void* state64[3]; // CHNS_FP32_STATE64: the state in double (S layout); state[] holds its float rounding
-  void* coef64;     // CHNS_FP32_STATE64: the ETD coefficient tables in double
+  void* statelo[3]; // CHNS_FP32_STATE64: the low float of the state (S layout): state = state[] + statelo[]
   void* saved[3];
   void* nstar[3];   // when set, stage 2 also stores N(u*) there (adjoint recording)
   void* nw;

@@ -55,8 +55,8 @@ template <class R> struct Par {
   R force_hat;             // its spectral amplitude, added to N_w at (0, force_j)
   double k0coef[6];        // ETD coefficients at k = 0 (double)
   const int* mrow;         // [n/2+1] largest |m| kept by the truncation per row (-1: none)
-  const R* coef;           // [6][n/2+1][n/2+1] ETD coefficients at (row, |m|)
-  const double* coef64;    // the same in double (FP32 contexts with a double state), else null
+  const R* coef;           // [6][n/2+1][n/2+1] ETD coefficients at (row, |m|); with a
+                           // double-float state, slots 0 and 3 hold e - 1 (expm1) instead of e
   const cx<R>* tw;         // tw[q] = exp(-2 pi i q / n)
   double* k0;              // FP32 only: k = 0 modes in double [w, c1, c2, sw, s1, s2] x (re, im)
 };
@@ -72,7 +72,7 @@ template <class R> struct Bufs {
   cx<R>* x1;
   cx<R>* x2;
   cx<R>* nw;
-  cxd* m[3];   // FP32 contexts with a double state: w, c1, c2 in double (else null)
+  cx<R>* lo[3];  // FP32 contexts with a double-float state: low parts of w, c1, c2 (else null)
   cx<R>* g[NG];
   cx<R>* h[NH];
 };
@@ -597,26 +597,37 @@ __device__ __forceinline__ void etd_k0(double* st, double* sv, double nx, double
   }
 }
 
-// ETD update of one mode of an FP32 context whose state is kept in double:
-// u (read from and written back to u64[idx]) and the update in double with the
-// double coefficients cf[0], cf[cs], cf[2 cs] (e, z1, z2); N and the saved N
-// stay float.  Returns the float rounding of the new u for the float copy.
-template <int STAGE, class R>
-__device__ __forceinline__ cx<R> etd64(cxd* __restrict__ u64, size_t idx, bool live, cx<R> nl, cx<R>* saved,
-                                       const double* __restrict__ cf, size_t cs) {
-  const cxd u = live ? u64[idx] : mk<double>(0.0, 0.0);
-  cxd r;
+// ETD update of one mode of an FP32 context whose state is a double-float pair
+// u = hi + lo[idx] (hi the float state the right-hand side reads, lo the rest):
+// the update runs in double, as u + (u (e - 1) + N z1) in stage 1 (em1 = e - 1
+// keeps the decay of the slow modes that a float e = 1 - O(1e-9) would lose) and
+// u + (N - saved) z2 in stage 2; N and the saved N are float.  The new u is split
+// again: its float rounding is returned, the remainder stored in lo[idx].
+template <int STAGE>
+__device__ __forceinline__ cxf etd_hilo(cxf hi, cxf* __restrict__ lo, size_t idx, bool live, cxf nl, cxf* saved,
+                                        float em1, float z1, float z2) {
+  const cxf l = live ? lo[idx] : mk<float>(0.f, 0.f);
+  const double ux = (double)hi.x + (double)l.x, uy = (double)hi.y + (double)l.y;
+  double rx, ry;
   if (STAGE == 1) {
     *saved = nl;
-    const double e = cf[0], z1 = cf[cs];
-    r = mk<double>(u.x * e + (double)nl.x * z1, u.y * e + (double)nl.y * z1);
+    rx = ux + (ux * (double)em1 + (double)nl.x * (double)z1);
+    ry = uy + (uy * (double)em1 + (double)nl.y * (double)z1);
   } else {
-    const cx<R> s = *saved;
-    const double z2 = cf[2 * cs];
-    r = mk<double>(u.x + ((double)nl.x - (double)s.x) * z2, u.y + ((double)nl.y - (double)s.y) * z2);
+    const cxf s = *saved;
+    rx = ux + ((double)nl.x - (double)s.x) * (double)z2;
+    ry = uy + ((double)nl.y - (double)s.y) * (double)z2;
   }
-  if (live) u64[idx] = r;
-  return mk<R>((R)r.x, (R)r.y);
+  const cxf h = mk<float>((float)rx, (float)ry);
+  if (live) lo[idx] = mk<float>((float)(rx - (double)h.x), (float)(ry - (double)h.y));
+  return h;
+}
+
+// the same split of a double k = 0 mode (kept in double by FP32 contexts)
+__device__ __forceinline__ cxf split_k0(const double* st, cxf* lo) {
+  const cxf h = mk<float>((float)st[0], (float)st[1]);
+  lo[0] = mk<float>((float)(st[0] - (double)h.x), (float)(st[1] - (double)h.y));
+  return h;
 }
 
 // ---------------------------------------------------------------------------
@@ -627,7 +638,11 @@ __device__ __forceinline__ cx<R> etd64(cxd* __restrict__ u64, size_t idx, bool l
 // ternary: chem_potential.c:319-320 (F[mu^F]), surface_tension.c:116-137,
 //          nonlin.c:300-377, etd2rk.c:117-130 / 191-206
 // ---------------------------------------------------------------------------
-// S64: FP32 context whose state is kept in double (B.m, P.coef64)
+// S64: FP32 context with a double-float state (B.lo; e - 1 in the e slots of
+// P.coef).  Only the modes inside the truncation disc carry a low part: the
+// modes outside it never reach a right-hand side (every product's inputs are
+// truncated), so their float rounding is not amplified; they are updated in
+// float with their low part left at zero.
 template <int N, class R, int GPC, int MODEL, int STAGE, bool S64>
 __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
@@ -661,7 +676,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
     cx<R>* cst = fld == 0 ? B.c1 : B.c2;
     cx<R>* csv = fld == 0 ? B.s1 : B.s2;
     cx<R>* cx_out = fld == 0 ? B.x1 : B.x2;
-    cxd* c64 = B.m[1 + fld];
+    cx<R>* clo = B.lo[1 + fld];
     // F[f(c)] (binary) or F[mu^F_i] (ternary)
     if (MODEL == MODEL_BINARY) load_row<N>(f, B.h[HF], row, live, t);
     else load_row_pair<N>(f, B.h[HF], row, fld, live, t);
@@ -712,20 +727,20 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
       const size_t idx = (size_t)rowc * N + t + NT * m;
       cx<R> sv;
       if (STAGE == 2) sv = live ? csv[idx] : czero<R>();
-      if (S64) {
-        c[m] = etd64<STAGE>(c64, idx, live, nl, &sv, P.coef64 + (size_t)rowc * NR + 3 * cstride + am, cstride);
-      } else {
-        const R e = cf[3 * cstride + am], z1 = cf[4 * cstride + am], z2 = cf[5 * cstride + am];
-        c[m] = etd<STAGE>(c[m], nl, &sv, e, z1, z2);
+      const R e = cf[3 * cstride + am], z1 = cf[4 * cstride + am], z2 = cf[5 * cstride + am];
+      if constexpr (S64) {
+        if (am <= mlim) c[m] = etd_hilo<STAGE>(c[m], clo, idx, live, nl, &sv, e, z1, z2);
+        else c[m] = etd<STAGE>(c[m], nl, &sv, (R)1 + e, z1, z2);
       }
+      else c[m] = etd<STAGE>(c[m], nl, &sv, e, z1, z2);
       if (STAGE == 1 && live) csv[idx] = sv;
       if (STAGE == 2 && cx_out && live) cx_out[idx] = nl;
       if (F32 && row == 0 && t == 0 && m == 0) {
         double* st = P.k0 + 2 * (1 + fld);
         double* sd = P.k0 + 2 * (4 + fld);
         etd_k0<STAGE>(st, sd, (double)nl.x, (double)nl.y, P.k0coef, 3);
-        c[m] = mk<R>((R)st[0], (R)st[1]);
-        if (S64) c64[0] = mk<double>(st[0], st[1]);
+        if constexpr (S64) c[m] = split_k0(st, clo);
+        else c[m] = mk<R>((R)st[0], (R)st[1]);
       }
     }
     store_row<N>(c, cst, row, live, t);
@@ -751,6 +766,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
   const int row = blockIdx.x * GPC + g;
   const bool live = row < NR;
   const int rowc = live ? row : 0;
+  const int mlim = (live && row <= P.jt) ? P.mrow[row] : -1;  // truncation disc of this row (S64)
   const R ky = (R)(P.fy * (double)row);
   const R* cf = P.coef + (size_t)rowc * NR;
   const size_t cstride = (size_t)NR * NR;
@@ -778,7 +794,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
     for (int m = 0; m < 16; m++) a[m] = mk<R>(a[m].x * (R)(-1), a[m].y * (R)(-1));
   }
   if (P.force_j >= 0 && row == P.force_j && t == 0) a[0].x = radd(a[0].x, P.force_hat);
-  if (!S64) load_row<N>(b, B.w, row, live, t);  // a double state is read by the update itself
+  load_row<N>(b, B.w, row, live, t);
 #pragma unroll
   for (int m = 0; m < 16; m++) {
     const int am = amask<N>(t, m);
@@ -786,17 +802,17 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
     cx<R> sv;
     if (STAGE == 2) sv = live ? B.sw[idx] : czero<R>();
     if (STAGE == 2 && B.xw && live) B.xw[idx] = a[m];
-    if (S64) {
-      b[m] = etd64<STAGE>(B.m[0], idx, live, a[m], &sv, P.coef64 + (size_t)rowc * NR + am, cstride);
-    } else {
-      const R e = cf[0 * cstride + am], z1 = cf[1 * cstride + am], z2 = cf[2 * cstride + am];
-      b[m] = etd<STAGE>(b[m], a[m], &sv, e, z1, z2);
+    const R e = cf[0 * cstride + am], z1 = cf[1 * cstride + am], z2 = cf[2 * cstride + am];
+    if constexpr (S64) {
+      if (am <= mlim) b[m] = etd_hilo<STAGE>(b[m], B.lo[0], idx, live, a[m], &sv, e, z1, z2);
+      else b[m] = etd<STAGE>(b[m], a[m], &sv, (R)1 + e, z1, z2);
     }
+    else b[m] = etd<STAGE>(b[m], a[m], &sv, e, z1, z2);
     if (STAGE == 1 && live) B.sw[idx] = sv;
     if (F32 && row == 0 && t == 0 && m == 0) {
       etd_k0<STAGE>(P.k0 + 0, P.k0 + 6, (double)a[m].x, (double)a[m].y, P.k0coef, 0);
-      b[m] = mk<R>((R)P.k0[0], (R)P.k0[1]);
-      if (S64) B.m[0][0] = mk<double>(P.k0[0], P.k0[1]);
+      if constexpr (S64) b[m] = split_k0(P.k0, B.lo[0]);
+      else b[m] = mk<R>((R)P.k0[0], (R)P.k0[1]);
     }
   }
   store_row<N>(b, B.w, row, live, t);

@@ -63,7 +63,6 @@ template <class R> Par<R> make_par(const chns_ctx* c) {
   for (int k = 0; k < 6; k++) P.k0coef[k] = c->k0coef[k];
   P.mrow = c->mrow;
   P.coef = (const R*)c->coef;
-  P.coef64 = c->st64 ? (const double*)c->coef64 : nullptr;
   P.tw = (const cx<R>*)c->tw;
   P.k0 = c->k0;
   return P;
@@ -81,7 +80,7 @@ template <class R> Bufs<R> make_bufs(const chns_ctx* c) {
   B.x1 = (cx<R>*)c->nstar[1];
   B.x2 = (cx<R>*)c->nstar[2];
   B.nw = (cx<R>*)c->nw;
-  for (int f = 0; f < 3; f++) B.m[f] = c->st64 ? (cxd*)c->state64[f] : nullptr;
+  for (int f = 0; f < 3; f++) B.lo[f] = c->st64 ? (cx<R>*)c->statelo[f] : nullptr;
   for (int k = 0; k < NG; k++) B.g[k] = (cx<R>*)c->g[k];
   for (int k = 0; k < NH; k++) B.h[k] = (cx<R>*)c->h[k];
   return B;
@@ -113,7 +112,7 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   const int rows_all = S::grid_rows(N / 2 + 1);
   const int pairs = S::grid_rows(N / 2);
   int launches = 0;
-  // FP32 contexts with a double state run the P3 / P5 variants that update it
+  // FP32 contexts with a double-float state run the P3 / P5 variants that update it
   constexpr bool F32 = sizeof(R) == 4;
   const bool s64 = F32 && c->st64;
 
