@@ -82,7 +82,7 @@ DT_DEFAULT = 2e-6
 PREC_NOTE = {
     1: "FP32 transforms and point-wise work; ETD coefficients from FP64; k = 0 modes in FP64; FP32 state",
     2: "CHNS_FP32_STATE64: the FP32 right-hand side; w and c carried as float pairs (hi + lo) inside the "
-       "truncation disc, the ETD update in FP64 (e - 1 from expm1); k = 0 modes in FP64",
+       "truncation disc, the ETD update in float-float arithmetic (e - 1 from expm1); k = 0 modes in FP64",
 }
 
 

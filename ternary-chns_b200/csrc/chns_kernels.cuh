@@ -597,29 +597,52 @@ __device__ __forceinline__ void etd_k0(double* st, double* sv, double nx, double
   }
 }
 
-// ETD update of one mode of an FP32 context whose state is a double-float pair
-// u = hi + lo[idx] (hi the float state the right-hand side reads, lo the rest):
-// the update runs in double, as u + (u (e - 1) + N z1) in stage 1 (em1 = e - 1
-// keeps the decay of the slow modes that a float e = 1 - O(1e-9) would lose) and
-// u + (N - saved) z2 in stage 2; N and the saved N are float.  The new u is split
-// again: its float rounding is returned, the remainder stored in lo[idx].
+// s + e = a + b exactly (Knuth's TwoSum, round to nearest)
+__device__ __forceinline__ float two_sum(float a, float b, float& e) {
+  const float s = __fadd_rn(a, b);
+  const float bp = __fsub_rn(s, a);
+  const float ap = __fsub_rn(s, bp);
+  e = __fadd_rn(__fsub_rn(a, ap), __fsub_rn(b, bp));
+  return s;
+}
+
+// One component of the ETD update of a float pair u = hi + lo, in float-float
+// arithmetic (error-free sums and an FMA-exact product, no double):
+// stage 1  u + (u (e - 1) + N z1)   (em1 = e - 1 keeps the decay of the slow modes
+//                                    that a float e = 1 - O(1e-9) would lose)
+// stage 2  u + (N - saved) z2       (a correction, small against u)
+// Returns the new hi; the new lo in lo_out.
 template <int STAGE>
-__device__ __forceinline__ cxf etd_hilo(cxf hi, cxf* __restrict__ lo, size_t idx, bool live, cxf nl, cxf* saved,
-                                        float em1, float z1, float z2) {
-  const cxf l = live ? lo[idx] : mk<float>(0.f, 0.f);
-  const double ux = (double)hi.x + (double)l.x, uy = (double)hi.y + (double)l.y;
-  double rx, ry;
+__device__ __forceinline__ float etd_ff1(float hi, float lo, float n, float sv, float em1, float z1, float z2,
+                                         float& lo_out) {
+  float dh, de = 0.f;
   if (STAGE == 1) {
-    *saved = nl;
-    rx = ux + (ux * (double)em1 + (double)nl.x * (double)z1);
-    ry = uy + (uy * (double)em1 + (double)nl.y * (double)z1);
+    const float p = __fmul_rn(hi, em1);
+    const float pe = __fmaf_rn(hi, em1, -p);  // hi em1 = p + pe exactly
+    const float q = __fmaf_rn(lo, em1, __fmaf_rn(n, z1, pe));
+    dh = two_sum(p, q, de);
   } else {
-    const cxf s = *saved;
-    rx = ux + ((double)nl.x - (double)s.x) * (double)z2;
-    ry = uy + ((double)nl.y - (double)s.y) * (double)z2;
+    dh = __fmul_rn(__fsub_rn(n, sv), z2);
   }
-  const cxf h = mk<float>((float)rx, (float)ry);
-  if (live) lo[idx] = mk<float>((float)(rx - (double)h.x), (float)(ry - (double)h.y));
+  float se, e2;
+  const float sh = two_sum(hi, dh, se);
+  const float h = two_sum(sh, __fadd_rn(se, __fadd_rn(lo, de)), e2);
+  lo_out = e2;
+  return h;
+}
+
+// ETD update of one mode of an FP32 context whose state is a float pair
+// hi + lo (hi the float state the right-hand side reads; l the low part read by
+// the caller): returns the new hi, the new low part in lo_out.  N and the saved N
+// are float, as the right-hand side.
+template <int STAGE>
+__device__ __forceinline__ cxf etd_hilo(cxf hi, cxf l, cxf& lo_out, cxf nl, cxf* saved, float em1, float z1,
+                                        float z2) {
+  const cxf s = STAGE == 2 ? *saved : nl;
+  if (STAGE == 1) *saved = nl;
+  cxf h;
+  h.x = etd_ff1<STAGE>(hi.x, l.x, nl.x, s.x, em1, z1, z2, lo_out.x);
+  h.y = etd_ff1<STAGE>(hi.y, l.y, nl.y, s.y, em1, z1, z2, lo_out.y);
   return h;
 }
 
@@ -659,7 +682,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
   const bool do_mu = (int)(blockIdx.x * GPC) <= P.jt;  // CTA-uniform
   const int mlim = (live && row <= P.jt) ? P.mrow[row] : -1;
   const R ky = (R)(P.fy * (double)row);
-  const R* cf = P.coef + (size_t)rowc * NR;
+  const R* __restrict__ cf = P.coef + (size_t)rowc * NR;
   const size_t cstride = (size_t)NR * NR;
   auto kxm = [&](int m) -> R { return (R)(P.fx * (double)sidx<N>(t + NT * m)); };
 
@@ -676,7 +699,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
     cx<R>* cst = fld == 0 ? B.c1 : B.c2;
     cx<R>* csv = fld == 0 ? B.s1 : B.s2;
     cx<R>* cx_out = fld == 0 ? B.x1 : B.x2;
-    cx<R>* clo = B.lo[1 + fld];
+    cx<R>* __restrict__ clo = B.lo[1 + fld];
     // F[f(c)] (binary) or F[mu^F_i] (ternary)
     if (MODEL == MODEL_BINARY) load_row<N>(f, B.h[HF], row, live, t);
     else load_row_pair<N>(f, B.h[HF], row, fld, live, t);
@@ -729,8 +752,13 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
       if (STAGE == 2) sv = live ? csv[idx] : czero<R>();
       const R e = cf[3 * cstride + am], z1 = cf[4 * cstride + am], z2 = cf[5 * cstride + am];
       if constexpr (S64) {
-        if (am <= mlim) c[m] = etd_hilo<STAGE>(c[m], clo, idx, live, nl, &sv, e, z1, z2);
-        else c[m] = etd<STAGE>(c[m], nl, &sv, (R)1 + e, z1, z2);
+        if (am <= mlim) {
+          cxf lnew;
+          c[m] = etd_hilo<STAGE>(c[m], clo[idx], lnew, nl, &sv, e, z1, z2);
+          clo[idx] = lnew;  // am <= mlim only on live rows
+        } else {
+          c[m] = etd<STAGE>(c[m], nl, &sv, (R)1 + e, z1, z2);
+        }
       }
       else c[m] = etd<STAGE>(c[m], nl, &sv, e, z1, z2);
       if (STAGE == 1 && live) csv[idx] = sv;
@@ -768,7 +796,8 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
   const int rowc = live ? row : 0;
   const int mlim = (live && row <= P.jt) ? P.mrow[row] : -1;  // truncation disc of this row (S64)
   const R ky = (R)(P.fy * (double)row);
-  const R* cf = P.coef + (size_t)rowc * NR;
+  const R* __restrict__ cf = P.coef + (size_t)rowc * NR;
+  cx<R>* __restrict__ wlo = B.lo[0];
   const size_t cstride = (size_t)NR * NR;
   auto kxm = [&](int m) -> R { return (R)(P.fx * (double)sidx<N>(t + NT * m)); };
 
@@ -804,8 +833,13 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
     if (STAGE == 2 && B.xw && live) B.xw[idx] = a[m];
     const R e = cf[0 * cstride + am], z1 = cf[1 * cstride + am], z2 = cf[2 * cstride + am];
     if constexpr (S64) {
-      if (am <= mlim) b[m] = etd_hilo<STAGE>(b[m], B.lo[0], idx, live, a[m], &sv, e, z1, z2);
-      else b[m] = etd<STAGE>(b[m], a[m], &sv, (R)1 + e, z1, z2);
+      if (am <= mlim) {
+        cxf lnew;
+        b[m] = etd_hilo<STAGE>(b[m], wlo[idx], lnew, a[m], &sv, e, z1, z2);
+        wlo[idx] = lnew;  // am <= mlim only on live rows
+      } else {
+        b[m] = etd<STAGE>(b[m], a[m], &sv, (R)1 + e, z1, z2);
+      }
     }
     else b[m] = etd<STAGE>(b[m], a[m], &sv, e, z1, z2);
     if (STAGE == 1 && live) B.sw[idx] = sv;

@@ -1,5 +1,5 @@
 """CHNS_FP32_STATE64: FP32 right-hand side, the state carried as a float pair
-hi + lo (48 significant bits) and the ETD update done in double.
+hi + lo (48 significant bits) and the ETD update done in float-float arithmetic.
 
 The state given to chns_set_state comes back to 2^-48 per element inside the
 truncation disc (the modes that reach a right-hand side) and 2^-24 outside; the low part
