@@ -154,17 +154,24 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def read_profile_traffic(kernel: str, n: int):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary
-    profiles/<kernel>_<n>_fp32.md (a line 'dram_bytes_per_launch: <int>')."""
+def read_profile_value(kernel: str, n: int, key: str):
+    """A figure of the committed ncu summary profiles/<kernel>_<n>_fp32.md (a line
+    '<key>: <number>'), or None."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_{n}_fp32.md")
     try:
         for line in open(path):
-            if line.strip().startswith("dram_bytes_per_launch:"):
-                return int(line.split(":", 1)[1].strip())
-    except OSError:
+            if line.strip().startswith(key + ":"):
+                v = float(line.split(":", 1)[1].strip())
+                return int(v) if v.is_integer() else v
+    except (OSError, ValueError):
         pass
     return None
+
+
+def read_profile_traffic(kernel: str, n: int):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    profiles/<kernel>_<n>_fp32.md (a line 'dram_bytes_per_launch: <int>')."""
+    return read_profile_value(kernel, n, "dram_bytes_per_launch")
 
 
 def init_leg(C, n: int) -> dict:
@@ -542,7 +549,12 @@ def run_gpu(args):
             ach = kb[dom[0]] / (dom[1] / 1e3) / 1e9
             roof = {"kernel": dom[0], "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "peak_source": src,
                     "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": read_profile_traffic(dom[0], n),
-                    "algorithmic_bytes_per_launch": kb[dom[0]], "ms_per_launch": round(dom[1], 4)}
+                    "algorithmic_bytes_per_launch": kb[dom[0]], "ms_per_launch": round(dom[1], 4),
+                    "issue_active_pct": read_profile_value(dom[0], n, "issue_active_pct"),
+                    "warps_active_pct": read_profile_value(dom[0], n, "warps_active_pct"),
+                    "note": "no stage is a contraction, so the HBM roofline is the one that applies; the row "
+                            "kernels reach a fraction of it because they are latency-bound (two 256-thread CTAs "
+                            "per SM at 128 registers, barrier-synchronous transforms): see profiles/"}
         rsz = 4
         model_bytes = 120 * n * n * rsz
         out = {
