@@ -76,6 +76,7 @@ def load_library(path: str = LIB_PATH):
     L.chns_ifft.argtypes = [vp, dp, dp, ip]
     L.chns_diagnostics.argtypes = [vp, dp, dp]
     L.chns_launches_per_step.argtypes = [vp]
+    L.chns_tma_tiles.argtypes = [vp]
     L.chns_profile_step.argtypes = [vp, ip, vp, vp, ip]
     L.chns_profile_step.restype = ip
     L.chns_adjoint.argtypes = [vp, ip, ip, vp, vp, vp, vp, vp, ip]
@@ -338,6 +339,10 @@ class Context:
 
     def launches_per_step(self) -> int:
         return self.L.chns_launches_per_step(self._h)
+
+    def tma_tiles(self) -> bool:
+        """True when the step's row kernels load their tiles with TMA."""
+        return bool(self.L.chns_tma_tiles(self._h))
 
 
 class Member(Context):

@@ -11,7 +11,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <new>
 #include <vector>
+
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 
 #include "chns_internal.h"
 #include "chns_kernels.cuh"
@@ -170,18 +173,67 @@ void free_all(chns_ctx* c) {
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   void* ptrs[] = {c->state[0], c->state[1], c->state[2], c->saved[0], c->saved[1], c->saved[2], c->nw,
                   c->coef, c->mrow, c->tw, c->k0, c->stage, c->realbuf, c->realdbl, c->red, c->redscratch,
-                  c->statelo[0], c->statelo[1], c->statelo[2]};
+                  c->statelo[0], c->statelo[1], c->statelo[2], c->tma_err};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (void* q : c->g)
     if (q) cudaFree(q);
   for (void* q : c->h)
     if (q) cudaFree(q);
+  delete static_cast<chns::TmaG*>(c->tmag);
   if (c->hostpin) cudaFreeHost(c->hostpin);
   for (int k = 0; k < c->npinned; k++) cudaHostUnregister(c->pinned[k]);
   c->npinned = 0;
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   free(c);
+}
+
+// Tensor maps of the G slots for the TMA tiles of the FP32 row kernels (left
+// unused, with cp.async tiles instead, when the driver's encoder is unavailable
+// or refuses a map).  Each G slot holds rows 0..jt; a tile is nbox boxes of
+// {2 complex, boxr rows}.
+int build_tma(chns_ctx* c) {
+  chns::TmaG* T = new (std::nothrow) chns::TmaG();
+  if (!T) return CHNS_ERR_NOMEM;
+  c->tmag = T;
+  T->use = 0;
+  T->err = c->tma_err;
+  const int rows = c->jt + 1;
+  T->boxr = rows >= 256 ? 256 : (rows + 7) / 8 * 8;
+  T->nbox = (rows + T->boxr - 1) / T->boxr;
+  if (!c->f32) return CHNS_OK;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn) {
+    cudaGetLastError();
+    return CHNS_OK;
+  }
+  const auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  for (int k = 0; k < chns::NG; k++)
+    for (int v = 0; v < 2; v++) {
+      const cuuint64_t width = v == 0 ? 2 * (cuuint64_t)c->n : (cuuint64_t)c->n;  // complex per row
+      const cuuint64_t dims[2] = {width, (cuuint64_t)rows};
+      const cuuint64_t strides[1] = {width * 8};
+      const cuuint32_t box[2] = {2, (cuuint32_t)T->boxr};
+      const cuuint32_t estr[2] = {1, 1};
+      if (encode(&T->map[2 * k + v], CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, c->g[k], dims, strides, box, estr,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return CHNS_OK;
+    }
+  T->use = 1;
+  return CHNS_OK;
+}
+
+// CHNS_ERR_TIMEOUT when a row kernel flagged a timed-out tile wait (then clears it)
+int tma_status(chns_ctx* c) {
+  unsigned int h = 0;
+  CK(cudaMemcpyAsync(&h, c->tma_err, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (!h) return CHNS_OK;
+  CK(cudaMemsetAsync(c->tma_err, 0, sizeof(h), c->stream));
+  return CHNS_ERR_TIMEOUT;
 }
 
 int dmalloc(void** p, size_t bytes) {
@@ -399,6 +451,8 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
   if (rc == CHNS_OK) rc = dmalloc((void**)&c->realdbl, (size_t)n * n * sizeof(double));
   if (rc == CHNS_OK) rc = dmalloc((void**)&c->red, 16 * sizeof(double));
   if (rc == CHNS_OK) rc = dmalloc(&c->redscratch, (size_t)(n / 2 + 1) * 8 * sizeof(double));
+  if (rc == CHNS_OK) rc = dmalloc((void**)&c->tma_err, sizeof(unsigned int));
+  if (rc == CHNS_OK) rc = build_tma(c);
   if (rc != CHNS_OK) {
     free_all(c);
     return rc;
@@ -492,7 +546,7 @@ int chns_synchronize(chns_ctx* c) {
   if (!c) return CHNS_ERR_ARG;
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaGetLastError());
-  return CHNS_OK;
+  return tma_status(c);
 }
 
 // FFTW-layout double <-> S-layout double-float pair (hi = float rounding, lo =
@@ -778,7 +832,8 @@ int chns_check(chns_ctx* c) {
   unsigned int h = 0;
   CK(cudaMemcpyAsync(&h, flag, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  return h ? CHNS_ERR_NONFINITE : CHNS_OK;
+  if (h) return CHNS_ERR_NONFINITE;
+  return tma_status(c);
 }
 
 int chns_diagnostics(chns_ctx* c, double* out_fe, double* out_ke) {
@@ -811,6 +866,8 @@ int chns_diagnostics(chns_ctx* c, double* out_fe, double* out_ke) {
 }
 
 int chns_launches_per_step(const chns_ctx* c) { return c ? c->launches_per_step : 0; }
+
+int chns_tma_tiles(const chns_ctx* c) { return c && static_cast<const chns::TmaG*>(c->tmag)->use ? 1 : 0; }
 
 int chns_profile_step(chns_ctx* c, int reps, float* ms, int* kind, int maxk) {
   if (!c || reps < 1 || !ms || !kind || maxk < 1) return CHNS_ERR_ARG;

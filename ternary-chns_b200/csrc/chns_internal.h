@@ -66,6 +66,8 @@ struct chns_ctx {
   void* g[12];
   void* h[7];
   void* coef;
+  void* tmag;         // chns::TmaG (host): tensor maps of the G slots for the row kernels' TMA tiles
+  unsigned int* tma_err;  // device word the row kernels flag a timed-out tile wait in
   int* mrow;
   void* tw;
   double* k0;       // [12] k = 0 modes (FP32 contexts)

@@ -28,6 +28,8 @@
 // current transform runs.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
+
 #include "chns_fft.cuh"
 
 namespace chns {
@@ -103,7 +105,10 @@ static __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.as
 template <class R> struct RowSrc {
   const cx<R>* base;
   int stride, off;
+  int map;  // tensor map of the source (TmaG::map), -1: none
 };
+
+
 
 // Group-cooperative copy of rows 0..jt of `s` into this group's tile
 // (2 complex per row) with cp.async; the caller commits.
@@ -137,6 +142,99 @@ __device__ __forceinline__ void build_c2r_input(cx<R>* v, const cx<R>* tile, int
     if (kk == 0 || kk == N / 2) { a.y = (R)0; b.y = (R)0; }
     v[m] = cj ? mk<R>(a.x + b.y, b.x - a.y) : mk<R>(a.x - b.y, a.y + b.x);
   }
+}
+
+// ---------------------------------------------------------------------------
+// TMA tiles of the FP32 step's row kernels.  One 2D tensor map per G slot and
+// view (pair fields: rows of 2n complex; plain fields: rows of n complex) over
+// rows 0..jt, with 64-bit elements (one FP32 complex value); a tile is nbox
+// boxes of {2 elements, boxr rows}, 16 bytes a row, rows beyond jt zero-filled.
+// One thread per group issues the boxes on the group's mbarrier; every thread
+// of the group waits on it (bounded: on timeout the kernel flags *err and goes
+// on, so a broken copy ends in an error status, not a hang).
+// ---------------------------------------------------------------------------
+struct __align__(64) TmaG {
+  CUtensorMap map[2 * NG];  // [2 slot + 0]: pair view, [2 slot + 1]: plain view
+  int use;                  // maps built (FP32 contexts); 0: cp.async tiles
+  int boxr, nbox;           // rows per box, boxes per tile (nbox * boxr >= jt + 1)
+  unsigned int* err;        // bit 0: an mbarrier wait timed out
+};
+constexpr int kMbarSpins = 1 << 18;  // try_wait rounds before a tile wait gives up
+
+static __device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+static __device__ __forceinline__ void mbar_init(uint64_t* mb) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mb)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// waits for the phase of parity `par` to complete; false on timeout
+static __device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned par) {
+  unsigned ok = 0;
+  for (int k = 0; k < kMbarSpins && !ok; k++)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(mb)), "r"(par)
+        : "memory");
+  return ok != 0;
+}
+// one tile (nbox boxes) of map `map` at column x into `tile`, completing on mb
+static __device__ __forceinline__ void tma_tile(void* tile, const TmaG& T, int map, int x, uint64_t* mb) {
+  const unsigned bytes = (unsigned)(T.nbox * T.boxr * 16);
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier generic reads of the tile
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mb)), "r"(bytes)
+               : "memory");
+  for (int b = 0; b < T.nbox; b++)
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];\n" ::"r"(smem_u32(tile) + (unsigned)(b * T.boxr * 16)),
+        "l"(reinterpret_cast<uint64_t>(&T.map[map])), "r"(x), "r"(b * T.boxr), "r"(smem_u32(mb))
+        : "memory");
+}
+
+// Tile state of a row kernel: TMA (FP32 contexts with maps) or cp.async.
+template <class R> struct TileLoader {
+  bool tma;
+  uint64_t* mb;  // this group's mbarrier (TMA)
+  unsigned par;  // parity of the next phase to wait for
+};
+
+// Starts the copy of `s` into `tile` (group g, thread t of the group).
+template <int N, class R>
+__device__ __forceinline__ void tile_start(TileLoader<R>& L, const TmaG& T, cx<R>* tile, RowSrc<R> s, int jt,
+                                           bool live, int t) {
+  if (L.tma) {
+    if (t == 0 && live) tma_tile(tile, T, s.map, s.off, L.mb);
+  } else {
+    tile_issue<N>(tile, s, jt, live, t);
+    cp_async_commit();
+  }
+}
+
+// Waits for the copy in flight to `tile` (every thread of the group).
+template <class R>
+__device__ __forceinline__ void tile_wait(TileLoader<R>& L, const TmaG& T, bool live) {
+  if (L.tma) {
+    if (live && !mbar_wait(L.mb, L.par)) atomicOr(T.err, 1u);
+    L.par ^= 1u;
+  } else {
+    cp_async_wait_all();
+  }
+}
+
+// row_c2r_tiled with the row kernels' tile loader (TMA or cp.async)
+template <int N, class R>
+__device__ __forceinline__ void row_c2r_loaded(cx<R>* v, cx<R>* tile, TileLoader<R>& L, const TmaG& T,
+                                               bool has_next, RowSrc<R> next, int jt, bool live, int t, cx<R>* sh,
+                                               const Tw<R>& tw) {
+  tile_wait(L, T, live);
+  __syncthreads();
+  build_c2r_input<N>(v, tile, jt, t);
+  __syncthreads();
+  if (has_next) tile_start<N>(L, T, tile, next, jt, live, t);
+  fft<N, +1>(v, sh, t, tw);
 }
 
 // Inverse y transform of the input already in flight to `tile`; issues the
@@ -206,11 +304,39 @@ template <int N, class R, int GPC> struct RowSmem {
     tile = base + GPC * FftShape<N>::SMEM + (size_t)g * 2 * (jt + 1);
     frag = reinterpret_cast<R*>(base + GPC * FftShape<N>::SMEM + (size_t)GPC * 2 * (jt + 1)) + (size_t)g * N;
   }
-  static size_t bytes(int jt, int nfrag) {
+  static __host__ __device__ size_t bytes(int jt, int nfrag) {
     return (size_t)GPC * FftShape<N>::SMEM * sizeof(cx<R>) + (size_t)GPC * 2 * (jt + 1) * sizeof(cx<R>) +
            (size_t)nfrag * GPC * N * sizeof(R);
   }
 };
+
+// Shared-memory layout of a row kernel with a tile loader: RowSmem after the
+// twiddles (aligned to 128 bytes for TMA: the launch adds 128 bytes of slack),
+// then one mbarrier per group.  tjt: last tile row (TMA tiles are whole boxes).
+template <int N, class R, int GPC> struct LoadedRowSmem {
+  RowSmem<N, R, GPC> S;
+  uint64_t* mb;
+  __device__ __forceinline__ LoadedRowSmem(unsigned char* raw, int g, int tjt, int nfrag)
+      : S(raw, g, tjt), mb(reinterpret_cast<uint64_t*>(raw + RowSmem<N, R, GPC>::bytes(tjt, nfrag)) + g) {}
+};
+static __device__ __forceinline__ unsigned char* align128(unsigned char* p) {
+  return p + ((128u - (smem_u32(p) & 127u)) & 127u);
+}
+// TMA tiles are used when the context has tensor maps (FP32) and every group's
+// tile and box starts on 128 bytes once the layout's base is aligned: the
+// transform buffers and the tiles must be whole multiples of 128 bytes.
+template <int N, class R, int GPC>
+__device__ __forceinline__ bool tma_tiles_ok(const TmaG& T, const unsigned char* /*raw*/) {
+  if (sizeof(R) != 4 || !T.use) return false;
+  const size_t sh_bytes = (size_t)GPC * FftShape<N>::SMEM * sizeof(cx<R>);
+  const size_t box_bytes = (size_t)T.boxr * 2 * sizeof(cx<R>);
+  return sh_bytes % 128 == 0 && box_bytes % 128 == 0;
+}
+// bytes of a row kernel's shared memory after the twiddles
+template <int N, class R, int GPC> size_t loaded_row_smem_bytes(bool tma, int jt, int boxr, int nbox, int nfrag) {
+  const int tjt = tma ? nbox * boxr - 1 : jt;
+  return RowSmem<N, R, GPC>::bytes(tjt, nfrag) + (size_t)GPC * sizeof(uint64_t) + (tma ? 128 : 0);
+}
 
 // ---------------------------------------------------------------------------
 // spectral-pass helpers
@@ -375,6 +501,11 @@ template <class R> __device__ __forceinline__ void mu_ternary(const Par<R>& P, R
 // dot product of two pair-field transforms: f0 g0 + f1 g1 (e.g. ux*tux + uy*tuy)
 template <class R> __device__ __forceinline__ R dot2(cx<R> f, cx<R> g) { return radd(rmul(f.x, g.x), rmul(f.y, g.y)); }
 
+// real frags per group of the row kernels (thread-private values kept across
+// transforms in shared memory)
+template <int MODEL> constexpr int row_adv_frags() { return 1; }
+template <int MODEL> constexpr int row_force_frags() { return MODEL == MODEL_TERNARY ? 2 : 0; }
+
 // The row kernels run a fixed schedule of inverse y transforms as a loop with
 // one call site per transform direction (the unrolled transforms are long, so
 // one copy of each keeps the kernel inside the instruction cache).  Step `it`
@@ -396,24 +527,27 @@ template <int N, class R, int MODEL>
 __device__ __forceinline__ RowSrc<R> adv_src(const Bufs<R>& B, int it, int i0) {
   using Sc = AdvSchedule<MODEL>;
   if (it < Sc::PRE) {
-    if (MODEL == MODEL_BINARY) return RowSrc<R>{B.g[GCT], N, i0};
-    return RowSrc<R>{B.g[GCT], 2 * N, 2 * (i0 + it)};
+    if (MODEL == MODEL_BINARY) return RowSrc<R>{B.g[GCT], N, i0, 2 * GCT + 1};
+    return RowSrc<R>{B.g[GCT], 2 * N, 2 * (i0 + it), 2 * GCT};
   }
   const int q = it - Sc::PRE, h = q / Sc::PER, r = q % Sc::PER;
   const int slot = r == 0 ? GUV : (r == 1 ? GW : (r == 2 ? GD1 : GD2));
-  return RowSrc<R>{B.g[slot], 2 * N, 2 * (i0 + h)};
+  return RowSrc<R>{B.g[slot], 2 * N, 2 * (i0 + h), 2 * slot};
 }
 
 template <int N, class R, int GPC, int MODEL>
-__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par<R> P) {
+__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par<R> P, const __grid_constant__ TmaG T) {
   using Sc = AdvSchedule<MODEL>;
   constexpr int NT = N / 16;
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
   unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  const bool tma = tma_tiles_ok<N, R, GPC>(T, smem_raw);  // CTA-uniform
+  if (tma) smem_raw = align128(smem_raw);
   const int jt = P.jt;
-  const RowSmem<N, R, GPC> S(smem_raw, g, jt);
+  const LoadedRowSmem<N, R, GPC> LS(smem_raw, g, tma ? T.nbox * T.boxr - 1 : jt, row_adv_frags<MODEL>());
+  const RowSmem<N, R, GPC>& S = LS.S;
   const int pair = blockIdx.x * GPC + g;
   const bool live = pair < N / 2;
   const int i0 = 2 * pair;
@@ -421,12 +555,15 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par
   cx<R> z[16], v[16];
   R a[16];
 
-  tile_issue<N>(S.tile, adv_src<N, R, MODEL>(B, 0, i0), jt, live, t);
-  cp_async_commit();
+  TileLoader<R> TL{tma, LS.mb, 0u};
+  if (tma && t == 0) mbar_init(TL.mb);
+  __syncthreads();
+  tile_start<N>(TL, T, S.tile, adv_src<N, R, MODEL>(B, 0, i0), jt, live, t);
 #pragma unroll 1
   for (int it = 0; it < Sc::STEPS; it++) {
     const bool more = it + 1 < Sc::STEPS;
-    row_c2r_tiled<N>(v, S.tile, more, adv_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t, S.sh, TW);
+    row_c2r_loaded<N>(v, S.tile, TL, T, more, adv_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t, S.sh,
+                      TW);
     cx<R>* dst = nullptr;
     int stride = 0, off = 0;
     if (it < Sc::PRE) {
@@ -486,7 +623,6 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par
   }
 }
 
-template <int MODEL> constexpr int row_adv_frags() { return 1; }
 
 // ---------------------------------------------------------------------------
 // P4: surface-tension force mu grad c on x-row pairs (G -> H)
@@ -498,35 +634,41 @@ template <int MODEL> constexpr int row_adv_frags() { return 1; }
 template <int N, class R, int MODEL>
 __device__ __forceinline__ RowSrc<R> force_src(const Bufs<R>& B, int it, int i0) {
   if (MODEL == MODEL_BINARY) {
-    if (it == 0) return RowSrc<R>{B.g[GMU], N, i0};
-    return RowSrc<R>{B.g[GD1], 2 * N, 2 * (i0 + it - 1)};
+    if (it == 0) return RowSrc<R>{B.g[GMU], N, i0, 2 * GMU + 1};
+    return RowSrc<R>{B.g[GD1], 2 * N, 2 * (i0 + it - 1), 2 * GD1};
   }
   const int h = it / 3, r = it % 3;
-  return RowSrc<R>{B.g[r == 0 ? GMU : (r == 1 ? GD1 : GD2)], 2 * N, 2 * (i0 + h)};
+  const int slot = r == 0 ? GMU : (r == 1 ? GD1 : GD2);
+  return RowSrc<R>{B.g[slot], 2 * N, 2 * (i0 + h), 2 * slot};
 }
 
 template <int N, class R, int GPC, int MODEL>
-__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const Par<R> P) {
+__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const Par<R> P, const __grid_constant__ TmaG T) {
   constexpr int NT = N / 16;
   constexpr int STEPS = MODEL == MODEL_BINARY ? 3 : 6;
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
   unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  const bool tma = tma_tiles_ok<N, R, GPC>(T, smem_raw);  // CTA-uniform
+  if (tma) smem_raw = align128(smem_raw);
   const int jt = P.jt;
-  const RowSmem<N, R, GPC> S(smem_raw, g, jt);
+  const LoadedRowSmem<N, R, GPC> LS(smem_raw, g, tma ? T.nbox * T.boxr - 1 : jt, row_force_frags<MODEL>());
+  const RowSmem<N, R, GPC>& S = LS.S;
   const int pair = blockIdx.x * GPC + g;
   const bool live = pair < N / 2;
   const int i0 = 2 * pair;
   Frag<N, R> w1{S.frag}, w2{S.frag + N * GPC};
   cx<R> a[16], v[16];
-  tile_issue<N>(S.tile, force_src<N, R, MODEL>(B, 0, i0), jt, live, t);
-  cp_async_commit();
+  TileLoader<R> TL{tma, LS.mb, 0u};
+  if (tma && t == 0) mbar_init(TL.mb);
+  __syncthreads();
+  tile_start<N>(TL, T, S.tile, force_src<N, R, MODEL>(B, 0, i0), jt, live, t);
 #pragma unroll 1
   for (int it = 0; it < STEPS; it++) {
     const bool more = it + 1 < STEPS;
-    row_c2r_tiled<N>(v, S.tile, more, force_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t, S.sh,
-                     TW);
+    row_c2r_loaded<N>(v, S.tile, TL, T, more, force_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t,
+                      S.sh, TW);
     bool store = false;
     int i = i0;
     if (MODEL == MODEL_BINARY) {
@@ -569,7 +711,6 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const P
   }
 }
 
-template <int MODEL> constexpr int row_force_frags() { return MODEL == MODEL_TERNARY ? 2 : 0; }
 
 // ETD update of one mode (etd2rk.c:99,113,129-130 / 174,188,205-206).
 // STAGE 1: u <- u e + N z1, save N.  STAGE 2: u <- u + (N - saved) z2.

@@ -115,6 +115,9 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   // FP32 contexts with a double-float state run the P3 / P5 variants that update it
   constexpr bool F32 = sizeof(R) == 4;
   const bool s64 = F32 && c->st64;
+  // the row kernels' tiles come by TMA when the context has its tensor maps (FP32)
+  const TmaG& TG = *static_cast<const TmaG*>(c->tmag);
+  const bool tma = F32 && TG.use;
 
   // P1: spectral fan-out and x inverse transforms
   if (model == CHNS_MODEL_NS) {
@@ -136,19 +139,19 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   // P2: advection products (+ chemical potential)
   if (model == CHNS_MODEL_NS) {
     auto k = k_row_adv<N, R, GPC, MODEL_NS>;
-    const size_t sm = S::TW + RowSmem<N, R, GPC>::bytes(jt, row_adv_frags<MODEL_NS>());
+    const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_NS>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   } else if (model == CHNS_MODEL_BINARY) {
     auto k = k_row_adv<N, R, GPC, MODEL_BINARY>;
-    const size_t sm = S::TW + RowSmem<N, R, GPC>::bytes(jt, row_adv_frags<MODEL_BINARY>());
+    const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_BINARY>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   } else {
     auto k = k_row_adv<N, R, GPC, MODEL_TERNARY>;
-    const size_t sm = S::TW + RowSmem<N, R, GPC>::bytes(jt, row_adv_frags<MODEL_TERNARY>());
+    const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_TERNARY>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   }
   launches++;
   mark(c, KIND_ROW_ADV);
@@ -196,14 +199,14 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   // P4: surface-tension force
   if (model == CHNS_MODEL_BINARY) {
     auto k = k_row_force<N, R, GPC, MODEL_BINARY>;
-    const size_t sm = S::TW + RowSmem<N, R, GPC>::bytes(jt, row_force_frags<MODEL_BINARY>());
+    const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_force_frags<MODEL_BINARY>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   } else {
     auto k = k_row_force<N, R, GPC, MODEL_TERNARY>;
-    const size_t sm = S::TW + RowSmem<N, R, GPC>::bytes(jt, row_force_frags<MODEL_TERNARY>());
+    const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_force_frags<MODEL_TERNARY>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P);
+    k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   }
   launches++;
   mark(c, KIND_ROW_FORCE);

@@ -73,7 +73,7 @@ def test_status_strings(lib):
 
 
 def test_calls_reject_a_null_context_without_cuda(lib):
-    for fn in ("chns_step", "chns_check", "chns_synchronize", "chns_launches_per_step"):
+    for fn in ("chns_step", "chns_check", "chns_synchronize", "chns_launches_per_step", "chns_tma_tiles"):
         f = getattr(lib, fn)
         rc = f(None, 1) if fn == "chns_step" else f(None)
-        assert rc in (-1, 0) if fn == "chns_launches_per_step" else rc == -1, fn
+        assert rc in (-1, 0) if fn in ("chns_launches_per_step", "chns_tma_tiles") else rc == -1, fn

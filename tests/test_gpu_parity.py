@@ -52,6 +52,47 @@ def test_fft_vs_numpy(chns, n, prec):
         assert rel_l2(c.ifft(Z), np.fft.irfft2(Z, s=(n, n))) <= tol
 
 
+@pytest.mark.parametrize("n", [256, 1024, 4096])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_fft_vs_cufft(chns, n, prec):
+    """Cross-check of the own transforms against cuFFT (torch.fft on the same GPU)
+    in the same precision: FP64 <= 1e-13, FP32 <= 2e-6 relative L2."""
+    import torch
+
+    p = dict(model=0, nx=n, ny=n, lx=2 * math.pi, dt=1e-3, nu=0.01, precision=prec)
+    dt = torch.float64 if prec == 0 else torch.float32
+    with _ctx(chns, p) as c:
+        rng = np.random.default_rng(n + 7)
+        x = rng.standard_normal((n, n))
+        ref = torch.fft.rfft2(torch.from_numpy(x).to("cuda", dt)).cpu().numpy().astype(np.complex128)
+        tol = 1e-13 if prec == 0 else 2e-6
+        assert rel_l2(c.dfft(x), ref) <= tol
+        back = torch.fft.irfft2(torch.from_numpy(ref).to("cuda"), s=(n, n)).cpu().numpy()
+        assert rel_l2(c.ifft(ref), back) <= tol
+
+
+@pytest.mark.parametrize("n", [32, 64, 256, 512, 2048, 4096])
+def test_fp32_row_tiles_by_tma(chns, n):
+    """FP32 contexts load the row kernels' tiles with TMA (tensor maps encoded at
+    creation); no tile wait runs out over a few steps (chns_check would return
+    CHNS_ERR_TIMEOUT), and the FP32 state stays within 1e-5 of the FP64 one."""
+    rng = np.random.default_rng(n)
+    lx = 2 * math.pi
+    p = dict(model=1, nx=n, ny=n, lx=lx, dt=1e-6, nu=0.01, sigma=0.2, epsilon=2 * lx / n, coef_mode=1)
+    p["lambda"] = 0.005
+    c0 = 0.5 + 0.05 * rng.uniform(-1, 1, (n, n))
+    res = []
+    for prec in (0, 1):
+        with _ctx(chns, p, precision=prec) as c:
+            assert c.tma_tiles() == (prec == 1)
+            c.set_phase_real(c0)
+            c.step(3)
+            c.check()
+            res.append(c.get_state())
+    for a, b in zip(res[1], res[0]):
+        assert rel_l2(a, b) <= 1e-5
+
+
 @pytest.mark.parametrize("name", SMALL_CONFIGS)
 def test_rhs_matches_reference(chns, name):
     g = load_small(name)
