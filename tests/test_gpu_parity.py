@@ -71,21 +71,29 @@ def test_fft_vs_cufft(chns, n, prec):
         assert rel_l2(c.ifft(ref), back) <= tol
 
 
-@pytest.mark.parametrize("n", [32, 64, 256, 512, 2048, 4096])
-def test_fp32_row_tiles_by_tma(chns, n):
+@pytest.mark.parametrize("model,n", [(1, 32), (1, 64), (1, 256), (1, 512), (1, 2048), (1, 4096), (0, 128),
+                                     (0, 1024), (2, 128), (2, 1024)])
+def test_fp32_row_tiles_by_tma(chns, model, n):
     """FP32 contexts load the row kernels' tiles with TMA (tensor maps encoded at
     creation); no tile wait runs out over a few steps (chns_check would return
     CHNS_ERR_TIMEOUT), and the FP32 state stays within 1e-5 of the FP64 one."""
     rng = np.random.default_rng(n)
     lx = 2 * math.pi
-    p = dict(model=1, nx=n, ny=n, lx=lx, dt=1e-6, nu=0.01, sigma=0.2, epsilon=2 * lx / n, coef_mode=1)
+    p = dict(model=model, nx=n, ny=n, lx=lx, dt=1e-6, nu=0.01, sigma=0.2, epsilon=2 * lx / n, coef_mode=1,
+             sigma12=0.2, sigma13=0.3, sigma23=0.25)
     p["lambda"] = 0.005
-    c0 = 0.5 + 0.05 * rng.uniform(-1, 1, (n, n))
+    ph = [0.5 + 0.05 * rng.uniform(-1, 1, (n, n)) for _ in range(model)]
+    w = np.zeros((n, n // 2 + 1), np.complex128)
+    w[1, 2], w[3, 1] = 0.3 * n * n, 0.2 * n * n  # a few vorticity modes (ky > 0: no Hermitian pairing)
     res = []
     for prec in (0, 1):
         with _ctx(chns, p, precision=prec) as c:
             assert c.tma_tiles() == (prec == 1)
-            c.set_phase_real(c0)
+            if model:
+                c.set_phase_real(*ph)
+            st = c.get_state()
+            st[0] = w
+            c.set_state(*st)
             c.step(3)
             c.check()
             res.append(c.get_state())
