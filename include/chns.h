@@ -47,9 +47,9 @@ enum { CHNS_MODEL_NS = 0, CHNS_MODEL_BINARY = 1, CHNS_MODEL_TERNARY = 2 };
  * arithmetic).  FP32: transforms and point-wise work in float, ETD coefficients
  * computed in double, k = 0 modes kept in double.  FP32_STATE64: the FP32
  * right-hand side, with the state (w, c_i) carried as a pair of floats hi + lo
- * (48 significant bits) and the ETD update done in float-float arithmetic
- * (error-free sums and products: u + (u (e - 1) + N z1), e - 1 from expm1); the
- * right-hand side reads hi, the float rounding of the state.  At small dt an FP32 state loses the low bits of every increment, and
+ * (48 significant bits) and the ETD update u + d, d = u (e - 1) + N z1 (e - 1
+ * from expm1), added to the pair without rounding error; the right-hand side
+ * reads hi, the float rounding of the state.  At small dt an FP32 state loses the low bits of every increment, and
  * the spinodal modes amplify that rounding: FP32_STATE64 removes this error
  * source for one more float read and write of the modes inside the truncation
  * disc per stage (the modes outside it never reach a right-hand side, so they

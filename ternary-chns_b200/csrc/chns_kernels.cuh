@@ -747,28 +747,25 @@ __device__ __forceinline__ float two_sum(float a, float b, float& e) {
   return s;
 }
 
-// One component of the ETD update of a float pair u = hi + lo, in float-float
-// arithmetic (error-free sums and an FMA-exact product, no double):
-// stage 1  u + (u (e - 1) + N z1)   (em1 = e - 1 keeps the decay of the slow modes
-//                                    that a float e = 1 - O(1e-9) would lose)
-// stage 2  u + (N - saved) z2       (a correction, small against u)
-// Returns the new hi; the new lo in lo_out.
+// One component of the ETD update of a float pair u = hi + lo:
+// stage 1  u + d, d = u (e - 1) + N z1   (em1 = e - 1 keeps the decay of the slow
+//                                         modes that a float e = 1 - O(1e-9) would lose)
+// stage 2  u + d, d = (N - saved) z2     (a correction, small against u)
+// The increment d is formed in float from hi (lo em1 is below its rounding): its
+// rounding, 2^-24 |d|, matters only for
+// modes that change fast (|d| ~ |u|), whose errors decay with them; what must not
+// be lost is the part of a small d that a float sum hi + d would round away, so
+// that sum is error-free (TwoSum) and its error joins lo.  Returns the new hi;
+// the new lo in lo_out.
 template <int STAGE>
 __device__ __forceinline__ float etd_ff1(float hi, float lo, float n, float sv, float em1, float z1, float z2,
                                          float& lo_out) {
-  float dh, de = 0.f;
-  if (STAGE == 1) {
-    const float p = __fmul_rn(hi, em1);
-    const float pe = __fmaf_rn(hi, em1, -p);  // hi em1 = p + pe exactly
-    const float q = __fmaf_rn(lo, em1, __fmaf_rn(n, z1, pe));
-    dh = two_sum(p, q, de);
-  } else {
-    dh = __fmul_rn(__fsub_rn(n, sv), z2);
-  }
-  float se, e2;
-  const float sh = two_sum(hi, dh, se);
-  const float h = two_sum(sh, __fadd_rn(se, __fadd_rn(lo, de)), e2);
-  lo_out = e2;
+  const float d = STAGE == 1 ? __fmaf_rn(hi, em1, __fmul_rn(n, z1)) : __fmul_rn(__fsub_rn(n, sv), z2);
+  float se;
+  const float sh = two_sum(hi, d, se);
+  const float t = __fadd_rn(se, lo);
+  const float h = __fadd_rn(sh, t);  // Fast2Sum: |t| <= ulp(sh) but where hi + d cancels
+  lo_out = __fsub_rn(t, __fsub_rn(h, sh));
   return h;
 }
 
