@@ -572,6 +572,7 @@ def run_gpu(args):
             "step_model": {"bytes_per_step": model_bytes, "achieved_gbs": round(model_bytes * value / world / 1e9, 1),
                            "frac_of_peak": round(model_bytes * value / world / 1e9 / hbm, 4),
                            "note": "whole step against the 120 N^2 s bytes/step model"},
+            "grid_point_steps_per_s": round(value * n * n, 1),
             "fp64_steps_per_s": round(fp64_sps, 3),
             "fp32_over_fp64": round((value / world) / fp64_sps, 3),
             "fp32_vs_fp64": acc,
