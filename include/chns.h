@@ -239,8 +239,8 @@ int chns_ensemble_synchronize(chns_ensemble *ens);
 /* Kernel launches of one step (known after the first chns_step). */
 int chns_launches_per_step(const chns_ctx *ctx);
 
-/* 1 when the step's row kernels load their input tiles with TMA (FP32 contexts
- * whose tensor maps the driver encoded), 0 when they use cp.async.  A tile wait
+/* 1 when the step's row kernels load their input tiles with TMA (contexts whose
+ * tensor maps the driver encoded), 0 when they use cp.async.  A tile wait
  * that runs out (bounded, about a second) is reported by the next
  * chns_synchronize / chns_check as CHNS_ERR_TIMEOUT.  No counterpart in the
  * reference (tracing). */

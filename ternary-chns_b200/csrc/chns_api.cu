@@ -201,7 +201,7 @@ int build_tma(chns_ctx* c) {
   const int rows = c->jt + 1;
   T->boxr = rows >= 256 ? 256 : (rows + 7) / 8 * 8;
   T->nbox = (rows + T->boxr - 1) / T->boxr;
-  if (!c->f32) return CHNS_OK;
+  T->ecx = c->f32 ? 1 : 2;
   void* fn = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
@@ -212,10 +212,10 @@ int build_tma(chns_ctx* c) {
   const auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   for (int k = 0; k < chns::NG; k++)
     for (int v = 0; v < 2; v++) {
-      const cuuint64_t width = v == 0 ? 2 * (cuuint64_t)c->n : (cuuint64_t)c->n;  // complex per row
+      const cuuint64_t width = (v == 0 ? 2 * (cuuint64_t)c->n : (cuuint64_t)c->n) * T->ecx;  // elements per row
       const cuuint64_t dims[2] = {width, (cuuint64_t)rows};
       const cuuint64_t strides[1] = {width * 8};
-      const cuuint32_t box[2] = {2, (cuuint32_t)T->boxr};
+      const cuuint32_t box[2] = {(cuuint32_t)(2 * T->ecx), (cuuint32_t)T->boxr};
       const cuuint32_t estr[2] = {1, 1};
       if (encode(&T->map[2 * k + v], CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, c->g[k], dims, strides, box, estr,
                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,

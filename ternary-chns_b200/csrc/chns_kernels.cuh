@@ -145,10 +145,11 @@ __device__ __forceinline__ void build_c2r_input(cx<R>* v, const cx<R>* tile, int
 }
 
 // ---------------------------------------------------------------------------
-// TMA tiles of the FP32 step's row kernels.  One 2D tensor map per G slot and
-// view (pair fields: rows of 2n complex; plain fields: rows of n complex) over
-// rows 0..jt, with 64-bit elements (one FP32 complex value); a tile is nbox
-// boxes of {2 elements, boxr rows}, 16 bytes a row, rows beyond jt zero-filled.
+// TMA tiles of the step's row kernels.  One 2D tensor map per G slot and view
+// (pair fields: rows of 2n complex; plain fields: rows of n complex) over rows
+// 0..jt, with 64-bit elements (one FP32 complex value, half an FP64 one); a tile
+// is nbox boxes of {2 complex, boxr rows} (16 bytes a row in FP32, 32 in FP64),
+// rows beyond jt zero-filled.
 // One thread per group issues the boxes on the group's mbarrier; every thread
 // of the group waits on it (bounded: on timeout the kernel flags *err and goes
 // on, so a broken copy ends in an error status, not a hang).
@@ -157,6 +158,7 @@ struct __align__(64) TmaG {
   CUtensorMap map[2 * NG];  // [2 slot + 0]: pair view, [2 slot + 1]: plain view
   int use;                  // maps built (FP32 contexts); 0: cp.async tiles
   int boxr, nbox;           // rows per box, boxes per tile (nbox * boxr >= jt + 1)
+  int ecx;                  // 64-bit elements per complex value (1: FP32, 2: FP64)
   unsigned int* err;        // bit 0: an mbarrier wait timed out
 };
 constexpr int kMbarSpins = 1 << 18;  // try_wait rounds before a tile wait gives up
@@ -180,17 +182,18 @@ static __device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned par) {
         : "memory");
   return ok != 0;
 }
-// one tile (nbox boxes) of map `map` at column x into `tile`, completing on mb
+// one tile (nbox boxes) of map `map` at complex column x into `tile`, completing on mb
 static __device__ __forceinline__ void tma_tile(void* tile, const TmaG& T, int map, int x, uint64_t* mb) {
-  const unsigned bytes = (unsigned)(T.nbox * T.boxr * 16);
+  const unsigned rowb = (unsigned)(16 * T.ecx);  // bytes of a tile row: two complex values
+  const unsigned bytes = (unsigned)(T.nbox * T.boxr) * rowb;
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier generic reads of the tile
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mb)), "r"(bytes)
                : "memory");
   for (int b = 0; b < T.nbox; b++)
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-        "[%4];\n" ::"r"(smem_u32(tile) + (unsigned)(b * T.boxr * 16)),
-        "l"(reinterpret_cast<uint64_t>(&T.map[map])), "r"(x), "r"(b * T.boxr), "r"(smem_u32(mb))
+        "[%4];\n" ::"r"(smem_u32(tile) + (unsigned)(b * T.boxr) * rowb),
+        "l"(reinterpret_cast<uint64_t>(&T.map[map])), "r"(x * T.ecx), "r"(b * T.boxr), "r"(smem_u32(mb))
         : "memory");
 }
 
@@ -322,12 +325,12 @@ template <int N, class R, int GPC> struct LoadedRowSmem {
 static __device__ __forceinline__ unsigned char* align128(unsigned char* p) {
   return p + ((128u - (smem_u32(p) & 127u)) & 127u);
 }
-// TMA tiles are used when the context has tensor maps (FP32) and every group's
+// TMA tiles are used when the context has tensor maps and every group's
 // tile and box starts on 128 bytes once the layout's base is aligned: the
 // transform buffers and the tiles must be whole multiples of 128 bytes.
 template <int N, class R, int GPC>
 __device__ __forceinline__ bool tma_tiles_ok(const TmaG& T, const unsigned char* /*raw*/) {
-  if (sizeof(R) != 4 || !T.use) return false;
+  if (!T.use || T.ecx != (int)(sizeof(R) / 4)) return false;
   const size_t sh_bytes = (size_t)GPC * FftShape<N>::SMEM * sizeof(cx<R>);
   const size_t box_bytes = (size_t)T.boxr * 2 * sizeof(cx<R>);
   return sh_bytes % 128 == 0 && box_bytes % 128 == 0;

@@ -115,9 +115,9 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   // FP32 contexts with a double-float state run the P3 / P5 variants that update it
   constexpr bool F32 = sizeof(R) == 4;
   const bool s64 = F32 && c->st64;
-  // the row kernels' tiles come by TMA when the context has its tensor maps (FP32)
+  // the row kernels' tiles come by TMA when the context has its tensor maps
   const TmaG& TG = *static_cast<const TmaG*>(c->tmag);
-  const bool tma = F32 && TG.use;
+  const bool tma = TG.use != 0;
 
   // P1: spectral fan-out and x inverse transforms
   if (model == CHNS_MODEL_NS) {
