@@ -23,9 +23,10 @@
 // Ternary adds the chemical potential (chem_potential.c) to P2.  Pure
 // Navier-Stokes is P1, P2 and P5 without the curl.
 //
-// The row passes stream their inputs through a shared-memory tile filled with
-// cp.async: the copy of the next transform's input is in flight while the
-// current transform runs.
+// The row passes stream their inputs through a shared-memory tile filled by TMA
+// (cp.async per thread where no tensor map exists): the copy of the next
+// transform's input is in flight while the current transform runs.  With a
+// float-pair state (FP32 contexts) P3 / P5 also update the state's low parts.
 #pragma once
 
 #include <cuda.h>  // CUtensorMap
@@ -156,7 +157,7 @@ __device__ __forceinline__ void build_c2r_input(cx<R>* v, const cx<R>* tile, int
 // ---------------------------------------------------------------------------
 struct __align__(64) TmaG {
   CUtensorMap map[2 * NG];  // [2 slot + 0]: pair view, [2 slot + 1]: plain view
-  int use;                  // maps built (FP32 contexts); 0: cp.async tiles
+  int use;                  // maps built; 0: cp.async tiles
   int boxr, nbox;           // rows per box, boxes per tile (nbox * boxr >= jt + 1)
   int ecx;                  // 64-bit elements per complex value (1: FP32, 2: FP64)
   unsigned int* err;        // bit 0: an mbarrier wait timed out
