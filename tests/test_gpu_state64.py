@@ -179,3 +179,30 @@ def test_checkpoint_keeps_double_state(chns, tmp_path):
         c.load(path)
         for a, b in zip(c.get_state(), want):
             assert rel_l2(a, b) <= 1e-15
+
+
+def test_forced_drops_4096_within_1e5_of_fp64(chns):
+    """The benchmark's 4096^2 forced drop workload (dt = 2e-6), 50 steps: the
+    float-pair state within 1e-5 relative L2 of the FP64 step (the bench checks
+    1000 steps), the plain FP32 state further away."""
+    from chns_b200 import configs
+
+    n = 4096
+    p, c0, w0 = configs.binary_kolmogorov(n, dt=2e-6)
+    p["coef_mode"] = 1
+    with _ctx(chns, p, precision=chns.FP64) as c:
+        c.set_phase_real(c0)
+        st0 = c.get_state()
+    st0[0] = w0
+    res = {}
+    for prec in (chns.FP64, chns.FP32, chns.FP32_STATE64):
+        with _ctx(chns, p, precision=prec) as c:
+            c.set_state(*st0)
+            c.step(50)
+            c.check()
+            res[prec] = c.get_state()
+    for k in range(2):
+        e64 = rel_l2(res[chns.FP32_STATE64][k], res[chns.FP64][k])
+        e32 = rel_l2(res[chns.FP32][k], res[chns.FP64][k])
+        assert e64 <= 1e-5, (k, e64)
+        assert e64 <= e32, (k, e64, e32)
