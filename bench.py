@@ -382,6 +382,41 @@ def ensemble_members(seed: int = 3000):
     return configs.ternary_ensemble(seed)
 
 
+def ternary_leg(C, stream, n: int = 4096, steps: int = 100) -> dict:
+    """The ternary model at n^2 (sigma_12/13/23 = 0.2/0.3/0.25, nu = 0.01, M = 0.005,
+    eps = 2 dx, dt = 5e-8: stable at this resolution; spinodal noise c_i = 1/3 +
+    U[-0.02, 0.02]): steps/s per precision (CUDA events on the context's stream), and
+    the relative L2 distance of the FP32 states from the FP64 one after `steps`."""
+    import numpy as np
+
+    from chns_b200 import configs
+
+    p = configs.ternary(n, 5e-8, 0.01, 0.005, 0.2, 0.3, 0.25, coef_mode=1)
+    rng = np.random.default_rng(7)
+    ph = (1 / 3 + 0.02 * rng.uniform(-1, 1, (n, n)), 1 / 3 + 0.02 * rng.uniform(-1, 1, (n, n)))
+    import torch
+
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    out, states = {"grid": n, "steps": steps, "dt": 5e-8}, {}
+    for prec, name in ((C.FP64, "fp64"), (C.FP32, "fp32"), (C.FP32_STATE64, "fp32_state64")):
+        with C.Context(dict(p, precision=prec)) as c:
+            c.set_phase_real(*ph)
+            C.load_library().chns_set_stream(c.handle, ctypes_stream(stream))
+            c.step(3)
+            c.synchronize()
+            ev0.record(stream)
+            c.step(steps)
+            ev1.record(stream)
+            ev1.synchronize()
+            out[f"{name}_steps_per_s"] = round(steps / (ev0.elapsed_time(ev1) / 1e3), 2)
+            states[name] = c.get_state()
+    for name in ("fp32", "fp32_state64"):
+        out[f"{name}_rel_l2_vs_fp64"] = [float(np.linalg.norm(b - a) / np.linalg.norm(a))
+                                         for a, b in zip(states["fp64"], states[name])]
+    return out
+
+
 def ensemble_leg(C, steps: int):
     """Throughput of the 64-member ternary ensemble, together and one by one."""
     import numpy as np
@@ -538,6 +573,7 @@ def run_gpu(args):
     diag = diagnostics_leg(C, n, st0, not args.no_cpu_baseline) if solo else None
     adj = adjoint_leg(C, stream, args.adjoint_big_steps) if args.adjoint and solo else None
     ens = ensemble_leg(C, args.ensemble_steps) if args.ensemble_steps > 0 and solo else None
+    tern = ternary_leg(C, stream, n) if args.ternary and solo else None
 
     out = None
     if rank == 0:
@@ -581,6 +617,7 @@ def run_gpu(args):
             "diagnostics": diag,
             "adjoint": adj,
             "ensemble": ens,
+            "ternary": tern,
             "per_kernel_ms": prof["per_kernel_ms"],
             "gpu_launches": launches,
             "state_finite": bool(finite),
@@ -810,6 +847,8 @@ def main():
                     help="steps of the throughput leg of the other FP32 mode (0: skip)")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
     ap.add_argument("--ensemble-steps", type=int, default=500, help="steps of the ensemble leg (0: skip)")
+    ap.add_argument("--no-ternary", dest="ternary", action="store_false",
+                    help="skip the ternary leg (the ternary model at the bench grid, three precisions)")
     ap.add_argument("--adjoint-big-steps", type=int, default=1000,
                     help="steps of the 4096^2 FP32 adjoint memory check (0: skip)")
     ap.add_argument("--profile-case", nargs="?", const="step", default=None,
