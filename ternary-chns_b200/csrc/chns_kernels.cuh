@@ -198,7 +198,7 @@ static __device__ __forceinline__ void tma_tile(void* tile, const TmaG& T, int m
         : "memory");
 }
 
-// Tile state of a row kernel: TMA (FP32 contexts with maps) or cp.async.
+// Tile state of a row kernel: TMA (contexts with tensor maps) or cp.async.
 template <class R> struct TileLoader {
   bool tma;
   uint64_t* mb;  // this group's mbarrier (TMA)
