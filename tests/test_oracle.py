@@ -118,6 +118,25 @@ def test_taylor_green_decays_exactly():
     assert np.abs(w - w0 * math.exp(-2 * p["nu"] * 0.5)).max() <= 1e-12
 
 
+@pytest.mark.parametrize("coef_mode", [0, 1])
+def test_kolmogorov_laminar_flow_exact(coef_mode):
+    """Kolmogorov forcing f = F0 sin(kf y) x-hat from rest (pure Navier-Stokes): the
+    flow stays a shear w(y), so u.grad w = 0 and the forcing is constant; ETD2RK
+    integrates w' = -nu kf^2 w - F0 kf cos(kf y) exactly:
+    w(t) = -(F0 / (nu kf)) (1 - exp(-nu kf^2 t)) cos(kf y)."""
+    n, nu, dt, steps, f0, kf = 32, 0.05, 1e-2, 50, 1.3, 4.0
+    p = dict(model=0, nx=n, ny=n, lx=2 * math.pi, ly=2 * math.pi, dt=dt, nu=nu, coef_mode=coef_mode,
+             force_amp=f0, force_k=kf)
+    o = O.Oracle(p)
+    o.set_state(np.zeros((n, n // 2 + 1), np.complex128))
+    o.step(steps)
+    w = o.ifft(o.get_state()[0])
+    y = np.arange(n) * (2 * math.pi / n)
+    amp = -(f0 / (nu * kf)) * (1 - math.exp(-nu * kf * kf * steps * dt))
+    want = amp * np.cos(kf * y)[None, :] * np.ones(n)[:, None]
+    assert np.abs(w - want).max() <= 1e-12 * abs(amp)
+
+
 def test_mean_concentration_conserved():
     for name in ("bin32", "ter32"):
         g = load_small(name)
