@@ -160,9 +160,10 @@ def _run_physical(p, ph, w, steps):
 
 @pytest.mark.parametrize("model", [1, 2])
 def test_restatement_commutes_with_grid_shifts(model):
-    """The step commutes with a translation by whole grid cells (the scheme is
-    translation invariant; only rounding differs): 20 steps, rel L2 <= 1e-13
-    (a sign error in the advection or the surface-tension curl breaks it by 1e-4)."""
+    """The step commutes with a translation by whole grid cells (without forcing,
+    nothing in the scheme depends on position; only rounding differs): 20 steps,
+    rel L2 <= 1e-13.  A transform that is not an exact DFT (a wrong twiddle, a
+    misplaced mode) would break it."""
     p, ph, w = _sym_case(model)
     sh = (5, 11)
     a = _run_physical(p, ph, w, 20)
