@@ -865,7 +865,7 @@ def main():
     if args.impl == "reference":
         if args.n == N_DEFAULT and args.steps > 10:
             args.steps = 10  # one reference step at 4096^2 takes seconds
-            args.warmup = 1
+            args.warmup = 3
         run_reference(args)
     else:
         run_gpu(args)
