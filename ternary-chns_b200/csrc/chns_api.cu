@@ -748,25 +748,34 @@ int chns_rhs(chns_ctx* c, double* nw, double* nc1, double* nc2, int where) {
         rc = CHNS_ERR_CUDA;
     }
   }
-  if (rc == CHNS_OK && c->f32 && cudaMemcpy(k0keep, c->k0, sizeof(k0keep), cudaMemcpyDeviceToHost) != cudaSuccess)
-    rc = CHNS_ERR_CUDA;
-  if (rc == CHNS_OK) c->L->stage(c, 1);
+  bool k0kept = false;  // k0keep holds the k = 0 modes (FP32 contexts)
+  if (rc == CHNS_OK && c->f32) {
+    if (cudaMemcpy(k0keep, c->k0, sizeof(k0keep), cudaMemcpyDeviceToHost) != cudaSuccess) rc = CHNS_ERR_CUDA;
+    else k0kept = true;
+  }
+  const bool ran = rc == CHNS_OK;  // the stage overwrites the state: restore it from the copies
+  if (ran) c->L->stage(c, 1);
   double* dst[3] = {nw, nc1, nc2};
   for (int f = 0; f <= c->p.model && rc == CHNS_OK; f++)
     if (dst[f]) rc = get_field(c, f, c->saved[f], dst[f], where, 3 + f);
+  // restore the state (a failed restore is reported: the state is then undefined)
+  int rrc = CHNS_OK;
   for (int f = 0; f <= c->p.model; f++) {
     if (keep[f]) {
-      cudaMemcpyAsync(c->state[f], keep[f], bytes, cudaMemcpyDeviceToDevice, c->stream);
-      cudaStreamSynchronize(c->stream);
+      if (ran && cudaMemcpyAsync(c->state[f], keep[f], bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+        rrc = CHNS_ERR_CUDA;
+      if (cudaStreamSynchronize(c->stream) != cudaSuccess) rrc = CHNS_ERR_CUDA;
       cudaFree(keep[f]);
     }
     if (keeplo[f]) {
-      cudaMemcpyAsync(c->statelo[f], keeplo[f], bytes, cudaMemcpyDeviceToDevice, c->stream);
-      cudaStreamSynchronize(c->stream);
+      if (ran && cudaMemcpyAsync(c->statelo[f], keeplo[f], bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+        rrc = CHNS_ERR_CUDA;
+      if (cudaStreamSynchronize(c->stream) != cudaSuccess) rrc = CHNS_ERR_CUDA;
       cudaFree(keeplo[f]);
     }
   }
-  if (c->f32) cudaMemcpy(c->k0, k0keep, sizeof(k0keep), cudaMemcpyHostToDevice);
+  if (ran && k0kept && cudaMemcpy(c->k0, k0keep, sizeof(k0keep), cudaMemcpyHostToDevice) != cudaSuccess) rrc = CHNS_ERR_CUDA;
+  if (rc == CHNS_OK) rc = rrc;
   if (rc == CHNS_OK) rc = chns_synchronize(c);
   return rc;
 }
