@@ -90,6 +90,12 @@ static const double *twiddles(int n)
 /* scratch buffer of the same size.                                           */
 /* ------------------------------------------------------------------------- */
 
+/* 0: radix-4 stages, two real rows per complex transform; 1: radix-2 stages, one
+ * real row per complex transform (a second rounding order of the same DFT) */
+static int g_variant = 0;
+void fftc_set_variant(int v) { g_variant = v ? 1 : 0; }
+int fftc_get_variant(void) { return g_variant; }
+
 static void stockham(int n, double *x, double *y, int sign)
 {
     const double *tw = twiddles(n);
@@ -98,7 +104,7 @@ static void stockham(int n, double *x, double *y, int sign)
     if (n <= 1) return;
     while (Ns < n) {
         int rem = n / Ns;
-        int R = (rem % 4 == 0) ? 4 : 2;
+        int R = (g_variant == 0 && rem % 4 == 0) ? 4 : 2;
         int m = n / R;                  /* butterflies */
         int step = n / (Ns * R);        /* twiddle stride */
         for (int b = 0; b < m / Ns; b++) {
@@ -262,12 +268,39 @@ typedef struct {
 
 #define COLBLK 8
 
+/* variant 1: one real row x (n1 + 2 doubles) -> its half spectrum, in place */
+static void row_r2c_single(int n1, double *x, double *z, double *y)
+{
+    for (int n = 0; n < n1; n++) { z[2 * n] = x[n]; z[2 * n + 1] = 0.0; }
+    stockham(n1, z, y, -1);
+    for (int k = 0; k <= n1 / 2; k++) { x[2 * k] = z[2 * k]; x[2 * k + 1] = z[2 * k + 1]; }
+}
+
+/* variant 1: one half spectrum -> its real row, in place (imaginary parts of the
+ * k = 0 and k = n1/2 bins ignored) */
+static void row_c2r_single(int n1, double *x, double *z, double *y)
+{
+    int h = n1 / 2;
+    z[0] = x[0]; z[1] = 0.0;
+    z[2 * h] = x[2 * h]; z[2 * h + 1] = 0.0;
+    for (int k = 1; k < h; k++) {
+        z[2 * k] = x[2 * k];            z[2 * k + 1] = x[2 * k + 1];
+        z[2 * (n1 - k)] = x[2 * k];     z[2 * (n1 - k) + 1] = -x[2 * k + 1];
+    }
+    stockham(n1, z, y, +1);
+    for (int n = 0; n < n1; n++) x[n] = z[2 * n];
+}
+
 /* rows [lo, hi) (even), forward: pack two rows, FFT, split into half spectra */
 static void rows_r2c(void *vctx, int lo, int hi, double *s)
 {
     pass_ctx *c = (pass_ctx *)vctx;
     int n1 = c->n1, h = n1 / 2, rs = n1 + 2;
     double *z = s, *y = s + 2 * (size_t)n1;
+    if (g_variant) {
+        for (int r = lo; r < hi; r++) row_r2c_single(n1, c->data + (size_t)r * rs, z, y);
+        return;
+    }
     for (int r = lo; r < hi; r += 2) {
         double *xa = c->data + (size_t)r * rs;
         double *xb = xa + rs;
@@ -292,6 +325,10 @@ static void rows_c2r(void *vctx, int lo, int hi, double *s)
     pass_ctx *c = (pass_ctx *)vctx;
     int n1 = c->n1, h = n1 / 2, rs = n1 + 2;
     double *z = s, *y = s + 2 * (size_t)n1;
+    if (g_variant) {
+        for (int r = lo; r < hi; r++) row_c2r_single(n1, c->data + (size_t)r * rs, z, y);
+        return;
+    }
     for (int r = lo; r < hi; r += 2) {
         double *xa = c->data + (size_t)r * rs;
         double *xb = xa + rs;

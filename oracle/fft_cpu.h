@@ -34,6 +34,13 @@ void fftc_c2r_2d(fftc_plan *p, double *data);
  * sign = -1 forward (exp(-2 pi i jk/n)), +1 inverse. */
 void fftc_c2c_1d(int n, double *z, int sign);
 
+/* Rounding order of the transforms (default 0): 0 = radix-4 stages with two real
+ * rows packed into one complex transform; 1 = radix-2 stages, one real row per
+ * complex transform.  Both compute the same DFT; comparing runs under the two
+ * measures how much the FFT's own rounding moves a trajectory. */
+void fftc_set_variant(int v);
+int fftc_get_variant(void);
+
 /* Number of host threads used for the 2D passes (default 1). */
 void fftc_set_threads(int nthreads);
 int fftc_get_threads(void);

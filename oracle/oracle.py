@@ -74,8 +74,15 @@ def _load():
             getattr(L, f).argtypes = [vp, vp]
         L.orc_etd_coefs.argtypes = [vp, ip, ip, dp]
         L.fftc_set_threads.argtypes = [ip]
+        L.fftc_set_variant.argtypes = [ip]
         _lib = L
     return _lib
+
+
+def set_fft_variant(v: int) -> None:
+    """Selects the oracle FFT's rounding order (0: default radix-4, paired rows;
+    1: radix-2, single rows) for every Oracle in this process."""
+    _load().fftc_set_variant(int(v))
 
 
 def _ptr(a):

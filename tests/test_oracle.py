@@ -1,6 +1,7 @@
 """CPU tests of the oracle: the FFT, the C restatement against the reference's
 own compiled code (golden fixtures made by tests/golden/make_golden.py, and live
 when oracle/_ref is built), and analytic known answers."""
+import functools
 import math
 import os
 
@@ -77,18 +78,44 @@ def test_restatement_bitwise_vs_live_reference(name):
         assert np.array_equal(a, b), name
 
 
+@functools.lru_cache(maxsize=None)
+def _cfg0_final(fft_variant: int):
+    """Final state of the binary spinodal 256^2 run (1000 steps) under an oracle FFT
+    rounding order (0: the default)."""
+    g = load_full("bin256")
+    p = g["params"]
+    O.set_fft_variant(fft_variant)
+    try:
+        o = O.Oracle(p, nthreads=1)
+        p1, p2, w = MG.initial_state(p["model"], p["nx"], p["lx"], 100, None, 0, 0)
+        MG.apply_initial(o, p["model"], p1, p2, w)
+        o.step(g["steps"])
+        return tuple(o.get_state())
+    finally:
+        O.set_fft_variant(0)
+
+
 def test_restatement_cfg0_full_fingerprint():
     """Binary spinodal 256^2, 1000 steps, against the reference run."""
     g = load_full("bin256")
-    p = g["params"]
-    o = O.Oracle(p, nthreads=1)
-    p1, p2, w = MG.initial_state(p["model"], p["nx"], p["lx"], 100, None, 0, 0)
-    MG.apply_initial(o, p["model"], p1, p2, w)
-    o.step(g["steps"])
-    for k, a in enumerate(o.get_state()):
+    for k, a in enumerate(_cfg0_final(0)):
         fp = MG.fingerprint(a)
         ref = {key: g[f"final{k}_{key}"] for key in ("low", "proj", "norm")}
         assert MG.fingerprint_rel_err(ref, fp) <= 1e-12
+
+
+def test_fft_rounding_order_moves_cfg0_far_below_the_parity_tolerance():
+    """FFTW is not available here, and a GPU transform rounds in its own order, so
+    the parity target (1e-10 after the 1000 steps of the binary spinodal run) must
+    be far above what the order of the FFT's own roundings alone does to the
+    trajectory.  The same run with the oracle FFT in a second order (radix-2 stages,
+    one real row per transform, instead of radix-4 stages on row pairs) ends
+    3.8e-13 (w) and 1.1e-13 (c) from the first: bound 1e-11, and the two orders must
+    differ (else the check measures nothing)."""
+    a, b = _cfg0_final(0), _cfg0_final(1)
+    for x, y in zip(a, b):
+        d = rel_l2(y, x)
+        assert 0 < d <= 1e-11, d
 
 
 @pytest.mark.slow
