@@ -211,6 +211,12 @@ class Context:
             raise ValueError(f"expected spectral shape {self.shape}, got {a.shape}")
         return a
 
+    def _real(self, a):
+        a = np.ascontiguousarray(a, np.float64)
+        if a.shape != (self.nx, self.ny):
+            raise ValueError(f"expected real shape {(self.nx, self.ny)}, got {a.shape}")
+        return a
+
     def set_state(self, w, c1=None, c2=None):
         arrs = [self._spec(a) if a is not None else None for a in (w, c1, c2)]
         _check(self.L.chns_set_state(self._h, *[_ptr(a) for a in arrs], HOST), "chns_set_state")
@@ -222,8 +228,8 @@ class Context:
         return out
 
     def set_phase_real(self, p1, p2=None):
-        a = np.ascontiguousarray(p1, np.float64)
-        b = np.ascontiguousarray(p2, np.float64) if p2 is not None else None
+        a = self._real(p1)
+        b = self._real(p2) if p2 is not None else None
         _check(self.L.chns_set_phase_real(self._h, _ptr(a), _ptr(b), HOST), "chns_set_phase_real")
 
     def pin_host(self, a: np.ndarray):
@@ -301,7 +307,7 @@ class Context:
         return out
 
     def dfft(self, real):
-        x = np.ascontiguousarray(real, np.float64)
+        x = self._real(real)
         out = np.empty(self.shape, np.complex128)
         _check(self.L.chns_dfft(self._h, _ptr(x), _ptr(out), HOST), "chns_dfft")
         return out
@@ -328,6 +334,8 @@ class Context:
         sigma); for the ternary model it is a pair (c1, c2) and the parameters are
         (nu, lambda, sigma_12, sigma_13, sigma_23).  The state is unchanged."""
         lw = np.ascontiguousarray(loss_w, np.float64)
+        if lw.shape != (3,):
+            raise ValueError("loss_w: three weights")
         J = np.zeros(1)
         gw = np.empty(self.shape, np.complex128)
         nc = max(self.model, 1)

@@ -77,3 +77,25 @@ def test_calls_reject_a_null_context_without_cuda(lib):
         f = getattr(lib, fn)
         rc = f(None, 1) if fn == "chns_step" else f(None)
         assert rc in (-1, 0) if fn in ("chns_launches_per_step", "chns_tma_tiles") else rc == -1, fn
+
+
+def test_binding_rejects_wrongly_shaped_host_arrays(lib):
+    """The binding checks host array shapes before the C call reads nx * ny values
+    from them (no GPU needed: the checks come first)."""
+    import numpy as np
+
+    import chns_b200
+
+    c = chns_b200.Context.__new__(chns_b200.Context)
+    c.L, c._h, c.model, c.nx, c.ny = lib, None, 1, 32, 32
+    c.shape = (32, 17)
+    with pytest.raises(ValueError):
+        c.set_phase_real(np.zeros((32, 30)))
+    with pytest.raises(ValueError):
+        c.set_phase_real(np.zeros((32, 32)), np.zeros(32 * 32))
+    with pytest.raises(ValueError):
+        c.dfft(np.zeros((16, 32)))
+    with pytest.raises(ValueError):
+        c.set_state(np.zeros((32, 16), np.complex128))
+    with pytest.raises(ValueError):
+        c.adjoint(2, 1, loss_w=(1.0, 1.0))
