@@ -748,13 +748,14 @@ def e2e_host_loop(ctx, stream, steps: int):
     ptrs = [a.data_ptr() for a in pin]
     import ctypes
 
+    def ok(what, rc):
+        if rc != 0:
+            raise RuntimeError(f"{what} returned {rc} in the end-to-end leg")
+
     def one():
-        rc = L.chns_set_state(ctx.handle, ctypes.c_void_p(ptrs[0]), ctypes.c_void_p(ptrs[1]), None, 0)
-        assert rc == 0
-        rc = L.chns_step(ctx.handle, 1)
-        assert rc == 0
-        rc = L.chns_get_state(ctx.handle, ctypes.c_void_p(ptrs[0]), ctypes.c_void_p(ptrs[1]), None, 0)
-        assert rc == 0
+        ok("chns_set_state", L.chns_set_state(ctx.handle, ctypes.c_void_p(ptrs[0]), ctypes.c_void_p(ptrs[1]), None, 0))
+        ok("chns_step", L.chns_step(ctx.handle, 1))
+        ok("chns_get_state", L.chns_get_state(ctx.handle, ctypes.c_void_p(ptrs[0]), ctypes.c_void_p(ptrs[1]), None, 0))
 
     one()
     torch.cuda.synchronize()
