@@ -234,6 +234,34 @@ def test_free_energy_non_increasing_when_viscosity_dominates(lam):
     assert e[-1] < 0.75 * e[0]
 
 
+@pytest.mark.parametrize("lam", [0.005, 0.05])
+def test_ternary_energy_with_the_lambda_term_non_increasing(lam):
+    """Ternary Cahn-Hilliard with the flow suppressed (omega_0 = 0, nu = 1): the
+    chemical potentials of chem_potential.c and surface_tension.c are the gradient
+    of E = E_bulk + E_grad (free_energy.c) + (12/eps) 3 Lambda <c1^2 c2^2 c3^2>
+    (the Lambda part of G_i, 6 Lambda c_i c_j^2 c_k^2, is the derivative of
+    3 Lambda c1^2 c2^2 c3^2), so E falls at every one of 400 steps.  free_energy.c
+    leaves the Lambda term out; its E rises in most of the early steps at M = 0.005."""
+    g = load_small("ter64")
+    p = dict(g["params"], nu=1.0)
+    p["lambda"] = lam
+    lam_x = p.get("xlambda", 2.0)
+    o = O.Oracle(p)
+    o.set_state(np.zeros_like(g["init"][0]), g["init"][1], g["init"][2])
+    full, ref = [], []
+    for _ in range(400):
+        eb, eg = o.free_energy()
+        st = o.get_state()
+        c1, c2 = o.ifft(st[1]), o.ifft(st[2])
+        c3 = 1.0 - c1 - c2
+        ref.append(eb + eg)
+        full.append(eb + eg + (12.0 / p["epsilon"]) * 3.0 * lam_x * np.mean(c1 ** 2 * c2 ** 2 * c3 ** 2))
+        o.step(1)
+    assert np.all(np.diff(full) < 0)
+    if lam == 0.005:
+        assert np.sum(np.diff(ref) > 0) > 300
+
+
 def test_mean_concentration_conserved():
     for name in ("bin32", "ter32"):
         g = load_small(name)
