@@ -262,6 +262,27 @@ def test_ternary_energy_with_the_lambda_term_non_increasing(lam):
         assert np.sum(np.diff(ref) > 0) > 300
 
 
+def test_binary_kinetic_plus_free_energy_non_increasing():
+    """The coupled binary CHNS energy law: with the capillary force mu grad c
+    driving a flow from rest (omega_0 = 0, nu = 1e-3, M = 0.05), <|u|^2>/2 grows
+    from zero while <|u|^2>/2 + E_bulk + E_grad falls at every one of 400 steps
+    (kinetic_energy.c, free_energy.c)."""
+    g = load_small("bin64")
+    p = dict(g["params"], nu=1e-3)
+    p["lambda"] = 0.05
+    o = O.Oracle(p)
+    o.set_state(np.zeros_like(g["init"][0]), g["init"][1])
+    tot, ke = [], []
+    for _ in range(400):
+        eb, eg = o.free_energy()
+        k = o.kinetic_energy()[0]
+        tot.append(eb + eg + k)
+        ke.append(k)
+        o.step(1)
+    assert np.all(np.diff(tot) < 0)
+    assert ke[0] == 0.0 and ke[-1] > 1e-3
+
+
 def test_mean_concentration_conserved():
     for name in ("bin32", "ter32"):
         g = load_small(name)
