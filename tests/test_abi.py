@@ -99,3 +99,24 @@ def test_binding_rejects_wrongly_shaped_host_arrays(lib):
         c.set_state(np.zeros((32, 16), np.complex128))
     with pytest.raises(ValueError):
         c.adjoint(2, 1, loss_w=(1.0, 1.0))
+
+
+@pytest.mark.parametrize("std,lang", [("c89", "c"), ("c99", "c"), ("c++11", "c++")])
+def test_header_compiles_and_links_for_c_and_cpp_hosts(lib, tmp_path, std, lang):
+    """include/chns.h is a plain C header: it compiles warning-free as C89, C99
+    (pedantic) and C++11, and a host program links against the library and calls
+    an entry point that needs no GPU."""
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "host.c"
+    src.write_text('#include "chns.h"\n'
+                   "int main(void) { chns_params p; chns_default_params(&p, CHNS_MODEL_BINARY, 256);\n"
+                   "  return p.nx == 256 && p.ny == 256 ? 0 : 1; }\n")
+    cc = "g++" if lang == "c++" else "gcc"
+    libdir = os.path.join(root, "ternary-chns_b200", "lib")
+    exe = tmp_path / "host"
+    subprocess.run([cc, f"-std={std}", "-Wall", "-Wextra", "-Werror"] + (["-pedantic"] if std == "c99" else [])
+                   + ["-x", lang, str(src), "-x", "none", "-I", os.path.join(root, "include"), "-L", libdir,
+                      "-lchns_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True, capture_output=True)
+    assert subprocess.run([str(exe)]).returncode == 0
