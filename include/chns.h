@@ -91,6 +91,19 @@ void chns_default_params(chns_params *p, int model, int n);
 int chns_create(const chns_params *p, chns_ctx **out);
 int chns_destroy(chns_ctx *ctx);
 
+/* The host-side tables chns_create builds, computed without a context or a GPU
+ * (no counterpart in the reference, which recomputes them inside its loops; these
+ * expose the exact values the step uses so that they can be checked):
+ * chns_etd_coefficients gives, for the mode (kx index i in 0..nx-1, ky index j in
+ * 0..nx/2), out[0..5] = e^{-nu k^2 dt}, zeta1, zeta2 of the vorticity and
+ * e^{c dt}, z1, z2 of the phase fields (etd2rk.c:88-111,117-127 / 162-186,191-203,
+ * per coef_mode; NS contexts: 1, dt, dt/2), in double;
+ * chns_truncation_rows fills mrow[0..nx/2] with the largest |kx index| kept in
+ * each ky row by the truncation (functions.c:47-84), -1 for an empty row.
+ * Parameters are checked as by chns_create. */
+int chns_etd_coefficients(const chns_params *p, int i, int j, double *out);
+int chns_truncation_rows(const chns_params *p, int *mrow);
+
 /* Uses `stream` (a cudaStream_t) for all later work instead of the context's own. */
 int chns_set_stream(chns_ctx *ctx, void *stream);
 int chns_synchronize(chns_ctx *ctx);

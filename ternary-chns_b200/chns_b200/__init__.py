@@ -77,6 +77,8 @@ def load_library(path: str = LIB_PATH):
     L.chns_diagnostics.argtypes = [vp, dp, dp]
     L.chns_launches_per_step.argtypes = [vp]
     L.chns_tma_tiles.argtypes = [vp]
+    L.chns_etd_coefficients.argtypes = [vp, ip, ip, vp]
+    L.chns_truncation_rows.argtypes = [vp, vp]
     L.chns_profile_step.argtypes = [vp, ip, vp, vp, ip]
     L.chns_profile_step.restype = ip
     L.chns_adjoint.argtypes = [vp, ip, ip, vp, vp, vp, vp, vp, ip]

@@ -147,6 +147,33 @@ void etd_coefs(const chns_params& p, double ksqr, double* o) {
   o[5] = z2c;
 }
 
+// k^2 of the mode (|kx index| m, ky index j): kx = fx m, ky = fy j (functions.c:11-33;
+// the sign of kx does not enter)
+double mode_ksq(double fx, double fy, int m, int j) {
+  const double kx = fx * m, ky = fy * j;
+  return kx * kx + ky * ky;
+}
+
+// The truncation table (functions.c:47-84, the sharp cut k^2 > ((nx/dealias_div) fx)^2):
+// mrow[j] = the largest |m| kept in ky row j (-1: none), j = 0..nx/2.  Returns jt,
+// the last row with a kept mode.
+int truncation_rows(const chns_params& p, double fx, double fy, int* mrow) {
+  const int n = p.nx, nr = p.nx / 2 + 1;
+  const double dax = (p.nx / p.dealias_div) * fx;
+  const double dealias = dax * dax;
+  int jt = -1;
+  for (int j = 0; j < nr; j++) {
+    int lim = -1;
+    for (int m = 0; m <= n / 2; m++) {
+      if (mode_ksq(fx, fy, m, j) > dealias) break;
+      lim = m;
+    }
+    mrow[j] = lim;
+    if (lim >= 0) jt = j;
+  }
+  return jt;
+}
+
 int validate(const chns_params* p) {
   if (!p) return CHNS_ERR_ARG;
   if (p->model < 0 || p->model > 2) return CHNS_ERR_ARG;
@@ -363,22 +390,8 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
   const int n = c->n, nr = c->nr;
   c->fx = (2 * M_PI) / p.lx;
   c->fy = (2 * M_PI) / p.ly;
-  const double dax = (p.nx / p.dealias_div) * c->fx;
-  const double dealias = dax * dax;
   std::vector<int> mrow(nr, -1);
-  c->jt = -1;
-  for (int j = 0; j < nr; j++) {
-    const double ky = c->fy * j;
-    int lim = -1;
-    for (int m = 0; m <= n / 2; m++) {
-      const double kx = c->fx * m;
-      const double ks = kx * kx + ky * ky;
-      if (ks > dealias) break;
-      lim = m;
-    }
-    mrow[j] = lim;
-    if (lim >= 0) c->jt = j;
-  }
+  c->jt = truncation_rows(p, c->fx, c->fy, mrow.data());
   if (c->jt < 0 || c->jt >= n / 2) {
     free_all(c);
     return CHNS_ERR_UNSUPPORTED;
@@ -407,12 +420,9 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
   const size_t tsz = (size_t)nr * nr;
   std::vector<double> coef(6 * tsz);
   for (int j = 0; j < nr; j++) {
-    const double ky = c->fy * j;
     for (int m = 0; m < nr; m++) {
-      const double kx = c->fx * m;
-      const double ks = kx * kx + ky * ky;
       double o[6];
-      etd_coefs(p, ks, o);
+      etd_coefs(p, mode_ksq(c->fx, c->fy, m, j), o);
       for (int q = 0; q < 6; q++) coef[q * tsz + (size_t)j * nr + m] = o[q];
     }
   }
@@ -486,6 +496,23 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
     return CHNS_ERR_CUDA;
   }
   *out = c;
+  return CHNS_OK;
+}
+
+int chns_etd_coefficients(const chns_params* p, int i, int j, double* out) {
+  const int rc = validate(p);
+  if (rc != CHNS_OK) return rc;
+  if (!out || i < 0 || i >= p->nx || j < 0 || j > p->nx / 2) return CHNS_ERR_ARG;
+  const int m = i <= p->nx / 2 ? i : p->nx - i;
+  etd_coefs(*p, mode_ksq((2 * M_PI) / p->lx, (2 * M_PI) / p->ly, m, j), out);
+  return CHNS_OK;
+}
+
+int chns_truncation_rows(const chns_params* p, int* mrow) {
+  const int rc = validate(p);
+  if (rc != CHNS_OK) return rc;
+  if (!mrow) return CHNS_ERR_ARG;
+  truncation_rows(*p, (2 * M_PI) / p->lx, (2 * M_PI) / p->ly, mrow);
   return CHNS_OK;
 }
 
