@@ -100,6 +100,16 @@ template <int N, class R> struct Sizes {
   static int grid_rows(int rows) { return (rows + GPC - 1) / GPC; }
 };
 
+// P3's shared memory: the transform buffers, plus (CHNS_P3_STAGE_F builds) one
+// spectrum per transform group kept between two of its transforms
+template <int N, class R> constexpr size_t p3_smem() {
+#ifdef CHNS_P3_STAGE_F
+  return Sizes<N, R>::FFT_SMEM + Sizes<N, R>::FRAG;
+#else
+  return Sizes<N, R>::FFT_SMEM;
+#endif
+}
+
 template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   using S = Sizes<N, R>;
   constexpr int GPC = S::GPC;
@@ -175,22 +185,22 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   if (model == CHNS_MODEL_BINARY) {
     if (stage == 1) {
       auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1, F32> : k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1, false>;
-      set_smem(k, S::FFT_SMEM);
-      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+      set_smem(k, (p3_smem<N, R>()));
+      k<<<rows_all, S::THREADS, (p3_smem<N, R>()), st>>>(B, P);
     } else {
       auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 2, F32> : k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 2, false>;
-      set_smem(k, S::FFT_SMEM);
-      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+      set_smem(k, (p3_smem<N, R>()));
+      k<<<rows_all, S::THREADS, (p3_smem<N, R>()), st>>>(B, P);
     }
   } else {
     if (stage == 1) {
       auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 1, F32> : k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 1, false>;
-      set_smem(k, S::FFT_SMEM);
-      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+      set_smem(k, (p3_smem<N, R>()));
+      k<<<rows_all, S::THREADS, (p3_smem<N, R>()), st>>>(B, P);
     } else {
       auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 2, F32> : k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 2, false>;
-      set_smem(k, S::FFT_SMEM);
-      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+      set_smem(k, (p3_smem<N, R>()));
+      k<<<rows_all, S::THREADS, (p3_smem<N, R>()), st>>>(B, P);
     }
   }
   launches++;
