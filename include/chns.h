@@ -283,8 +283,11 @@ const char *chns_status_string(int status);
  * fixed device array of 2 x 257 x 512 complex doubles (4.2 MB) that every GPU
  * loading this library holds until exit, so n must be a power of two with
  * 32 <= n <= CHNS_NOALLOC_MAX_N (else CHNS_ERR_UNSUPPORTED).  The first call on a
- * device does a one-time set-up for that device (symbol lookup and twiddle
- * upload); make it before any stream capture.  All calls share the array:
+ * device does a one-time set-up for that device (symbol lookup, twiddle upload,
+ * loading the kernels of every supported n, then a device synchronisation so
+ * that the first transform on any stream reads a complete table); make it before
+ * any stream capture.  The set-up is redone after a cudaDeviceReset.  All calls
+ * share the array:
  * calls that overlap on the GPU race, so order them on one stream.  Work is
  * enqueued on `stream` (a cudaStream_t, NULL = legacy default stream); the call
  * returns without waiting for it. */

@@ -13,10 +13,15 @@ a generated global.h (the reference's file with the parameter values substituted
 and a generated macro.h into the configuration's build folder under oracle/_ref/,
 and compiles with ``-I <that folder> -I-`` so that the reference's
 ``#include "global.h"`` resolves to the generated header instead of the file next
-to the source.  Nothing under /root/reference is written, and no reference source
+to the source.  Nothing in the reference's folder is written, and no reference source
 is kept in the repository: oracle/_ref/ is git-ignored build output.
 
-Usage:  python oracle/build_ref.py [config ...]      (default: all configurations)
+The reference's source folder comes only from the caller: the environment
+variable CHNS_REFERENCE_DIR, set_reference_dir(), or ``--ref DIR`` on the command
+line.  With none of them set, nothing is built (and the command line fails with a
+message saying so).
+
+Usage:  python oracle/build_ref.py --ref DIR [config ...]   (default: all configurations)
 """
 from __future__ import annotations
 
@@ -26,7 +31,20 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("CHNS_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("CHNS_REFERENCE_DIR") or None
+
+
+def set_reference_dir(path: str | None) -> None:
+    """Names the folder holding the reference's sources (global.h, etd2rk.c, ...)."""
+    global REF
+    REF = path or None
+
+
+def _ref(*parts: str) -> str:
+    if not REF:
+        raise RuntimeError("the reference's source folder is not set: CHNS_REFERENCE_DIR, "
+                           "set_reference_dir() or --ref DIR")
+    return os.path.join(REF, *parts)
 OUT = os.path.join(HERE, "_ref")
 
 # The reference files that the hot path and its set-up/diagnostics need
@@ -82,7 +100,7 @@ _SUBST = {  # macro name -> key in the config dict
 
 
 def _gen_global_h(cfg: dict) -> str:
-    src = open(os.path.join(REF, "global.h")).read()
+    src = open(_ref("global.h")).read()
     out = []
     for line in src.splitlines():
         m = re.match(r"^(\s*)#define\s+(\w+)\b(.*)$", line)
@@ -109,7 +127,7 @@ def _run(cmd):
 
 
 def reference_present() -> bool:
-    return all(os.path.isfile(os.path.join(REF, f)) for f in REF_SOURCES + ["global.h"])
+    return bool(REF) and all(os.path.isfile(os.path.join(REF, f)) for f in REF_SOURCES + ["global.h"])
 
 
 def lib_path(name: str, dropin: bool = False) -> str:
@@ -128,7 +146,7 @@ def build(name: str, force: bool = False, dropin: bool = False) -> str:
         raise FileNotFoundError("build libchns_b200.so before the drop-in oracle")
     deps = [os.path.join(HERE, f) for f in ("ref_harness.c", "fft_cpu.c", "fft_cpu.h", "build_ref.py",
                                             "shim/shim.c", "shim/mpi.h", "shim/fftw3-mpi.h")]
-    deps += [os.path.join(REF, f) for f in REF_SOURCES + ["global.h"]]
+    deps += [_ref(f) for f in REF_SOURCES + ["global.h"]]
     if dropin:
         deps += [os.path.join(repo, "ternary-chns_b200", "csrc", "etd2rk_dropin.c"),
                  os.path.join(repo, "include", "chns.h"), os.path.join(chns_lib_dir, "libchns_b200.so")]
@@ -152,7 +170,7 @@ def build(name: str, force: bool = False, dropin: bool = False) -> str:
         sources = [s for s in sources if s != "etd2rk.c"]
     for s in sources:
         o = os.path.join(bdir, s.replace(".c", ".o"))
-        _run([cc, *flags, *inc, "-c", os.path.join(REF, s), "-o", o])
+        _run([cc, *flags, *inc, "-c", _ref(s), "-o", o])
         objs.append(o)
     if dropin:
         o = os.path.join(bdir, "etd2rk_dropin.o")
@@ -195,9 +213,15 @@ def build_all(names=None, force=False, dropin: bool = True) -> list[str]:
 
 
 if __name__ == "__main__":
-    names = sys.argv[1:] or None
+    args = sys.argv[1:]
+    if "--ref" in args:
+        k = args.index("--ref")
+        set_reference_dir(args[k + 1])
+        del args[k:k + 2]
+    names = args or None
+    if not REF:
+        sys.exit("build_ref.py: give the reference's source folder with --ref DIR or CHNS_REFERENCE_DIR")
     if not reference_present():
-        print(f"reference sources not found under {REF}; nothing built")
-        sys.exit(0)
+        sys.exit(f"build_ref.py: the reference's sources are not under {REF}")
     for p in build_all(names, force=True):
         print(p)

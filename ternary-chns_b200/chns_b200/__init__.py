@@ -19,7 +19,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
-LIB_PATH = os.path.join(PKG, "lib", "libchns_b200.so")
+# CHNS_B200_LIB names a variant build of the same library (e.g. one compiled
+# with other CHNS_* defines by build.build(defines=..., lib=...)) for parity
+# tests and timing of that variant; the default is the in-tree build.
+LIB_PATH = os.environ.get("CHNS_B200_LIB") or os.path.join(PKG, "lib", "libchns_b200.so")
 
 MODEL_NS, MODEL_BINARY, MODEL_TERNARY = 0, 1, 2
 FP64, FP32, FP32_STATE64 = 0, 1, 2

@@ -593,18 +593,15 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par
 #pragma unroll
         for (int m = 0; m < 16; m++) z[m] = v[m];
       } else if (r == 1) {
-        // A = u dx w + v dy w (nonlin.c:62)
+        // A = u dx w + v dy w (nonlin.c:62).  Binary: A waits across the next
+        // transform in the group's (otherwise unused) shared real slot instead of
+        // in registers (at the 128-register bound of two CTAs per SM: spills 112 ->
+        // 40 bytes a thread, P2 -5% at 4096^2 FP32)
 #pragma unroll
-#ifdef CHNS_P2_KEEP_A
-        // binary: A stays in the group's (otherwise unused) shared real slot across
-        // the next transform instead of in registers
         for (int m = 0; m < 16; m++) {
           if (MODEL == MODEL_BINARY) keep[m] = dot2(z[m], v[m]);
           else a[m] = dot2(z[m], v[m]);
         }
-#else
-        for (int m = 0; m < 16; m++) a[m] = dot2(z[m], v[m]);
-#endif
         if (MODEL == MODEL_NS) {
           if (h == 0) {
 #pragma unroll
@@ -618,11 +615,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par
       } else if (r == 2) {
         // B1 = u dx c1 + v dy c1 (nonlin.c:207 / 292-293), stored with A
 #pragma unroll
-#ifdef CHNS_P2_KEEP_A
         for (int m = 0; m < 16; m++) v[m] = mk<R>(MODEL == MODEL_BINARY ? keep[m] : a[m], dot2(z[m], v[m]));
-#else
-        for (int m = 0; m < 16; m++) v[m] = mk<R>(a[m], dot2(z[m], v[m]));
-#endif
         dst = B.h[HAB]; stride = 2 * N; off = 2 * (i0 + h);
       } else {
         // B2 = u dx c2 + v dy c2 (nonlin.c:334-335) of x-rows i0, i1, transformed together
@@ -831,10 +824,6 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
   unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
-#ifdef CHNS_P3_STAGE_F
-  // F[f] (F[mu^F_i]) waits in shared memory between the mu transform and N_c
-  cx<R>* fs = reinterpret_cast<cx<R>*>(smem_raw) + GPC * FftShape<N>::SMEM + (size_t)g * N;
-#endif
   const int row = blockIdx.x * GPC + g;
   const bool live = row < NR;
   const int rowc = live ? row : 0;
@@ -863,10 +852,6 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
     if (MODEL == MODEL_BINARY) load_row<N>(f, B.h[HF], row, live, t);
     else load_row_pair<N>(f, B.h[HF], row, fld, live, t);
     fft<N, -1>(f, sh, t, TW);
-#ifdef CHNS_P3_STAGE_F
-#pragma unroll
-    for (int m = 0; m < 16; m++) fs[t + NT * m] = f[m];
-#endif
     load_row<N>(c, cst, row, live, t);
     if (do_mu) {
       // binary: mu = T[1.5 sigma eps k^2 c + 24 (sigma/eps) F[f]]   (surface_tension.c:45-46)
@@ -903,9 +888,6 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
       const int am = amask<N>(t, m);
       const R ks = ksq(kxm(m), ky);
       cx<R> nl;
-#ifdef CHNS_P3_STAGE_F
-      f[m] = fs[t + NT * m];
-#endif
       if (MODEL == MODEL_BINARY) {
         const R q = rmul(P.st24, ks);
         nl = mk<R>(rsub(-v[m].x, rmul(P.lam, rmul(q, f[m].x))), rsub(-v[m].y, rmul(P.lam, rmul(q, f[m].y))));

@@ -100,15 +100,8 @@ template <int N, class R> struct Sizes {
   static int grid_rows(int rows) { return (rows + GPC - 1) / GPC; }
 };
 
-// P3's shared memory: the transform buffers, plus (CHNS_P3_STAGE_F builds) one
-// spectrum per transform group kept between two of its transforms
-template <int N, class R> constexpr size_t p3_smem() {
-#ifdef CHNS_P3_STAGE_F
-  return Sizes<N, R>::FFT_SMEM + Sizes<N, R>::FRAG;
-#else
-  return Sizes<N, R>::FFT_SMEM;
-#endif
-}
+// P3's shared memory: the transform buffers
+template <int N, class R> constexpr size_t p3_smem() { return Sizes<N, R>::FFT_SMEM; }
 
 template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   using S = Sizes<N, R>;

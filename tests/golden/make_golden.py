@@ -8,10 +8,14 @@ oracle's FP64 FFT behind its FFTW calls.  They pin both the C restatement
 (oracle/chns_oracle.c) and, through it, the GPU path.
 
 Small grids store full spectral states; the two full-size configurations
-(binary 256^2 x 1000 steps, ternary 512^2 x 2000 steps) store a fingerprint of
-the final state (see fingerprint()).
+(binary 256^2 x 1000 steps, ternary 512^2 x 2000 steps) store the full final
+spectral state (1 MB and 6.3 MB) beside a fingerprint of it (see fingerprint());
+the big grids (4096^2, 1024^2) store only the fingerprint.
 
-Usage:  python tests/golden/make_golden.py [--full] [--big] [--init]  (--init: only init_ref.npz)
+The reference's source folder is taken from CHNS_REFERENCE_DIR (oracle/build_ref.py).
+
+Usage:  python tests/golden/make_golden.py [--full] [--big] [--init] [--only]
+  (--init: only init_ref.npz; --only: skip the small fixtures and init_ref.npz)
 """
 from __future__ import annotations
 
@@ -148,6 +152,8 @@ def make_full(O, cases=None):
         s1 = R.get_state()
         out = dict(params=json.dumps(p), steps=steps)
         for k, a in enumerate(s1):
+            if n <= 512:
+                out[f"final{k}"] = a
             fp = fingerprint(a)
             for key, v in fp.items():
                 out[f"final{k}_{key}"] = np.asarray(v)
@@ -178,7 +184,7 @@ if __name__ == "__main__":
     O.build_ref.build_all()
     if "--init" in sys.argv:
         make_init(O)
-    else:
+    elif "--only" not in sys.argv:
         make_small(O)
         make_init(O)
     if "--full" in sys.argv:

@@ -4,9 +4,7 @@ by reverse mode through a torch restatement of the reference step that is pinned
 the CPU against the C restatement (tests/test_oracle_adjoint.py).  The hand-written
 adjoint transposes the same operations, so it must agree to round-off rather than
 to the 1e-6 of central differences: J to 1e-12, the state and parameter gradients
-to 1e-9 relative L2.
-
-Opt-in (CHNS_ADJOINT_GOLDEN=1) until this comparison has been run on a B200."""
+to 1e-9 relative L2."""
 import json
 import os
 
@@ -15,9 +13,7 @@ import pytest
 
 from _golden import load_small, rel_l2
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(os.environ.get("CHNS_ADJOINT_GOLDEN") != "1",
-                                 reason="opt-in: CHNS_ADJOINT_GOLDEN=1 (not yet run on a B200)")]
+pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 

@@ -153,8 +153,10 @@ def test_phase_init_matches_reference(chns, name):
 @pytest.mark.parametrize("name,seed", [("bin256", 100), ("ter512", 101)])
 def test_baseline_configs_match_reference(chns, name, seed):
     """The binary 256^2 (1000 steps) and ternary 512^2 (2000 steps, dt = 5e-5)
-    spinodal runs against the reference's run: fingerprint (low modes, random
-    projections, norm) within 1e-10, mean concentration conserved to round-off."""
+    spinodal runs against the reference's run: every field (omega and each c_i)
+    within 1e-10 relative L2 of the reference's final state, its fingerprint (low
+    modes, random projections, norm) too, mean concentration conserved to
+    round-off."""
     g = load_full(name)
     p = g["params"]
     p1, p2, w = MG.initial_state(p["model"], p["nx"], p["lx"], seed, None, 0, 0)
@@ -164,6 +166,12 @@ def test_baseline_configs_match_reference(chns, name, seed):
         c.step(g["steps"])
         st = c.get_state()
     for k, a in enumerate(st):
+        ref_field = g[f"final{k}"]
+        if k == 0 and not np.any(ref_field):
+            assert not np.any(a), (name, "omega stays zero")
+        else:
+            err = rel_l2(a, ref_field)
+            assert err <= 1e-10, (name, k, err)
         fp = MG.fingerprint(a)
         ref = {key: g[f"final{k}_{key}"] for key in ("low", "proj", "norm")}
         err = MG.fingerprint_rel_err(ref, fp)
