@@ -41,9 +41,10 @@ enum { MODEL_NS = 0, MODEL_BINARY = 1, MODEL_TERNARY = 2 };
 // GCT truncated c (binary plain, ternary pair (c1,c2)); GMU mu (binary plain,
 // ternary pair (mu1, mu2)).  Every slot holds rows 0..jt of width 2n.
 enum { GUV = 0, GW, GD1, GD2, GCT, GMU, NG };
-// H slots: HAB pair (A, B1) = (u.grad w, u.grad c1) (pure Navier-Stokes: plain
-// A); HF binary plain f(c), ternary pair (mu^F_1, mu^F_2); HB2 plain
-// u.grad c2; HFF pair (Fx, Fy).  Every slot holds rows 0..n/2 of width 2n.
+// H slots: HAB ternary pair (A, B1) = (u.grad w, u.grad c1), binary plain A then
+// plain B1 behind it, pure Navier-Stokes plain A; HF binary plain f(c), ternary
+// pair (mu^F_1, mu^F_2); HB2 plain u.grad c2; HFF ternary pair (Fx, Fy), binary
+// plain Fx then plain Fy behind it.  Every slot holds rows 0..n/2 of width 2n.
 enum { HAB = 0, HF, HB2, HFF, NH };
 
 template <class R> struct Par {
@@ -507,8 +508,8 @@ template <class R> __device__ __forceinline__ R dot2(cx<R> f, cx<R> g) { return 
 
 // real frags per group of the row kernels (thread-private values kept across
 // transforms in shared memory)
-template <int MODEL> constexpr int row_adv_frags() { return 1; }
-template <int MODEL> constexpr int row_force_frags() { return MODEL == MODEL_TERNARY ? 2 : 0; }
+template <int MODEL> constexpr int row_adv_frags() { return MODEL == MODEL_BINARY ? 2 : 1; }
+template <int MODEL> constexpr int row_force_frags() { return 2; }
 
 // The row kernels run a fixed schedule of inverse y transforms as a loop with
 // one call site per transform direction (the unrolled transforms are long, so
@@ -517,7 +518,8 @@ template <int MODEL> constexpr int row_force_frags() { return MODEL == MODEL_TER
 // step it computes.
 
 // binary P2 schedule: 0 c_t (plain, x-rows i0, i1); then per x-row i:
-// 1 + 3h: (u, v); 2 + 3h: (dx w, dy w); 3 + 3h: (dx c, dy c)
+// 1 + 3h: (u, v); 2 + 3h: (dx w, dy w); 3 + 3h: (dx c, dy c); the forward
+// transforms of A and B run at 5 and 6 (both x-rows together)
 // ternary P2 schedule: 0, 1: (c1_t, c2_t) of x-rows i0, i1; then per x-row:
 // 2 + 4h: (u, v); 3 + 4h: (dx w, dy w); 4 + 4h: (dx c1, dy c1); 5 + 4h: (dx c2, dy c2)
 // pure Navier-Stokes P2 schedule: per x-row 2h: (u, v); 2h + 1: (dx w, dy w)
@@ -555,7 +557,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par
   const int pair = blockIdx.x * GPC + g;
   const bool live = pair < N / 2;
   const int i0 = 2 * pair;
-  Frag<N, R> keep{S.frag};
+  Frag<N, R> keep{S.frag}, keep2{S.frag + (size_t)N * GPC};
   cx<R> z[16], v[16];
   R a[16];
 
@@ -592,16 +594,27 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par
         // (u, v) of x-row i0 + h
 #pragma unroll
         for (int m = 0; m < 16; m++) z[m] = v[m];
-      } else if (r == 1) {
-        // A = u dx w + v dy w (nonlin.c:62).  Binary: A waits across the next
-        // transform in the group's (otherwise unused) shared real slot instead of
-        // in registers (at the 128-register bound of two CTAs per SM: spills 112 ->
-        // 40 bytes a thread, P2 -5% at 4096^2 FP32)
+      } else if (MODEL == MODEL_BINARY && r != 0) {
+        // binary: A = u dx w + v dy w (r = 1, nonlin.c:62) and B = u dx c + v dy c
+        // (r = 2, nonlin.c:207).  Those of x-row i0 wait in the group's shared real
+        // slots (not registers: at the 128-register bound of two CTAs per SM) until
+        // x-row i1's are formed; each field of the two x-rows is then transformed as
+        // one complex row and stored as a plain field, A at HAB, B behind it.  The
+        // group thus writes both halves of each 16-byte pair of x-rows at once, and
+        // P3 reads whole rows.
+        Frag<N, R>& kp = r == 1 ? keep : keep2;
+        if (h == 0) {
 #pragma unroll
-        for (int m = 0; m < 16; m++) {
-          if (MODEL == MODEL_BINARY) keep[m] = dot2(z[m], v[m]);
-          else a[m] = dot2(z[m], v[m]);
+          for (int m = 0; m < 16; m++) kp[m] = dot2(z[m], v[m]);
+        } else {
+#pragma unroll
+          for (int m = 0; m < 16; m++) v[m] = mk<R>(kp[m], dot2(z[m], v[m]));
+          dst = B.h[HAB] + (r == 1 ? 0 : (size_t)(N / 2 + 1) * N); stride = N; off = i0;
         }
+      } else if (r == 1) {
+        // A = u dx w + v dy w (nonlin.c:62)
+#pragma unroll
+        for (int m = 0; m < 16; m++) a[m] = dot2(z[m], v[m]);
         if (MODEL == MODEL_NS) {
           if (h == 0) {
 #pragma unroll
@@ -613,9 +626,9 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par
           }
         }
       } else if (r == 2) {
-        // B1 = u dx c1 + v dy c1 (nonlin.c:207 / 292-293), stored with A
+        // ternary: B1 = u dx c1 + v dy c1 (nonlin.c:292-293), stored with A as a pair field
 #pragma unroll
-        for (int m = 0; m < 16; m++) v[m] = mk<R>(MODEL == MODEL_BINARY ? keep[m] : a[m], dot2(z[m], v[m]));
+        for (int m = 0; m < 16; m++) v[m] = mk<R>(a[m], dot2(z[m], v[m]));
         dst = B.h[HAB]; stride = 2 * N; off = 2 * (i0 + h);
       } else {
         // B2 = u dx c2 + v dy c2 (nonlin.c:334-335) of x-rows i0, i1, transformed together
@@ -655,7 +668,8 @@ __device__ __forceinline__ RowSrc<R> force_src(const Bufs<R>& B, int it, int i0)
 template <int N, class R, int GPC, int MODEL>
 __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const Par<R> P, const __grid_constant__ TmaG T) {
   constexpr int NT = N / 16;
-  constexpr int STEPS = MODEL == MODEL_BINARY ? 3 : 6;
+  constexpr int NIN = MODEL == MODEL_BINARY ? 3 : 6;      // inverse transforms
+  constexpr int STEPS = MODEL == MODEL_BINARY ? 4 : 6;    // binary: a last step only stores
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
@@ -676,24 +690,44 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const P
   tile_start<N>(TL, T, S.tile, force_src<N, R, MODEL>(B, 0, i0), jt, live, t);
 #pragma unroll 1
   for (int it = 0; it < STEPS; it++) {
-    const bool more = it + 1 < STEPS;
-    row_c2r_loaded<N>(v, S.tile, TL, T, more, force_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t,
-                      S.sh, TW);
+    if (it < NIN) {
+      const bool more = it + 1 < NIN;
+      row_c2r_loaded<N>(v, S.tile, TL, T, more, force_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t,
+                        S.sh, TW);
+    }
     bool store = false;
-    int i = i0;
+    cx<R>* dst = B.h[HFF];
+    int stride = 2 * N, off = 2 * i0;
     if (MODEL == MODEL_BINARY) {
+      // tux *= nphi, tuy *= nphi (surface_tension.c:87-88).  Fx and Fy of x-row i0
+      // wait in the shared real slots until x-row i1's are formed; each is then
+      // transformed for both x-rows as one complex row and stored as a plain field
+      // (Fx at HFF, Fy behind it), so the group writes both halves of each 16-byte
+      // pair of x-rows at once and P5 reads whole rows.
       if (it == 0) {
 #pragma unroll
         for (int m = 0; m < 16; m++) a[m] = v[m];  // mu_t of x-rows i0, i1
-      } else {
-        // tux *= nphi, tuy *= nphi (surface_tension.c:87-88)
+      } else if (it == 1) {
 #pragma unroll
         for (int m = 0; m < 16; m++) {
-          const R mu = it == 1 ? a[m].x : a[m].y;
-          v[m] = mk<R>(rmul(v[m].x, mu), rmul(v[m].y, mu));
+          w1[m] = rmul(v[m].x, a[m].x);
+          w2[m] = rmul(v[m].y, a[m].x);
+        }
+      } else if (it == 2) {
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+          const R mu = a[m].y;
+          const R fx = rmul(v[m].x, mu), fy = rmul(v[m].y, mu);
+          v[m] = mk<R>(w1[m], fx);
+          a[m] = mk<R>(w2[m], fy);
         }
         store = true;
-        i = i0 + it - 1;
+        stride = N; off = i0;
+      } else {
+#pragma unroll
+        for (int m = 0; m < 16; m++) v[m] = a[m];
+        store = true;
+        dst = B.h[HFF] + (size_t)(N / 2 + 1) * N; stride = N; off = i0;
       }
     } else {
       const int h = it / 3, r = it % 3;
@@ -714,10 +748,10 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const P
           v[m] = mk<R>(radd(a[m].x, rmul(v[m].x, s)), radd(a[m].y, rmul(v[m].y, s)));
         }
         store = true;
-        i = i0 + h;
+        off = 2 * (i0 + h);
       }
     }
-    if (store) row_r2c_store<N>(v, B.h[HFF], 2 * N, 2 * i, live, t, S.sh, TW);  // CTA-uniform
+    if (store) row_r2c_store<N>(v, dst, stride, off, live, t, S.sh, TW);  // CTA-uniform
   }
 }
 
@@ -835,8 +869,9 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
   auto kxm = [&](int m) -> R { return (R)(P.fx * (double)sidx<N>(t + NT * m)); };
 
   cx<R> f[16], c[16], v[16];
-  // N_w partial = -F[u.grad w]   (nonlin.c:74, 92)
-  load_row_pair<N>(v, B.h[HAB], row, 0, live, t);
+  // N_w partial = -F[u.grad w]   (nonlin.c:74, 92); binary: the plain field at HAB
+  if (MODEL == MODEL_BINARY) load_row<N>(v, B.h[HAB], row, live, t);
+  else load_row_pair<N>(v, B.h[HAB], row, 0, live, t);
   fft<N, -1>(v, sh, t, TW);
 #pragma unroll
   for (int m = 0; m < 16; m++) v[m] = mk<R>(v[m].x * (R)(-1), v[m].y * (R)(-1));
@@ -880,7 +915,8 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
     }
     // N_c  binary: -F[u.grad c] - lambda (24 (sigma/eps) k^2) F[f]   (nonlin.c:240, 251)
     //      ternary: -F[u.grad c_i] - (lambda/gamma_i) k^2 F[mu^F_i]  (nonlin.c:369-370)
-    if (fld == 0) load_row_pair<N>(v, B.h[HAB], row, 1, live, t);
+    if (MODEL == MODEL_BINARY) load_row<N>(v, B.h[HAB] + (size_t)NR * N, row, live, t);
+    else if (fld == 0) load_row_pair<N>(v, B.h[HAB], row, 1, live, t);
     else load_row<N>(v, B.h[HB2], row, live, t);
     fft<N, -1>(v, sh, t, TW);
 #pragma unroll
@@ -929,7 +965,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
 // etd2rk.c:88-99 / 162-174.  Pure Navier-Stokes (CURL = false):
 // N_w = -F[u.grad w] (nonlin.c:74-101) from the plain field in HAB.
 // ---------------------------------------------------------------------------
-template <int N, class R, int GPC, bool CURL, int STAGE, bool S64>
+template <int N, class R, int GPC, bool CURL, int STAGE, bool S64, bool PLAINF = false>
 __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
@@ -951,9 +987,12 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
 
   cx<R> a[16], b[16];
   if constexpr (CURL) {
-    load_row_pair<N>(a, B.h[HFF], row, 0, live, t);
+    // the force: binary (PLAINF) Fx and Fy as plain fields, ternary a pair field
+    if (PLAINF) load_row<N>(a, B.h[HFF], row, live, t);
+    else load_row_pair<N>(a, B.h[HFF], row, 0, live, t);
     fft<N, -1>(a, sh, t, TW);
-    load_row_pair<N>(b, B.h[HFF], row, 1, live, t);
+    if (PLAINF) load_row<N>(b, B.h[HFF] + (size_t)NR * N, row, live, t);
+    else load_row_pair<N>(b, B.h[HFF], row, 1, live, t);
     fft<N, -1>(b, sh, t, TW);
     // N_w = N_w partial + I (kx F[Fy] - ky F[Fx])
 #pragma unroll

@@ -214,13 +214,14 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   launches++;
   mark(c, KIND_ROW_FORCE);
 
-  // P5: curl, N_w, ETD of w
-  if (stage == 1) {
-    auto k = s64 ? k_spec_curl_w<N, R, GPC, true, 1, F32> : k_spec_curl_w<N, R, GPC, true, 1, false>;
-    set_smem(k, S::FFT_SMEM);
-    k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
-  } else {
-    auto k = s64 ? k_spec_curl_w<N, R, GPC, true, 2, F32> : k_spec_curl_w<N, R, GPC, true, 2, false>;
+  // P5: curl, N_w, ETD of w (binary: the force as two plain fields)
+  {
+    const bool bin = model == CHNS_MODEL_BINARY;
+    auto k = stage == 1
+                 ? (s64 ? (bin ? k_spec_curl_w<N, R, GPC, true, 1, F32, true> : k_spec_curl_w<N, R, GPC, true, 1, F32>)
+                        : (bin ? k_spec_curl_w<N, R, GPC, true, 1, false, true> : k_spec_curl_w<N, R, GPC, true, 1, false>))
+                 : (s64 ? (bin ? k_spec_curl_w<N, R, GPC, true, 2, F32, true> : k_spec_curl_w<N, R, GPC, true, 2, F32>)
+                        : (bin ? k_spec_curl_w<N, R, GPC, true, 2, false, true> : k_spec_curl_w<N, R, GPC, true, 2, false>));
     set_smem(k, S::FFT_SMEM);
     k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
   }
