@@ -183,8 +183,17 @@ int chns_perimeter(chns_ctx *ctx, double *out);
  *   CHNS_INIT_W_ZERO           omega = 0 (ZERO_INIT, INIT_READ_DATA)
  *   CHNS_INIT_W_TAYLOR_GREEN   TG_INIT: u = amplitude (sin x cos y, -cos x sin y),
  *                              omega_hat = I (kx uy_hat - ky ux_hat), truncated
- * The reference's remaining branch (random-phase modes, init.c:98-180) draws from
- * a time-seeded rand() and is not provided.  Phase fields (init.c:229-292):
+ *   CHNS_INIT_W_SHELL          neither macro (init.c:102-182): velocity modes of
+ *                              amplitude uamp vk, vk^2 = k^4 e^{-2k^2} / (3 den(|k|))
+ *                              nx ny (den = modes per shell), projected by the
+ *                              p11/p12/p22 tensor, curl, truncation; amplitude =
+ *                              uamp (global.h:44).  The reference draws two
+ *                              time-seeded phases per mode but passes
+ *                              I 2 pi r to the real exp() of math.h (no tgmath.h),
+ *                              which takes the real part, 0: every phase factor is
+ *                              exactly 1, so the field is deterministic and is
+ *                              reproduced as compiled.
+ * Phase fields (init.c:229-292):
  *   CHNS_INIT_C_DROP    binary: c = (1 - tanh((r - pi/4.5) / (eps/2))) / 2, r the
  *                       distance to the box centre
  *   CHNS_INIT_C_NOISE   ternary: c_i = 1/4 + 0.001 rand()/RAND_MAX, two draws per
@@ -194,6 +203,7 @@ int chns_perimeter(chns_ctx *ctx, double *out);
  * chns_init_phase leaves omega unchanged; the other fields are replaced. */
 #define CHNS_INIT_W_ZERO 0
 #define CHNS_INIT_W_TAYLOR_GREEN 1
+#define CHNS_INIT_W_SHELL 2
 #define CHNS_INIT_C_DROP 0
 #define CHNS_INIT_C_NOISE 1
 int chns_init_vorticity(chns_ctx *ctx, int kind, double amplitude);

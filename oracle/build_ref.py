@@ -90,6 +90,11 @@ CONFIGS = {
     # binary with the reference defaults (L = 4 pi, eps = 3 dx), whose init also lays the drop
     "nstg32": dict(model=0, n=32, lx="(2.0*pi)", dt="(1e-3)", nu="(0.01)", init="tg"),
     "bintg64": dict(_BIN_DEF, n=64, init="tg"),
+    # the k-space shell initial vorticity (neither TG_INIT nor ZERO_INIT, init.c:102-182):
+    # pure NS at L = 2 pi, and binary with the reference defaults (L = 4 pi, whose
+    # half-integer wavenumbers put some |k| exactly half-way between two shells)
+    "nssh32": dict(model=0, n=32, lx="(2.0*pi)", dt="(1e-3)", nu="(0.01)", init="shell"),
+    "binsh64": dict(_BIN_DEF, n=64, init="shell"),
 }
 
 _SUBST = {  # macro name -> key in the config dict
@@ -112,7 +117,12 @@ def _gen_global_h(cfg: dict) -> str:
 
 
 def _gen_macro_h(cfg: dict) -> str:
-    lines = ["/* generated by oracle/build_ref.py */", "#define TG_INIT" if cfg.get("init") == "tg" else "#define ZERO_INIT"]
+    init = cfg.get("init")
+    lines = ["/* generated by oracle/build_ref.py */"]
+    if init == "tg":
+        lines.append("#define TG_INIT")
+    elif init != "shell":  # "shell": neither macro, init.c's k-space branch
+        lines.append("#define ZERO_INIT")
     if cfg["model"] == 1:
         lines.append("#define BINARY")
     elif cfg["model"] == 2:

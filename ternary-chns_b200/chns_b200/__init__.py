@@ -28,7 +28,7 @@ MODEL_NS, MODEL_BINARY, MODEL_TERNARY = 0, 1, 2
 FP64, FP32, FP32_STATE64 = 0, 1, 2
 COEF_REFERENCE, COEF_ACCURATE = 0, 1
 HOST, DEVICE = 0, 1
-INIT_W_ZERO, INIT_W_TAYLOR_GREEN = 0, 1
+INIT_W_ZERO, INIT_W_TAYLOR_GREEN, INIT_W_SHELL = 0, 1, 2
 INIT_C_DROP, INIT_C_NOISE = 0, 1
 
 STATUS = {0: "ok", -1: "bad argument", -2: "CUDA error", -3: "non-finite or blown-up state",

@@ -308,21 +308,23 @@ __device__ __forceinline__ void fft_last_stage(cx<R>* v, int t, const Tw<R>& tw)
 
 // Full transform of one group.  All threads of the CTA must call it together
 // (it uses __syncthreads); sh is this group's padded buffer of FftShape<N>::SMEM.
-// The leading barrier protects the buffer from the previous transform's readers.
-template <int N, int DIR, class R>
+// The leading barrier protects the buffer from the previous transform's readers;
+// LEAD = false drops it where the caller has just passed a barrier that every
+// earlier reader of the buffer had reached.
+template <int N, int DIR, class R, bool LEAD = true>
 __device__ __forceinline__ void fft(cx<R>* v, cx<R>* sh, int t, const Tw<R>& tw) {
   using S = FftShape<N>;
   if constexpr (S::N16 == 1 && S::R0 == 1) {
     fft_last_stage<N, DIR>(v, t, tw);  // N = 16: single stage
   } else {
     if constexpr (S::R0 > 1) {
-      __syncthreads();
+      if (LEAD) __syncthreads();
       fft_stage_to_smem<N, DIR, S::R0, 1>(v, sh, t, tw);
       __syncthreads();
       fft_load_smem<N>(v, sh, t);
     }
     if constexpr (S::N16 >= 2) {
-      __syncthreads();
+      if (LEAD || S::R0 > 1) __syncthreads();
       fft_stage_to_smem<N, DIR, 16, S::R0>(v, sh, t, tw);
       __syncthreads();
       fft_load_smem<N>(v, sh, t);

@@ -1,8 +1,8 @@
 // chns_init.cu -- the reference's initial conditions (init.c) on the device.
 //
-// Vorticity: zero (ZERO_INIT / INIT_READ_DATA, init.c:67-96) or the Taylor-Green
+// Vorticity: zero (ZERO_INIT / INIT_READ_DATA, init.c:67-96), the Taylor-Green
 // field (TG_INIT, init.c:38-65: u = a (sin x cos y, -cos x sin y), dfft, curl,
-// truncation).  Phase fields: the binary centred tanh drop (init.c:231-248) and
+// truncation) or the k-space shell field of the remaining branch (init.c:102-182).  Phase fields: the binary centred tanh drop (init.c:231-248) and
 // the ternary noise c_i = 1/4 + 0.001 r (init.c:264-292), each followed by dfft
 // and truncation as in init.c.  The noise draws are the C library's rand()
 // sequence after srand(seed) (the reference seeds 10 + 2 rank), produced on the
@@ -70,6 +70,62 @@ __global__ void k_init_curl(const chns::cx<R>* __restrict__ ux, const chns::cx<R
   w[idx] = chns::mk<R>(-im, re);
 }
 
+// init.c:102-128: modes per shell rint(|k|) (MPI_Allreduce over one rank), the
+// ky = 0 and ky = kymax columns counted once, the others twice (their conjugates)
+__global__ void k_shell_count(int* __restrict__ den, int n, int kmax, double fx, double fy, double kymax,
+                              int* __restrict__ err) {
+  const int nr = n / 2 + 1;
+  const size_t total = (size_t)n * nr;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / nr), j = (int)(idx % nr);  // FFTW layout: row i (kx), column j (ky)
+    const double kx = fx * (double)(i <= n / 2 ? i : i - n), ky = fy * (double)j;
+    const double ksqr = chns::radd(chns::rmul(kx, kx), chns::rmul(ky, ky));
+    const int ik = (int)rint(sqrt(ksqr));
+    if (ik < 0 || ik > kmax) { atomicOr(err, 1); continue; }
+    atomicAdd(&den[ik], (ky == 0.0 || ky == kymax) ? 1 : 2);
+  }
+}
+
+// init.c:130-181 per mode, into the S layout (row j = ky index, column i):
+// vk = sqrt(k^4 e^{-2 k^2} / (3 den[round |k|])) nx ny; v1 = v2 = uamp vk (the phase
+// factors exp(I 2 pi r) of init.c:156-157 go through the real exp() and are 1);
+// u_hat = P v with the projector of init.c:161-175; omega_hat = I (kx uy - ky ux).
+template <class R>
+__global__ void k_shell_omega(const int* __restrict__ den, chns::cx<R>* __restrict__ w, int n, double fx, double fy,
+                              double uamp, int* __restrict__ err) {
+  using namespace chns;
+  const size_t total = (size_t)(n / 2 + 1) * n;
+  const double ncube = (double)n * (double)n;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(idx / n), i = (int)(idx % n);
+    const double kx = fx * (double)(i <= n / 2 ? i : i - n), ky = fy * (double)j;
+    const double ksqr = radd(rmul(kx, kx), rmul(ky, ky));
+    const int ik = (int)round(sqrt(ksqr));
+    const double ee = rmul(rmul(ksqr, ksqr), exp(rmul(-2.0, ksqr)));
+    const int d = den[ik];
+    // an empty shell would make the reference reuse the previous mode's vk
+    if (d == 0) { atomicOr(err, 2); continue; }
+    const double vk = rmul(sqrt(rdiv(ee, rmul(3.0, (double)d))), ncube);
+    const double s = rmul(uamp, vk);
+    double p11, p22, p12;
+    if (ksqr > 1e-5) {
+      p11 = rsub(1.0, rdiv(rmul(kx, kx), ksqr));
+      p22 = rsub(1.0, rdiv(rmul(ky, ky), ksqr));
+      p12 = rdiv(rmul(-kx, ky), ksqr);
+    } else {
+      p11 = 1.0 / 2.0;
+      p22 = p11;
+      p12 = -1.0 / 2.0;
+    }
+    const double ux = radd(rmul(p11, s), rmul(p12, s));
+    const double uy = radd(rmul(p12, s), rmul(p22, s));
+    const double dr = rsub(rmul(kx, uy), rmul(ky, ux));  // curl.c:16-31; the imaginary parts are 0
+    w[idx] = mk<R>((R)0, (R)dr);
+  }
+}
+
 int grid_for(size_t nn) {
   const size_t b = (nn + 255) / 256;
   return (int)(b < 4096 ? b : 4096);
@@ -105,6 +161,27 @@ int chns_init_vorticity(chns_ctx* c, int kind, double amplitude) {
       k_init_curl<double><<<blocks, 256, 0, c->stream>>>((const chns::cx<double>*)uh[0],
                                                          (const chns::cx<double>*)uh[1],
                                                          (chns::cx<double>*)c->state[0], c->n, c->fx, c->fy);
+    c->L->truncate(c, c->state[0]);
+  } else if (kind == CHNS_INIT_W_SHELL) {
+    // the shell counts and an error word live in the context's real buffer
+    const double kxmax = (c->n / 2.0) * c->fx, kymax = (c->n / 2.0) * c->fy;
+    const int kmax = (int)round(sqrt(kxmax * kxmax + kymax * kymax));
+    if ((size_t)(kmax + 2) * sizeof(int) > (size_t)c->n * c->n * c->rsz || !c->realbuf) return CHNS_ERR_UNSUPPORTED;
+    int* den = (int*)c->realbuf;
+    int* err = den + kmax + 1;
+    IK(cudaMemsetAsync(den, 0, (size_t)(kmax + 2) * sizeof(int), c->stream));
+    const size_t modes = (size_t)c->n * c->nr;
+    k_shell_count<<<grid_for(modes), 256, 0, c->stream>>>(den, c->n, kmax, c->fx, c->fy, kymax, err);
+    if (c->f32)
+      k_shell_omega<float><<<grid_for(modes), 256, 0, c->stream>>>(den, (chns::cx<float>*)c->state[0], c->n, c->fx,
+                                                                   c->fy, amplitude, err);
+    else
+      k_shell_omega<double><<<grid_for(modes), 256, 0, c->stream>>>(den, (chns::cx<double>*)c->state[0], c->n,
+                                                                    c->fx, c->fy, amplitude, err);
+    int herr = 0;
+    IK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    IK(cudaStreamSynchronize(c->stream));
+    if (herr) return CHNS_ERR_UNSUPPORTED;
     c->L->truncate(c, c->state[0]);
   } else {
     return CHNS_ERR_ARG;

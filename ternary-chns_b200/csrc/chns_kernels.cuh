@@ -229,17 +229,52 @@ __device__ __forceinline__ void tile_wait(TileLoader<R>& L, const TmaG& T, bool 
   }
 }
 
-// row_c2r_tiled with the row kernels' tile loader (TMA or cp.async)
+// build_c2r_input for the reference's cut with a square box (jt = N/4, known at
+// compile time): the rows that can be nonzero are fixed per slot m, so no slot
+// tests jt or chooses between a row and its conjugate at run time.  Slots 0..3
+// read rows k = t + NT m < N/4; slot 4 only row N/4 (t = 0); slots 5..11 lie
+// beyond the cut on both sides (zero); slots 12..15 are the conjugates of rows
+// N - k in 1..N/4.  Only row 0 (t = 0, m = 0) has its imaginary part dropped.
 template <int N, class R>
+__device__ __forceinline__ void build_c2r_input_q(cx<R>* v, const cx<R>* tile, int t) {
+  constexpr int NT = N / 16;
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    if (m >= 5 && m <= 11) {
+      v[m] = czero<R>();
+      continue;
+    }
+    const int k = t + NT * m;
+    const int kk = m >= 12 ? N - k : k;
+    cx<R> a, b;
+    if (m == 4 && t != 0) {
+      a = czero<R>();
+      b = czero<R>();
+    } else {
+      a = tile[2 * kk];
+      b = tile[2 * kk + 1];
+    }
+    if (m == 0 && t == 0) { a.y = (R)0; b.y = (R)0; }
+    v[m] = m >= 12 ? mk<R>(a.x + b.y, b.x - a.y) : mk<R>(a.x - b.y, a.y + b.x);
+  }
+}
+
+// row_c2r_tiled with the row kernels' tile loader (TMA or cp.async).  With TMA
+// every thread has waited on the tile's mbarrier itself, so the tile needs no
+// barrier before it is read; the barrier after the reads (before the next copy
+// may overwrite the tile) also serves as the transform's leading barrier.
+// JT4: the context's cut is the reference's square-box one (jt = N/4).
+template <int N, class R, bool JT4 = false>
 __device__ __forceinline__ void row_c2r_loaded(cx<R>* v, cx<R>* tile, TileLoader<R>& L, const TmaG& T,
                                                bool has_next, RowSrc<R> next, int jt, bool live, int t, cx<R>* sh,
                                                const Tw<R>& tw) {
   tile_wait(L, T, live);
-  __syncthreads();
-  build_c2r_input<N>(v, tile, jt, t);
+  if (!L.tma) __syncthreads();
+  if (JT4) build_c2r_input_q<N>(v, tile, t);
+  else build_c2r_input<N>(v, tile, jt, t);
   __syncthreads();
   if (has_next) tile_start<N>(L, T, tile, next, jt, live, t);
-  fft<N, +1>(v, sh, t, tw);
+  fft<N, +1, R, false>(v, sh, t, tw);
 }
 
 // Inverse y transform of the input already in flight to `tile`; issues the
@@ -541,7 +576,7 @@ __device__ __forceinline__ RowSrc<R> adv_src(const Bufs<R>& B, int it, int i0) {
   return RowSrc<R>{B.g[slot], 2 * N, 2 * (i0 + h), 2 * slot};
 }
 
-template <int N, class R, int GPC, int MODEL>
+template <int N, class R, int GPC, int MODEL, bool JT4 = false>
 __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par<R> P, const __grid_constant__ TmaG T) {
   using Sc = AdvSchedule<MODEL>;
   constexpr int NT = N / 16;
@@ -568,8 +603,8 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par
 #pragma unroll 1
   for (int it = 0; it < Sc::STEPS; it++) {
     const bool more = it + 1 < Sc::STEPS;
-    row_c2r_loaded<N>(v, S.tile, TL, T, more, adv_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t, S.sh,
-                      TW);
+    row_c2r_loaded<N, R, JT4>(v, S.tile, TL, T, more, adv_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t,
+                              S.sh, TW);
     cx<R>* dst = nullptr;
     int stride = 0, off = 0;
     if (it < Sc::PRE) {
@@ -665,7 +700,7 @@ __device__ __forceinline__ RowSrc<R> force_src(const Bufs<R>& B, int it, int i0)
   return RowSrc<R>{B.g[slot], 2 * N, 2 * (i0 + h), 2 * slot};
 }
 
-template <int N, class R, int GPC, int MODEL>
+template <int N, class R, int GPC, int MODEL, bool JT4 = false>
 __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const Par<R> P, const __grid_constant__ TmaG T) {
   constexpr int NT = N / 16;
   constexpr int NIN = MODEL == MODEL_BINARY ? 3 : 6;      // inverse transforms
@@ -692,8 +727,8 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const P
   for (int it = 0; it < STEPS; it++) {
     if (it < NIN) {
       const bool more = it + 1 < NIN;
-      row_c2r_loaded<N>(v, S.tile, TL, T, more, force_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live, t,
-                        S.sh, TW);
+      row_c2r_loaded<N, R, JT4>(v, S.tile, TL, T, more, force_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live,
+                                t, S.sh, TW);
     }
     bool store = false;
     cx<R>* dst = B.h[HFF];

@@ -139,19 +139,21 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   launches++;
   mark(c, KIND_SPEC_INV);
 
-  // P2: advection products (+ chemical potential)
+  // P2: advection products (+ chemical potential).  The reference's cut on a
+  // square box (jt = N/4) has row kernels whose tile reads are fixed at compile time.
+  const bool jt4 = jt == N / 4;
   if (model == CHNS_MODEL_NS) {
-    auto k = k_row_adv<N, R, GPC, MODEL_NS>;
+    auto k = jt4 ? k_row_adv<N, R, GPC, MODEL_NS, true> : k_row_adv<N, R, GPC, MODEL_NS>;
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_NS>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   } else if (model == CHNS_MODEL_BINARY) {
-    auto k = k_row_adv<N, R, GPC, MODEL_BINARY>;
+    auto k = jt4 ? k_row_adv<N, R, GPC, MODEL_BINARY, true> : k_row_adv<N, R, GPC, MODEL_BINARY>;
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_BINARY>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   } else {
-    auto k = k_row_adv<N, R, GPC, MODEL_TERNARY>;
+    auto k = jt4 ? k_row_adv<N, R, GPC, MODEL_TERNARY, true> : k_row_adv<N, R, GPC, MODEL_TERNARY>;
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_TERNARY>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
@@ -201,12 +203,12 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
 
   // P4: surface-tension force
   if (model == CHNS_MODEL_BINARY) {
-    auto k = k_row_force<N, R, GPC, MODEL_BINARY>;
+    auto k = jt4 ? k_row_force<N, R, GPC, MODEL_BINARY, true> : k_row_force<N, R, GPC, MODEL_BINARY>;
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_force_frags<MODEL_BINARY>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   } else {
-    auto k = k_row_force<N, R, GPC, MODEL_TERNARY>;
+    auto k = jt4 ? k_row_force<N, R, GPC, MODEL_TERNARY, true> : k_row_force<N, R, GPC, MODEL_TERNARY>;
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_force_frags<MODEL_TERNARY>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);

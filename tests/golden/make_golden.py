@@ -163,8 +163,9 @@ def make_full(O, cases=None):
 
 
 # the reference's own init() (init.c) on configurations whose macros select each branch:
-# ZERO_INIT vorticity with the binary drop / ternary srand(10) noise, and TG_INIT
-INIT_CONFIGS = ["bin32", "ter32", "bindef64", "terdef64", "nstg32", "bintg64"]
+# ZERO_INIT vorticity with the binary drop / ternary srand(10) noise, TG_INIT, and the
+# k-space shell vorticity (neither macro)
+INIT_CONFIGS = ["bin32", "ter32", "bindef64", "terdef64", "nstg32", "bintg64", "nssh32", "binsh64"]
 
 
 def make_init(O):

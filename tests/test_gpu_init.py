@@ -1,6 +1,7 @@
 """init.c on the device (chns_init_vorticity / chns_init_phase) against the
 reference's own init() (tests/golden/init_ref.npz: ZERO_INIT vorticity with the
-binary drop and the ternary srand(10) noise, and TG_INIT).  FP64 relative L2
+binary drop and the ternary srand(10) noise, TG_INIT, and the k-space shell
+vorticity of the branch selected by neither macro).  FP64 relative L2
 <= 1e-13 (the GPU's tanh, sin and cos and the FFT differ from the host's in the
 last bits); FP32 contexts <= 1e-6."""
 import json
@@ -15,7 +16,7 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = {  # name: (vorticity kind, phase kind or None)
     "bin32": (0, 0), "ter32": (0, 1), "bindef64": (0, 0), "terdef64": (0, 1), "nstg32": (1, None),
-    "bintg64": (1, 0),
+    "bintg64": (1, 0), "nssh32": (2, None), "binsh64": (2, 0),
 }
 
 
