@@ -280,6 +280,33 @@ int chns_profile_step(chns_ctx *ctx, int reps, float *ms, int *kind, int maxk);
 
 const char *chns_status_string(int status);
 
+/* Slab-decomposed transforms over several GPUs: fft.c:11-31 as the reference
+ * runs it under FFTW-MPI (plans main.c:193-194, slabs main.c:43-46).  Rank r of
+ * P holds local_nx = n / P x-rows of the real field (row stride real_stride
+ * doubles, >= n; the reference's in-place rows are n + 2) and the same kx-rows
+ * of the spectrum in FFTW layout (local_nx x (n/2+1) complex doubles).  A
+ * transform is three local phases with an all-to-all exchange of equal blocks
+ * (exchange_complex / P complex doubles per peer) between consecutive phases,
+ * issued by the caller (NCCL all-to-all, or any other):
+ *   dfft: chns_slab_dfft_y, exchange, chns_slab_dfft_x, exchange, chns_slab_dfft_unpack
+ *   ifft: chns_slab_ifft_pack, exchange, chns_slab_ifft_x, exchange, chns_slab_ifft_y
+ * dfft is unnormalised; ifft includes the reference's 1/(nx ny) and writes only
+ * the n reals of each row.  Every pointer is a DEVICE pointer of this rank's
+ * GPU; a phase writes its second buffer (send, spec or real) and reads its
+ * first; work is enqueued on `stream` (a cudaStream_t).  n is a power of two,
+ * 32 <= n <= 4096, n divisible by P with local_nx even.  FP64, as the reference.
+ * chns_slab_create allocates the plan's twiddle table on the current device. */
+typedef struct chns_slab chns_slab;
+int chns_slab_create(int n, int nranks, int rank, chns_slab **out);
+void chns_slab_destroy(chns_slab *s);
+int chns_slab_sizes(const chns_slab *s, int *local_nx, int *rows_per_rank, size_t *exchange_complex);
+int chns_slab_dfft_y(const chns_slab *s, const double *real, size_t real_stride, double *send, void *stream);
+int chns_slab_dfft_x(const chns_slab *s, const double *recv, double *send, void *stream);
+int chns_slab_dfft_unpack(const chns_slab *s, const double *recv, double *spec, void *stream);
+int chns_slab_ifft_pack(const chns_slab *s, const double *spec, double *send, void *stream);
+int chns_slab_ifft_x(const chns_slab *s, const double *recv, double *send, void *stream);
+int chns_slab_ifft_y(const chns_slab *s, const double *recv, double *real, size_t real_stride, void *stream);
+
 /* Largest grid of chns_dfft_noalloc. */
 #define CHNS_NOALLOC_MAX_N 512
 

@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_diag_spec(const Bufs<R> B, c
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
-  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = blockIdx.x * GPC + g;
   const bool live = row < NR;
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_diag_row(const Bufs<R> B, co
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
-  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int pair = blockIdx.x * GPC + g;
   const bool live = pair < N / 2;

@@ -218,44 +218,59 @@ __device__ __forceinline__ void apply_tw16(cx<R>* u, const cx<R>* __restrict__ t
   for (int r = 1; r < 16; r++) u[r] = DIR < 0 ? cmul(u[r], w[r]) : cmulc(u[r], w[r]);
 }
 
-// Twiddles of the two twiddled stages of a transform, precomputed once per
-// thread and kept in shared memory: slot 0 serves the first twiddled radix-16
-// stage (span R0 when R0 > 1, else span 16 when there are three radix-16
-// stages), slot 1 the last stage (span N/16).  Element (slot, q) of thread tid
-// holds w^(2^q), q = 0..3, at p[(4 slot + q) * stride] with p = base + tid.
+// Twiddles of the two twiddled stages of a transform, precomputed once per CTA
+// and kept in shared memory.  Slot 0 serves the first twiddled radix-16 stage
+// (span R0 when R0 > 1, else span 16 when there are three radix-16 stages): its
+// base depends only on t mod that span, so it is one table of (at most) 16
+// bases x 4 powers shared by the CTA, element (b, q) = w_b^(2^q) at table[4 b + q];
+// thread t reads p0[q], p0 = table + 4 (t mod span).  Slot 1 serves the last stage (span
+// N/16, base t): thread tid's w^(2^q), q = 0..3, at p1[q * stride], p1 = table
+// + 64 + tid.  Slot 0 is first read after the transform's first exchange
+// barrier, so its fill needs no barrier of its own.
 template <class R> struct Tw {
-  const cx<R>* p;
+  const cx<R>* p0;
+  const cx<R>* p1;
   int stride;
 };
 
-template <int N, class R> constexpr size_t tw_smem_per_thread() { return 8 * sizeof(cx<R>); }
+// bytes of the twiddle region of a CTA of `threads` threads
+template <int N, class R> __host__ __device__ constexpr size_t tw_smem_bytes(int threads) {
+  return (size_t)(64 + 4 * threads) * sizeof(cx<R>);
+}
 
-// Fills this thread's slots from the table tw[q] = exp(-2 pi i q / N).
+// Fills the CTA's twiddle region from the table tw[q] = exp(-2 pi i q / N)
+// (every thread of the CTA calls it).
 template <int N, class R>
 __device__ __forceinline__ Tw<R> tw_setup(cx<R>* smem, const cx<R>* __restrict__ tw, int t) {
   constexpr int NT = N / 16;
   constexpr int LOGN = ilog2c(N);
   constexpr int R0 = 1 << (LOGN % 4);
   constexpr int N16 = LOGN / 4;
+  constexpr bool SLOT0 = (R0 > 1 && N16 >= 2) || N16 >= 3;
+  constexpr int SPAN0 = R0 > 1 ? R0 : 16;                       // distinct slot-0 bases
+  constexpr int STEP0 = R0 > 1 ? N / (R0 * 16) : N / 256;       // base b is tw[b STEP0]
   const int tid = threadIdx.x, stride = blockDim.x;
-  int base0 = -1;
-  if (R0 > 1 && N16 >= 2) base0 = (t % R0) * (N / (R0 * 16));
-  else if (N16 >= 3) base0 = (t % 16) * (N / 256);
-  const int base1 = NT > 1 ? t : -1;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    if (base0 >= 0) smem[(0 * 4 + q) * stride + tid] = tw[(base0 << q) & (N - 1)];
-    if (base1 >= 0) smem[(1 * 4 + q) * stride + tid] = tw[(base1 << q) & (N - 1)];
+  if (SLOT0) {
+    for (int e = tid; e < 4 * SPAN0; e += stride) smem[e] = tw[(((e / 4) * STEP0) << (e % 4)) & (N - 1)];
   }
-  return Tw<R>{smem + tid, stride};
+  cx<R>* p1 = smem + 64 + tid;
+  if (NT > 1) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) p1[q * stride] = tw[(t << q) & (N - 1)];
+  }
+  return Tw<R>{smem + 4 * (t % SPAN0), p1, stride};
 }
 
 // Multiplies u[r], r = 1..15, by w^r (conj for the inverse) from the
 // precomputed w, w^2, w^4, w^8 of `slot`; other powers by at most two products.
 template <int DIR, class R>
 __device__ __forceinline__ void apply_tw16_pre(cx<R>* u, const Tw<R>& T, int slot) {
-  const cx<R> w1 = T.p[(4 * slot + 0) * T.stride], w2 = T.p[(4 * slot + 1) * T.stride];
-  const cx<R> w4 = T.p[(4 * slot + 2) * T.stride], w8 = T.p[(4 * slot + 3) * T.stride];
+  cx<R> w1, w2, w4, w8;
+  if (slot == 0) {
+    w1 = T.p0[0]; w2 = T.p0[1]; w4 = T.p0[2]; w8 = T.p0[3];
+  } else {
+    w1 = T.p1[0]; w2 = T.p1[T.stride]; w4 = T.p1[2 * T.stride]; w8 = T.p1[3 * T.stride];
+  }
   const cx<R> w3 = cmul(w1, w2), w12 = cmul(w8, w4);
   cx<R> w[16];
   w[1] = w1; w[2] = w2; w[3] = w3; w[4] = w4;

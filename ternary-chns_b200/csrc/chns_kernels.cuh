@@ -63,6 +63,7 @@ template <class R> struct Par {
                            // double-float state, slots 0 and 3 hold e - 1 (expm1) instead of e
   const cx<R>* tw;         // tw[q] = exp(-2 pi i q / n)
   double* k0;              // FP32 only: k = 0 modes in double [w, c1, c2, sw, s1, s2] x (re, im)
+  unsigned int* err;       // bit 0: a bounded wait for an asynchronous copy ran out
 };
 
 template <class R> struct Bufs {
@@ -199,6 +200,59 @@ static __device__ __forceinline__ void tma_tile(void* tile, const TmaG& T, int m
         : "memory");
 }
 
+// One contiguous block (bytes a multiple of 16, both addresses 16-byte aligned)
+// into shared memory by the bulk-copy engine, completing on mb; one thread
+// issues it.  The fence orders the block's earlier generic-proxy reads (made
+// before the barrier that precedes this call) before the asynchronous write.
+static __device__ __forceinline__ void bulk_copy(void* smem, const void* gmem, unsigned bytes, uint64_t* mb) {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mb)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(smem)),
+               "l"(gmem), "r"(bytes), "r"(smem_u32(mb))
+               : "memory");
+}
+
+// Two row buffers of a spectral pass, each refilled by bulk copy while the
+// group transforms what it read from the other: the copy of the next input row
+// is in flight during a transform instead of its load latency following it.
+// Every wait is bounded; one that runs out sets bit 0 of *err.
+template <class R> struct RowPrefetch {
+  cx<R>* buf[2];
+  uint64_t* mb;
+  unsigned par[2];
+  unsigned int* err;
+  bool issuer, live;
+  __device__ __forceinline__ void start(int b, const cx<R>* row, int n) {
+    if (issuer && live) bulk_copy(buf[b], row, (unsigned)(n * sizeof(cx<R>)), mb + b);
+  }
+  __device__ __forceinline__ void wait(int b) {
+    if (live && !mbar_wait(mb + b, par[b])) atomicOr(err, 1u);
+    par[b] ^= 1u;
+  }
+  template <int N> __device__ __forceinline__ void read(int b, cx<R>* v, int t) const {
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = buf[b][t + (N / 16) * m];
+  }
+};
+
+// Row buffers of the prefetching spectral passes (binary P3 / P5 in FP32): two
+// rows of N complex per group, then their mbarriers.
+template <int N, class R, int GPC> __host__ __device__ constexpr size_t prefetch_smem() {
+  return (size_t)GPC * 2 * N * sizeof(cx<R>) + (size_t)GPC * 2 * sizeof(uint64_t);
+}
+template <int N, class R, int GPC>
+__device__ __forceinline__ RowPrefetch<R> prefetch_setup(unsigned char* raw, int g, int t, bool live,
+                                                         unsigned int* err) {
+  cx<R>* pf = reinterpret_cast<cx<R>*>(raw);
+  uint64_t* mb = reinterpret_cast<uint64_t*>(raw + (size_t)GPC * 2 * N * sizeof(cx<R>)) + 2 * g;
+  if (t == 0) {
+    mbar_init(mb);
+    mbar_init(mb + 1);
+  }
+  return RowPrefetch<R>{{pf + (size_t)(2 * g) * N, pf + (size_t)(2 * g + 1) * N}, mb, {0u, 0u}, err, t == 0, live};
+}
+
 // Tile state of a row kernel: TMA (contexts with tensor maps) or cp.async.
 template <class R> struct TileLoader {
   bool tma;
@@ -286,12 +340,12 @@ __device__ __forceinline__ void row_c2r_tiled(cx<R>* v, cx<R>* tile, bool has_ne
   cp_async_wait_all();
   __syncthreads();
   build_c2r_input<N>(v, tile, jt, t);
-  __syncthreads();
+  __syncthreads();  // also the transform's leading barrier
   if (has_next) {
     tile_issue<N>(tile, next, jt, live, t);
     cp_async_commit();
   }
-  fft<N, +1>(v, sh, t, tw);
+  fft<N, +1, R, false>(v, sh, t, tw);
 }
 
 // two adjacent complex values (one 16-byte access in FP32)
@@ -436,7 +490,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_inv(const Bufs<R> B, const Pa
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
-  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = blockIdx.x * GPC + g;
   const bool live = row <= P.jt;
@@ -461,26 +515,37 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_inv(const Bufs<R> B, const Pa
   // (blockIdx.y), half the transforms each: twice the CTAs for rows too few to
   // fill the GPU (measured: 5-8% more steps/s at 256^2-1024^2; at 4096^2 the
   // second read of the input row costs more than it gains).
+  // The vorticity's outputs run in the order dx w, dy w, u, v so that w can be
+  // turned into psi = w / k^2 in place once (velocity.c:12-42) for both u and v.
   constexpr int NOUT = MODEL == MODEL_NS ? 4 : (MODEL == MODEL_BINARY ? 7 : 10);
   constexpr int OSPLIT = spec_inv_split<N>() ? (MODEL == MODEL_NS ? 2 : (MODEL == MODEL_BINARY ? 3 : 4)) : NOUT;
   const int obeg = blockIdx.y == 0 ? 0 : OSPLIT, oend = blockIdx.y == 0 ? OSPLIT : NOUT;
+  bool loaded = false;
 #pragma unroll 1
-  for (int o = obeg; o < oend; o++) {
+  for (int idx = 0; idx < NOUT; idx++) {
+    const int o = idx < 4 ? (idx + 2) % 4 : idx;  // 2, 3, 0, 1, 4, 5, ...
+    if (o < obeg || o >= oend) continue;
     if (o == 6 || o == 9) continue;  // dy c: stored with c_t
-    if (o == obeg || o == 4 || o == 7) {
+    if (!loaded || o == 4 || o == 7) {
       const cx<R>* src = o < 4 ? B.w : (o < 7 ? B.c1 : B.c2);
 #pragma unroll
       for (int m = 0; m < 16; m++)
         in[m] = ((inmask >> m) & 1) ? src[(size_t)row * N + t + NT * m] : czero<R>();
+      loaded = true;
     }
     const int q = o < 4 ? o : 4 + (o - 4) % 3;  // 0 u, 1 v, 2 dx, 3 dy (w); 4 c_t, 5 dx, 6 dy (c)
     if (q < 2) {
-      // u = I ky psi, v = -I kx psi, psi = w / k^2
+      // u = I ky psi, v = -I kx psi, psi = w / k^2 (0 where k^2 <= 1e-12)
+      if (q == 0) {
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+          const R ks = ksq(kxm(m), ky);
+          in[m] = ks > (R)1e-12 ? mk<R>(rdiv(in[m].x, ks), rdiv(in[m].y, ks)) : czero<R>();
+        }
+      }
 #pragma unroll
       for (int m = 0; m < 16; m++) {
-        const R kx = kxm(m), ks = ksq(kx, ky);
-        R a = (R)0, b = (R)0;
-        if (ks > (R)1e-12) { a = rdiv(in[m].x, ks); b = rdiv(in[m].y, ks); }
+        const R kx = kxm(m), a = in[m].x, b = in[m].y;
         v[m] = q == 0 ? mk<R>(-rmul(ky, b) * sc, rmul(ky, a) * sc) : mk<R>(rmul(kx, b) * sc, -rmul(kx, a) * sc);
       }
     } else if (q == 4) {
@@ -583,7 +648,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
-  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   const bool tma = tma_tiles_ok<N, R, GPC>(T, smem_raw);  // CTA-uniform
   if (tma) smem_raw = align128(smem_raw);
   const int jt = P.jt;
@@ -708,7 +773,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const P
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
-  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   const bool tma = tma_tiles_ok<N, R, GPC>(T, smem_raw);  // CTA-uniform
   if (tma) smem_raw = align128(smem_raw);
   const int jt = P.jt;
@@ -891,7 +956,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
-  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = blockIdx.x * GPC + g;
   const bool live = row < NR;
@@ -904,10 +969,26 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
   auto kxm = [&](int m) -> R { return (R)(P.fx * (double)sidx<N>(t + NT * m)); };
 
   cx<R> f[16], c[16], v[16];
+  // binary FP32: u.grad w, f(c), the state row and u.grad c come by bulk copy
+  // into two row buffers, each copy in flight during the preceding transform
+  constexpr bool PF = MODEL == MODEL_BINARY && F32;
+  RowPrefetch<R> RP{};
   // N_w partial = -F[u.grad w]   (nonlin.c:74, 92); binary: the plain field at HAB
-  if (MODEL == MODEL_BINARY) load_row<N>(v, B.h[HAB], row, live, t);
-  else load_row_pair<N>(v, B.h[HAB], row, 0, live, t);
-  fft<N, -1>(v, sh, t, TW);
+  if constexpr (PF) {
+    RP = prefetch_setup<N, R, GPC>(smem_raw + (size_t)GPC * FftShape<N>::SMEM * sizeof(cx<R>), g, t, live, P.err);
+    __syncthreads();
+    RP.start(0, B.h[HAB] + (size_t)rowc * N, N);
+    RP.start(1, B.h[HF] + (size_t)rowc * N, N);
+    RP.wait(0);
+    RP.template read<N>(0, v, t);
+    __syncthreads();  // buffer 0 read by the whole group; also the transform's leading barrier
+    RP.start(0, B.c1 + (size_t)rowc * N, N);
+    fft<N, -1, R, false>(v, sh, t, TW);
+  } else {
+    if (MODEL == MODEL_BINARY) load_row<N>(v, B.h[HAB], row, live, t);
+    else load_row_pair<N>(v, B.h[HAB], row, 0, live, t);
+    fft<N, -1>(v, sh, t, TW);
+  }
 #pragma unroll
   for (int m = 0; m < 16; m++) v[m] = mk<R>(v[m].x * (R)(-1), v[m].y * (R)(-1));
   store_row<N>(v, B.nw, row, live, t);
@@ -919,10 +1000,20 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
     cx<R>* cx_out = fld == 0 ? B.x1 : B.x2;
     cx<R>* __restrict__ clo = B.lo[1 + fld];
     // F[f(c)] (binary) or F[mu^F_i] (ternary)
-    if (MODEL == MODEL_BINARY) load_row<N>(f, B.h[HF], row, live, t);
-    else load_row_pair<N>(f, B.h[HF], row, fld, live, t);
-    fft<N, -1>(f, sh, t, TW);
-    load_row<N>(c, cst, row, live, t);
+    if constexpr (PF) {
+      RP.wait(1);
+      RP.template read<N>(1, f, t);
+      __syncthreads();
+      RP.start(1, B.h[HAB] + (size_t)NR * N + (size_t)rowc * N, N);
+      fft<N, -1, R, false>(f, sh, t, TW);
+      RP.wait(0);
+      RP.template read<N>(0, c, t);
+    } else {
+      if (MODEL == MODEL_BINARY) load_row<N>(f, B.h[HF], row, live, t);
+      else load_row_pair<N>(f, B.h[HF], row, fld, live, t);
+      fft<N, -1>(f, sh, t, TW);
+      load_row<N>(c, cst, row, live, t);
+    }
     if (do_mu) {
       // binary: mu = T[1.5 sigma eps k^2 c + 24 (sigma/eps) F[f]]   (surface_tension.c:45-46)
       // ternary: mu_i = T[F[mu^F_i] + 0.75 gamma_i eps k^2 c_i]     (surface_tension.c:116-128)
@@ -950,7 +1041,10 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
     }
     // N_c  binary: -F[u.grad c] - lambda (24 (sigma/eps) k^2) F[f]   (nonlin.c:240, 251)
     //      ternary: -F[u.grad c_i] - (lambda/gamma_i) k^2 F[mu^F_i]  (nonlin.c:369-370)
-    if (MODEL == MODEL_BINARY) load_row<N>(v, B.h[HAB] + (size_t)NR * N, row, live, t);
+    if constexpr (PF) {
+      RP.wait(1);
+      RP.template read<N>(1, v, t);
+    } else if (MODEL == MODEL_BINARY) load_row<N>(v, B.h[HAB] + (size_t)NR * N, row, live, t);
     else if (fld == 0) load_row_pair<N>(v, B.h[HAB], row, 1, live, t);
     else load_row<N>(v, B.h[HB2], row, live, t);
     fft<N, -1>(v, sh, t, TW);
@@ -1008,7 +1102,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
-  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = blockIdx.x * GPC + g;
   const bool live = row < NR;
@@ -1021,7 +1115,36 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
   auto kxm = [&](int m) -> R { return (R)(P.fx * (double)sidx<N>(t + NT * m)); };
 
   cx<R> a[16], b[16];
-  if constexpr (CURL) {
+  // binary FP32: Fx, Fy, the partial N_w and the state row come by bulk copy
+  // into two row buffers, each copy in flight during the preceding transform
+  constexpr bool PF = CURL && PLAINF && F32;
+  RowPrefetch<R> RP{};
+  if constexpr (PF) {
+    RP = prefetch_setup<N, R, GPC>(smem_raw + (size_t)GPC * FftShape<N>::SMEM * sizeof(cx<R>), g, t, live, P.err);
+    __syncthreads();
+    RP.start(0, B.h[HFF] + (size_t)rowc * N, N);
+    RP.start(1, B.h[HFF] + (size_t)NR * N + (size_t)rowc * N, N);
+    RP.wait(0);
+    RP.template read<N>(0, a, t);
+    __syncthreads();  // buffer 0 read by the whole group; also the transform's leading barrier
+    RP.start(0, B.nw + (size_t)rowc * N, N);
+    fft<N, -1, R, false>(a, sh, t, TW);
+    RP.wait(1);
+    RP.template read<N>(1, b, t);
+    __syncthreads();
+    RP.start(1, B.w + (size_t)rowc * N, N);
+    fft<N, -1, R, false>(b, sh, t, TW);
+    RP.wait(0);
+    // N_w = N_w partial + I (kx F[Fy] - ky F[Fx])
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const R kx = kxm(m);
+      const R dr = rsub(rmul(kx, b[m].x), rmul(ky, a[m].x));
+      const R di = rsub(rmul(kx, b[m].y), rmul(ky, a[m].y));
+      const cx<R> p = RP.buf[0][t + NT * m];
+      a[m] = mk<R>(radd(p.x, -di), radd(p.y, dr));
+    }
+  } else if constexpr (CURL) {
     // the force: binary (PLAINF) Fx and Fy as plain fields, ternary a pair field
     if (PLAINF) load_row<N>(a, B.h[HFF], row, live, t);
     else load_row_pair<N>(a, B.h[HFF], row, 0, live, t);
@@ -1045,7 +1168,12 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
     for (int m = 0; m < 16; m++) a[m] = mk<R>(a[m].x * (R)(-1), a[m].y * (R)(-1));
   }
   if (P.force_j >= 0 && row == P.force_j && t == 0) a[0].x = radd(a[0].x, P.force_hat);
-  load_row<N>(b, B.w, row, live, t);
+  if constexpr (PF) {
+    RP.wait(1);
+    RP.template read<N>(1, b, t);
+  } else {
+    load_row<N>(b, B.w, row, live, t);
+  }
 #pragma unroll
   for (int m = 0; m < 16; m++) {
     const int am = amask<N>(t, m);
@@ -1128,7 +1256,7 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_row_r2c_plain(const R* __res
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), tw, t);
-  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int pair = blockIdx.x * GPC + g;
   const bool live = pair < N / 2;
@@ -1153,7 +1281,7 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_col_plain(const cx<R>* __res
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), tw, t);
-  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = blockIdx.x * GPC + g;
   const bool live = row < nrows;
@@ -1176,7 +1304,7 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_row_c2r_plain(const cx<R>* _
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), tw, t);
-  unsigned char* smem_raw = smem_all + tw_smem_per_thread<N, R>() * blockDim.x;
+  unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   const RowSmem<N, R, GPC> S(smem_raw, g, JT);
   const int pair = blockIdx.x * GPC + g;
   const bool live = pair < N / 2;

@@ -65,6 +65,7 @@ template <class R> Par<R> make_par(const chns_ctx* c) {
   P.coef = (const R*)c->coef;
   P.tw = (const cx<R>*)c->tw;
   P.k0 = c->k0;
+  P.err = c->tma_err;
   return P;
 }
 
@@ -94,14 +95,17 @@ template <int N, class R> struct Sizes {
   static constexpr int GPC = gpc_of<N, R>();
   static constexpr int NT = N / 16;
   static constexpr int THREADS = GPC * NT;
-  static constexpr size_t TW = tw_smem_per_thread<N, R>() * THREADS;  // precomputed twiddles
+  static constexpr size_t TW = tw_smem_bytes<N, R>(THREADS);  // precomputed twiddles
   static constexpr size_t FFT_SMEM = TW + (size_t)GPC * FftShape<N>::SMEM * sizeof(cx<R>);
   static constexpr size_t FRAG = (size_t)GPC * N * sizeof(cx<R>);
   static int grid_rows(int rows) { return (rows + GPC - 1) / GPC; }
 };
 
-// P3's shared memory: the transform buffers
-template <int N, class R> constexpr size_t p3_smem() { return Sizes<N, R>::FFT_SMEM; }
+// shared memory of P3 / P5: the transform buffers, plus the row buffers of the
+// binary FP32 passes, which prefetch their input rows
+template <int N, class R> constexpr size_t spec_smem(bool prefetch) {
+  return Sizes<N, R>::FFT_SMEM + (prefetch && sizeof(R) == 4 ? prefetch_smem<N, R, Sizes<N, R>::GPC>() : 0);
+}
 
 template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   using S = Sizes<N, R>;
@@ -180,22 +184,22 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   if (model == CHNS_MODEL_BINARY) {
     if (stage == 1) {
       auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1, F32> : k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1, false>;
-      set_smem(k, (p3_smem<N, R>()));
-      k<<<rows_all, S::THREADS, (p3_smem<N, R>()), st>>>(B, P);
+      set_smem(k, spec_smem<N, R>(model == CHNS_MODEL_BINARY));
+      k<<<rows_all, S::THREADS, spec_smem<N, R>(model == CHNS_MODEL_BINARY), st>>>(B, P);
     } else {
       auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 2, F32> : k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 2, false>;
-      set_smem(k, (p3_smem<N, R>()));
-      k<<<rows_all, S::THREADS, (p3_smem<N, R>()), st>>>(B, P);
+      set_smem(k, spec_smem<N, R>(model == CHNS_MODEL_BINARY));
+      k<<<rows_all, S::THREADS, spec_smem<N, R>(model == CHNS_MODEL_BINARY), st>>>(B, P);
     }
   } else {
     if (stage == 1) {
       auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 1, F32> : k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 1, false>;
-      set_smem(k, (p3_smem<N, R>()));
-      k<<<rows_all, S::THREADS, (p3_smem<N, R>()), st>>>(B, P);
+      set_smem(k, spec_smem<N, R>(model == CHNS_MODEL_BINARY));
+      k<<<rows_all, S::THREADS, spec_smem<N, R>(model == CHNS_MODEL_BINARY), st>>>(B, P);
     } else {
       auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 2, F32> : k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 2, false>;
-      set_smem(k, (p3_smem<N, R>()));
-      k<<<rows_all, S::THREADS, (p3_smem<N, R>()), st>>>(B, P);
+      set_smem(k, spec_smem<N, R>(model == CHNS_MODEL_BINARY));
+      k<<<rows_all, S::THREADS, spec_smem<N, R>(model == CHNS_MODEL_BINARY), st>>>(B, P);
     }
   }
   launches++;
@@ -224,8 +228,8 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
                         : (bin ? k_spec_curl_w<N, R, GPC, true, 1, false, true> : k_spec_curl_w<N, R, GPC, true, 1, false>))
                  : (s64 ? (bin ? k_spec_curl_w<N, R, GPC, true, 2, F32, true> : k_spec_curl_w<N, R, GPC, true, 2, F32>)
                         : (bin ? k_spec_curl_w<N, R, GPC, true, 2, false, true> : k_spec_curl_w<N, R, GPC, true, 2, false>));
-    set_smem(k, S::FFT_SMEM);
-    k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    set_smem(k, spec_smem<N, R>(bin));
+    k<<<rows_all, S::THREADS, spec_smem<N, R>(bin), st>>>(B, P);
   }
   launches++;
   mark(c, KIND_SPEC_CURL_W);

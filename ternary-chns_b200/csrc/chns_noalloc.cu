@@ -66,7 +66,7 @@ template <int N> constexpr int gpc() {
 }
 
 template <int N> constexpr size_t smem_bytes() {
-  return chns::tw_smem_per_thread<N, double>() * (gpc<N>() * (N / 16)) +
+  return chns::tw_smem_bytes<N, double>(gpc<N>() * (N / 16)) +
          (size_t)gpc<N>() * chns::FftShape<N>::SMEM * sizeof(chns::cxd);
 }
 

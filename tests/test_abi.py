@@ -120,3 +120,17 @@ def test_header_compiles_and_links_for_c_and_cpp_hosts(lib, tmp_path, std, lang)
                    + ["-x", lang, str(src), "-x", "none", "-I", os.path.join(root, "include"), "-L", libdir,
                       "-lchns_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True, capture_output=True)
     assert subprocess.run([str(exe)]).returncode == 0
+
+
+def test_slab_plan_rejects_bad_decompositions_without_cuda(lib):
+    """chns_slab_create validates the decomposition before it allocates."""
+    from chns_b200 import slab
+
+    slab._bind(lib)
+    h = ctypes.c_void_p()
+    assert lib.chns_slab_create(64, 3, 0, ctypes.byref(h)) == -1     # 64 x-rows do not split over 3 ranks
+    assert lib.chns_slab_create(64, 64, 0, ctypes.byref(h)) == -1    # one x-row per rank: the y passes need pairs
+    assert lib.chns_slab_create(64, 2, 2, ctypes.byref(h)) == -1     # rank out of range
+    assert lib.chns_slab_create(8192, 2, 0, ctypes.byref(h)) == -5   # beyond the largest grid
+    assert lib.chns_slab_create(96, 2, 0, ctypes.byref(h)) == -5     # not a power of two
+    assert not h.value
