@@ -257,6 +257,18 @@ int chns_ensemble_size(const chns_ensemble *ens);
 /* nsteps ETD2RK steps of every member; stream-ordered after earlier work on
  * each member's stream, and later work on member streams waits for it. */
 int chns_ensemble_step(chns_ensemble *ens, int nsteps);
+/* How chns_ensemble_step runs (no counterpart in the reference): 1 = every step
+ * is one persistent kernel over all members (its CTAs take the members' stage
+ * work from a queue, each item waiting only for its own member's previous
+ * pass), 0 = a graph with one branch of stage kernels per member (the default,
+ * faster on the benchmark's 64-member ensemble).  The persistent form needs
+ * every member ternary, CHNS_FP32, n = 256, 512 or 1024 and the reference's cut
+ * on a square box.  enable = 0 or 1 switches (CHNS_ERR_UNSUPPORTED if the
+ * members do not allow 1), any other value only queries; returns the mode in
+ * use.  Both modes give bitwise the same states.  A bounded wait of the
+ * persistent kernel that runs out is returned by chns_ensemble_synchronize as
+ * CHNS_ERR_TIMEOUT. */
+int chns_ensemble_persistent(chns_ensemble *ens, int enable);
 int chns_ensemble_synchronize(chns_ensemble *ens);
 
 /* Kernel launches of one step (known after the first chns_step). */

@@ -29,7 +29,8 @@ def _sources():
     srcs = [os.path.join(CSRC, "chns_api.cu"), os.path.join(CSRC, "chns_noalloc.cu"),
             os.path.join(CSRC, "chns_adjoint.cu"), os.path.join(CSRC, "chns_ensemble.cu"),
             os.path.join(CSRC, "chns_init.cu"), os.path.join(CSRC, "chns_io.cu"),
-            os.path.join(CSRC, "chns_diag_extra.cu"), os.path.join(CSRC, "chns_slab.cu")]
+            os.path.join(CSRC, "chns_diag_extra.cu"), os.path.join(CSRC, "chns_slab.cu"),
+            os.path.join(CSRC, "chns_persist.cu")]
     srcs += [os.path.join(CSRC, f"chns_inst_{n}.cu") for n in SIZES]
     return srcs
 

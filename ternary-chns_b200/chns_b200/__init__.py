@@ -119,6 +119,8 @@ def load_library(path: str = LIB_PATH):
     L.chns_ensemble_step.restype = ip
     L.chns_ensemble_synchronize.argtypes = [vp]
     L.chns_ensemble_synchronize.restype = ip
+    L.chns_ensemble_persistent.argtypes = [vp, ip]
+    L.chns_ensemble_persistent.restype = ip
     L.chns_dfft_noalloc.argtypes = [vp, vp, ip, vp]
     L.chns_dfft_noalloc.restype = ip
     L.chns_status_string.restype = ctypes.c_char_p
@@ -380,7 +382,9 @@ class Member(Context):
 class Ensemble:
     """Independent runs (any mix of models, sizes, precisions and parameters)
     advanced together by chns_ensemble_step: one CUDA graph launch per step with
-    every member on its own branch.  ``members[i]`` behaves like a Context."""
+    every member on its own branch, or (``persistent = True``, when every member
+    is a ternary FP32 run at 256^2..1024^2) one persistent kernel per step.
+    ``members[i]`` behaves like a Context."""
 
     def __init__(self, params_list):
         self.L = load_library()
@@ -400,6 +404,18 @@ class Ensemble:
 
     def synchronize(self):
         _check(self.L.chns_ensemble_synchronize(self._h), "chns_ensemble_synchronize")
+
+    @property
+    def persistent(self) -> bool:
+        """True when a step is one persistent kernel over all members."""
+        rc = self.L.chns_ensemble_persistent(self._h, -1)
+        _check(min(rc, 0), "chns_ensemble_persistent")
+        return rc == 1
+
+    @persistent.setter
+    def persistent(self, enable: bool):
+        rc = self.L.chns_ensemble_persistent(self._h, 1 if enable else 0)
+        _check(min(rc, 0), "chns_ensemble_persistent")
 
     def close(self):
         if getattr(self, "_h", None):

@@ -1,5 +1,10 @@
 // chns_ensemble.cu -- many independent runs advanced by one CUDA graph per step.
 //
+// Ensembles whose members are all ternary FP32 runs at 256^2..1024^2 (the
+// batched-run configuration) can also step as ONE persistent kernel
+// (chns_persist.cu, chns_ensemble_persistent), captured in the step graph; the
+// graph of per-member branches described below is the default.
+//
 // Each member is an ordinary context.  The ensemble step graph is captured once:
 // a fork event on the ensemble stream, then on every member's stream the two
 // ETD2RK stages of that member, then a join.  Replaying it runs the members'
@@ -22,6 +27,8 @@ struct chns_ensemble {
   std::vector<cudaEvent_t> ev;  // one per member
   cudaGraphExec_t graph;
   bool graph_ok, graph_tried;
+  chns_persist* persist;  // the one-kernel step when the members allow it (else null)
+  bool use_persist;
 };
 
 namespace {
@@ -36,6 +43,7 @@ void release(chns_ensemble* e) {
   if (!e) return;
   if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->persist) chns_persist_destroy(e->persist);
   for (cudaEvent_t v : e->ev)
     if (v) cudaEventDestroy(v);
   if (e->fork) cudaEventDestroy(e->fork);
@@ -47,6 +55,7 @@ void release(chns_ensemble* e) {
 
 // the members' stages on their own streams, forked from and joined to e->stream
 int enqueue(chns_ensemble* e) {
+  if (e->use_persist) return chns_persist_step(e->persist, e->stream);
   EK(cudaEventRecord(e->fork, e->stream));
   for (size_t i = 0; i < e->m.size(); i++) {
     chns_ctx* c = e->m[i];
@@ -108,6 +117,9 @@ int chns_ensemble_create(const chns_params* members, int count, chns_ensemble** 
       return CHNS_ERR_CUDA;
     }
   }
+  // members that allow it can step as one persistent kernel (chns_ensemble_persistent);
+  // the graph stays the default: on the batched-run ensemble it measured faster
+  if (chns_persist_create(e->m.data(), count, &e->persist) != CHNS_OK) e->persist = nullptr;
   *out = e;
   return CHNS_OK;
 }
@@ -155,11 +167,31 @@ int chns_ensemble_step(chns_ensemble* e, int nsteps) {
 int chns_ensemble_synchronize(chns_ensemble* e) {
   if (!e) return CHNS_ERR_ARG;
   EK(cudaStreamSynchronize(e->stream));
+  if (e->persist) {
+    const int rc = chns_persist_check(e->persist, e->stream);
+    if (rc != CHNS_OK) return rc;
+  }
   for (chns_ctx* c : e->m) {
     const int rc = chns_synchronize(c);
     if (rc != CHNS_OK) return rc;
   }
   return CHNS_OK;
+}
+
+int chns_ensemble_persistent(chns_ensemble* e, int enable) {
+  if (!e) return CHNS_ERR_ARG;
+  if (enable == 0 || enable == 1) {
+    if (enable && !e->persist) return CHNS_ERR_UNSUPPORTED;
+    if ((bool)enable != e->use_persist) {
+      // the captured step belongs to the other mode: capture again on the next step
+      if (e->stream) cudaStreamSynchronize(e->stream);
+      if (e->graph) cudaGraphExecDestroy(e->graph);
+      e->graph = nullptr;
+      e->graph_ok = e->graph_tried = false;
+      e->use_persist = enable != 0;
+    }
+  }
+  return e->use_persist ? 1 : 0;
 }
 
 }  // extern "C"

@@ -7,6 +7,14 @@
 
 struct chns_ctx;
 struct chns_adj;
+// an ensemble's step as one persistent cooperative kernel (chns_persist.cu):
+// CHNS_ERR_UNSUPPORTED when the members are not all ternary FP32 at 256..1024
+struct chns_persist;
+int chns_persist_create(chns_ctx* const* members, int count, chns_persist** out);
+void chns_persist_destroy(chns_persist* p);
+int chns_persist_step(chns_persist* p, cudaStream_t st);
+int chns_persist_check(chns_persist* p, cudaStream_t st);
+int chns_persist_grid(const chns_persist* p);
 void chns_adj_free(chns_ctx* c);
 // shared by chns_set_phase_real and the initial conditions (chns_init.cu)
 extern "C" int chns_realdbl_to_realbuf(chns_ctx* c);

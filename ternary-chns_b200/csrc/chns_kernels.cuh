@@ -85,6 +85,28 @@ template <class R> struct Bufs {
 // FP32 step kernels are built for two CTAs per SM (<= 128 registers), FP64 for one
 #define CHNS_STEP_BOUNDS(N, R, GPC) __launch_bounds__((GPC) * ((N) / 16), sizeof(R) == 4 ? 2 : 1)
 
+// The five stage kernels are kernels of their own (one launch per pass), or, in a
+// translation unit that defines CHNS_STAGE_BODIES before including this header,
+// device functions of the same text that a persistent kernel calls once per
+// virtual CTA: there CHNS_BX / CHNS_BY read that CTA's index from chns_vblock
+// (a shared int[2] that translation unit declares before the include and sets,
+// followed by a barrier, before each call) instead of blockIdx.
+#ifdef CHNS_STAGE_BODIES
+#define CHNS_STAGE_KERNEL(N, R, GPC) __device__ __forceinline__ void
+#define CHNS_TMAG_PARAM const TmaG&
+#define CHNS_BUFS_PARAM const Bufs<R>&
+#define CHNS_PAR_PARAM const Par<R>&
+#define CHNS_BX chns_vblock[0]
+#define CHNS_BY chns_vblock[1]
+#else
+#define CHNS_STAGE_KERNEL(N, R, GPC) __global__ void CHNS_STEP_BOUNDS(N, R, GPC)
+#define CHNS_TMAG_PARAM const __grid_constant__ TmaG
+#define CHNS_BUFS_PARAM const Bufs<R>
+#define CHNS_PAR_PARAM const Par<R>
+#define CHNS_BX blockIdx.x
+#define CHNS_BY blockIdx.y
+#endif
+
 template <class R> __device__ __forceinline__ cx<R> czero() { return mk<R>((R)0, (R)0); }
 
 // signed wavenumber index of column i (functions.c:17-24: Nyquist positive)
@@ -485,14 +507,14 @@ template <int N> __device__ __forceinline__ int amask(int t, int m) {
 template <int N> constexpr bool spec_inv_split() { return N <= 1024; }
 
 template <int N, class R, int GPC, int MODEL>
-__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_inv(const Bufs<R> B, const Par<R> P) {
+CHNS_STAGE_KERNEL(N, R, GPC) k_spec_inv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
   constexpr int NT = N / 16;
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
   unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
-  const int row = blockIdx.x * GPC + g;
+  const int row = CHNS_BX * GPC + g;
   const bool live = row <= P.jt;
   const int mlim = live ? P.mrow[row] : -1;
   const R ky = (R)(P.fy * (double)row);
@@ -512,14 +534,14 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_inv(const Bufs<R> B, const Pa
   // of c commutes with the x transform (ky is constant along the row), so dy c is
   // i ky times the transformed c_t and gets no transform of its own.
   // Grids up to 1024^2 split the outputs between the two CTAs of a row
-  // (blockIdx.y), half the transforms each: twice the CTAs for rows too few to
+  // (CHNS_BY), half the transforms each: twice the CTAs for rows too few to
   // fill the GPU (measured: 5-8% more steps/s at 256^2-1024^2; at 4096^2 the
   // second read of the input row costs more than it gains).
   // The vorticity's outputs run in the order dx w, dy w, u, v so that w can be
   // turned into psi = w / k^2 in place once (velocity.c:12-42) for both u and v.
   constexpr int NOUT = MODEL == MODEL_NS ? 4 : (MODEL == MODEL_BINARY ? 7 : 10);
   constexpr int OSPLIT = spec_inv_split<N>() ? (MODEL == MODEL_NS ? 2 : (MODEL == MODEL_BINARY ? 3 : 4)) : NOUT;
-  const int obeg = blockIdx.y == 0 ? 0 : OSPLIT, oend = blockIdx.y == 0 ? OSPLIT : NOUT;
+  const int obeg = CHNS_BY == 0 ? 0 : OSPLIT, oend = CHNS_BY == 0 ? OSPLIT : NOUT;
   bool loaded = false;
 #pragma unroll 1
   for (int idx = 0; idx < NOUT; idx++) {
@@ -642,7 +664,7 @@ __device__ __forceinline__ RowSrc<R> adv_src(const Bufs<R>& B, int it, int i0) {
 }
 
 template <int N, class R, int GPC, int MODEL, bool JT4 = false>
-__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par<R> P, const __grid_constant__ TmaG T) {
+CHNS_STAGE_KERNEL(N, R, GPC) k_row_adv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS_TMAG_PARAM T) {
   using Sc = AdvSchedule<MODEL>;
   constexpr int NT = N / 16;
   extern __shared__ __align__(16) unsigned char smem_all[];
@@ -654,7 +676,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_adv(const Bufs<R> B, const Par
   const int jt = P.jt;
   const LoadedRowSmem<N, R, GPC> LS(smem_raw, g, tma ? T.nbox * T.boxr - 1 : jt, row_adv_frags<MODEL>());
   const RowSmem<N, R, GPC>& S = LS.S;
-  const int pair = blockIdx.x * GPC + g;
+  const int pair = CHNS_BX * GPC + g;
   const bool live = pair < N / 2;
   const int i0 = 2 * pair;
   Frag<N, R> keep{S.frag}, keep2{S.frag + (size_t)N * GPC};
@@ -766,7 +788,7 @@ __device__ __forceinline__ RowSrc<R> force_src(const Bufs<R>& B, int it, int i0)
 }
 
 template <int N, class R, int GPC, int MODEL, bool JT4 = false>
-__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const Par<R> P, const __grid_constant__ TmaG T) {
+CHNS_STAGE_KERNEL(N, R, GPC) k_row_force(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS_TMAG_PARAM T) {
   constexpr int NT = N / 16;
   constexpr int NIN = MODEL == MODEL_BINARY ? 3 : 6;      // inverse transforms
   constexpr int STEPS = MODEL == MODEL_BINARY ? 4 : 6;    // binary: a last step only stores
@@ -779,7 +801,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_row_force(const Bufs<R> B, const P
   const int jt = P.jt;
   const LoadedRowSmem<N, R, GPC> LS(smem_raw, g, tma ? T.nbox * T.boxr - 1 : jt, row_force_frags<MODEL>());
   const RowSmem<N, R, GPC>& S = LS.S;
-  const int pair = blockIdx.x * GPC + g;
+  const int pair = CHNS_BX * GPC + g;
   const bool live = pair < N / 2;
   const int i0 = 2 * pair;
   Frag<N, R> w1{S.frag}, w2{S.frag + N * GPC};
@@ -949,7 +971,7 @@ __device__ __forceinline__ cxf split_k0(const double* st, cxf* lo) {
 // truncated), so their float rounding is not amplified; they are updated in
 // float with their low part left at zero.
 template <int N, class R, int GPC, int MODEL, int STAGE, bool S64>
-__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const Par<R> P) {
+CHNS_STAGE_KERNEL(N, R, GPC) k_spec_fwd_c(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
   constexpr bool F32 = sizeof(R) == 4;
@@ -958,10 +980,10 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
   unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
-  const int row = blockIdx.x * GPC + g;
+  const int row = CHNS_BX * GPC + g;
   const bool live = row < NR;
   const int rowc = live ? row : 0;
-  const bool do_mu = (int)(blockIdx.x * GPC) <= P.jt;  // CTA-uniform
+  const bool do_mu = (int)(CHNS_BX * GPC) <= P.jt;  // CTA-uniform
   const int mlim = (live && row <= P.jt) ? P.mrow[row] : -1;
   const R ky = (R)(P.fy * (double)row);
   const R* __restrict__ cf = P.coef + (size_t)rowc * NR;
@@ -1095,7 +1117,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_fwd_c(const Bufs<R> B, const 
 // N_w = -F[u.grad w] (nonlin.c:74-101) from the plain field in HAB.
 // ---------------------------------------------------------------------------
 template <int N, class R, int GPC, bool CURL, int STAGE, bool S64, bool PLAINF = false>
-__global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const Par<R> P) {
+CHNS_STAGE_KERNEL(N, R, GPC) k_spec_curl_w(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
   constexpr bool F32 = sizeof(R) == 4;
@@ -1104,7 +1126,7 @@ __global__ void CHNS_STEP_BOUNDS(N, R, GPC) k_spec_curl_w(const Bufs<R> B, const
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
   unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
-  const int row = blockIdx.x * GPC + g;
+  const int row = CHNS_BX * GPC + g;
   const bool live = row < NR;
   const int rowc = live ? row : 0;
   const int mlim = (live && row <= P.jt) ? P.mrow[row] : -1;  // truncation disc of this row (S64)

@@ -104,3 +104,55 @@ def test_member_calls_between_ensemble_steps(chns):
     for a, b in zip(final[2], g["final"]):
         assert rel_l2(a, b) <= 1e-11
     assert all(np.all(np.isfinite(f)) for f in fe)
+
+
+def _ternary_fp32_members(seed=21):
+    """A batched-run ensemble of the persistent kind: ternary FP32 members at
+    256^2, 512^2 and 1024^2 with their own sigma_ij and noise."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for n, dt in ((1024, 3e-6), (256, 1e-4), (512, 2.5e-5), (256, 1e-4), (512, 2.5e-5), (256, 1e-4)):
+        lx = 2 * math.pi
+        p = dict(model=2, nx=n, ny=n, lx=lx, dt=dt, nu=0.01, precision=1, coef_mode=1, epsilon=2 * lx / n,
+                 sigma12=0.2 + 0.05 * rng.uniform(), sigma13=0.3, sigma23=0.25 + 0.05 * rng.uniform(), xlambda=2.0)
+        p["lambda"] = 0.005
+        out.append((p, [1 / 3 + 0.02 * rng.uniform(-1, 1, (n, n)), 1 / 3 + 0.02 * rng.uniform(-1, 1, (n, n))]))
+    return out
+
+
+def test_persistent_step_matches_lone_contexts_and_the_graph(chns):
+    """One persistent cooperative kernel per step (every member ternary FP32 at
+    256..1024): each member bitwise equal to a lone context and to the same
+    ensemble stepped by the graph of per-member branches."""
+    members = _ternary_fp32_members()
+    steps = 12
+    states = {}
+    for mode in (True, False):
+        with chns.Ensemble([p for p, _ in members]) as ens:
+            assert not ens.persistent  # the graph is the default
+            ens.persistent = mode
+            assert ens.persistent == mode
+            for m, (_, ph) in zip(ens.members, members):
+                m.set_phase_real(*ph)
+            ens.step(steps - 4)
+            ens.step(4)
+            ens.synchronize()
+            states[mode] = [m.get_state() for m in ens.members]
+    for i, (p, ph) in enumerate(members):
+        with chns.Context(p) as c:
+            c.set_phase_real(*ph)
+            c.step(steps)
+            want = c.get_state()
+        for a, b, w in zip(states[True][i], states[False][i], want):
+            assert np.isfinite(a).all()
+            assert np.array_equal(a, w), (i, p["nx"], "persistent vs lone")
+            assert np.array_equal(b, w), (i, p["nx"], "graph vs lone")
+
+
+def test_persistent_mode_needs_eligible_members(chns):
+    members = _members()  # mixed models and precisions
+    with chns.Ensemble([p for p, _ in members]) as ens:
+        assert not ens.persistent
+        with pytest.raises(chns.ChnsError) as ei:
+            ens.persistent = True
+        assert ei.value.status == -5
