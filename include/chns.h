@@ -281,6 +281,16 @@ int chns_launches_per_step(const chns_ctx *ctx);
  * reference (tracing). */
 int chns_tma_tiles(const chns_ctx *ctx);
 
+/* Failure injection for tests (no counterpart in the reference): the row
+ * kernels' waits for their TMA tiles poll at most `spins` times (0 = the
+ * default bound) and, with skip_copies != 0, no tile copy is issued at all, so
+ * every wait runs out on a barrier nothing will complete -- no copy is in
+ * flight, the kernels finish, their results are garbage -- and the next
+ * chns_synchronize / chns_check returns CHNS_ERR_TIMEOUT.  chns_debug_tile_waits
+ * (ctx, 0, 0) restores normal operation.  CHNS_ERR_UNSUPPORTED when the context
+ * has no TMA tiles (chns_tma_tiles). */
+int chns_debug_tile_waits(chns_ctx *ctx, int spins, int skip_copies);
+
 /* Tracing: runs `reps` steps launching the kernels one by one (not from the
  * graph) with a CUDA event recorded after each launch on the context's stream;
  * writes the mean duration of every launch of one step to ms[] and its kind to

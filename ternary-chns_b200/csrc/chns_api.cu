@@ -905,6 +905,22 @@ int chns_launches_per_step(const chns_ctx* c) { return c ? c->launches_per_step 
 
 int chns_tma_tiles(const chns_ctx* c) { return c && static_cast<const chns::TmaG*>(c->tmag)->use ? 1 : 0; }
 
+int chns_debug_tile_waits(chns_ctx* c, int spins, int skip_copies) {
+  if (!c || spins < 0) return CHNS_ERR_ARG;
+  chns::TmaG* T = static_cast<chns::TmaG*>(c->tmag);
+  if (!T->use) return CHNS_ERR_UNSUPPORTED;
+  CK(cudaStreamSynchronize(c->stream));
+  T->spins = spins;
+  T->skip = skip_copies ? 1 : 0;
+  // the captured step holds the kernels' arguments: capture it again
+  if (c->step_graph) {
+    cudaGraphExecDestroy(c->step_graph);
+    c->step_graph = nullptr;
+    c->graph_ok = false;
+  }
+  return CHNS_OK;
+}
+
 int chns_profile_step(chns_ctx* c, int reps, float* ms, int* kind, int maxk) {
   if (!c || reps < 1 || !ms || !kind || maxk < 1) return CHNS_ERR_ARG;
   const int cap = 64;

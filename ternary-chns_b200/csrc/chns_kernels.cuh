@@ -185,6 +185,8 @@ struct __align__(64) TmaG {
   int boxr, nbox;           // rows per box, boxes per tile (nbox * boxr >= jt + 1)
   int ecx;                  // 64-bit elements per complex value (1: FP32, 2: FP64)
   unsigned int* err;        // bit 0: an mbarrier wait timed out
+  int spins;                // try_wait rounds of a tile wait (0: kMbarSpins)
+  int skip;                 // test hook: issue no tile copies (every tile wait then runs out)
 };
 constexpr int kMbarSpins = 1 << 18;  // try_wait rounds before a tile wait gives up
 
@@ -196,9 +198,9 @@ static __device__ __forceinline__ void mbar_init(uint64_t* mb) {
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
 // waits for the phase of parity `par` to complete; false on timeout
-static __device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned par) {
+static __device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned par, int spins = kMbarSpins) {
   unsigned ok = 0;
-  for (int k = 0; k < kMbarSpins && !ok; k++)
+  for (int k = 0; k < spins && !ok; k++)
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
@@ -287,7 +289,7 @@ template <int N, class R>
 __device__ __forceinline__ void tile_start(TileLoader<R>& L, const TmaG& T, cx<R>* tile, RowSrc<R> s, int jt,
                                            bool live, int t) {
   if (L.tma) {
-    if (t == 0 && live) tma_tile(tile, T, s.map, s.off, L.mb);
+    if (t == 0 && live && !T.skip) tma_tile(tile, T, s.map, s.off, L.mb);
   } else {
     tile_issue<N>(tile, s, jt, live, t);
     cp_async_commit();
@@ -298,7 +300,7 @@ __device__ __forceinline__ void tile_start(TileLoader<R>& L, const TmaG& T, cx<R
 template <class R>
 __device__ __forceinline__ void tile_wait(TileLoader<R>& L, const TmaG& T, bool live) {
   if (L.tma) {
-    if (live && !mbar_wait(L.mb, L.par)) atomicOr(T.err, 1u);
+    if (live && !mbar_wait(L.mb, L.par, T.spins > 0 ? T.spins : kMbarSpins)) atomicOr(T.err, 1u);
     L.par ^= 1u;
   } else {
     cp_async_wait_all();

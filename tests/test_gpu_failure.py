@@ -66,3 +66,41 @@ def test_blow_up_is_reported_by_check_and_diagnostics(chns):
         assert e.value.status == -3
         fe, ke, rc = c.diagnostics()
         assert rc == -3
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_tile_wait_that_runs_out_is_reported_and_recoverable(chns, prec):
+    """The bounded wait of the row kernels for their TMA tiles, made to run out
+    on the GPU without a fault: chns_debug_tile_waits stops the tile copies (no
+    copy is in flight, so the barriers are ones nothing completes) and bounds
+    each wait to 16 polls.  The step's results are garbage; chns_synchronize
+    returns CHNS_ERR_TIMEOUT; with the hook off and the flag cleared the same
+    context steps exactly as a fresh one."""
+    import ctypes
+
+    from chns_b200 import configs
+
+    L = chns.load_library()
+    L.chns_debug_tile_waits.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    p, (c_real,) = configs.binary_spinodal(256, prec)
+    with chns.Context(p) as ref:
+        ref.set_phase_real(c_real)
+        st0 = ref.get_state()
+        ref.step(5)
+        want = ref.get_state()
+    with chns.Context(p) as c:
+        assert c.tma_tiles()
+        c.set_state(*st0)
+        assert L.chns_debug_tile_waits(c.handle, 16, 1) == 0
+        c.step(2)
+        with pytest.raises(chns.ChnsError) as e:
+            c.synchronize()
+        assert e.value.status == -4
+        c.synchronize()  # the flag was cleared by the report
+        assert L.chns_debug_tile_waits(c.handle, 0, 0) == 0
+        c.set_state(*st0)
+        c.step(5)
+        c.synchronize()
+        for a, b in zip(c.get_state(), want):
+            assert np.array_equal(a, b)
+    assert L.chns_debug_tile_waits(None, 0, 0) == -1
