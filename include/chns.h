@@ -62,6 +62,16 @@ enum { CHNS_FP64 = 0, CHNS_FP32 = 1, CHNS_FP32_STATE64 = 2 };
  * small |c h| (more accurate than the reference for small |c h|). */
 enum { CHNS_COEF_REFERENCE = 0, CHNS_COEF_ACCURATE = 1 };
 enum { CHNS_HOST = 0, CHNS_DEVICE = 1 };
+/* Truncation of the spectra before their inverse transforms (functions.c:47-84).
+ * SHARP zeroes the modes with k^2 > ((nx/dealias_div) 2 pi/lx)^2, the reference's
+ * default build.  SMOOTH is the reference built with SMOOTH_FILTER (macro.h:15,
+ * functions.c:69-72): every mode is multiplied by f = exp(-36 (k^2/k^2max)^18),
+ * k^2max = kxmax^2 + kymax^2, twice (one rounding per product), and nothing is
+ * zeroed, so the intermediate fields of a step keep all nx/2+1 ky rows and
+ * dealias_div is ignored.  f is the host's exp and pow in double, the reference's
+ * own libm calls (rounded to float for the FP32 step).  SMOOTH contexts have no
+ * discrete adjoint (chns_adjoint returns CHNS_ERR_UNSUPPORTED). */
+enum { CHNS_FILTER_SHARP = 0, CHNS_FILTER_SMOOTH = 1 };
 
 typedef struct chns_params {
     int model;          /* CHNS_MODEL_*: none / BINARY / TERNARY (macro.h) */
@@ -78,6 +88,7 @@ typedef struct chns_params {
     int coef_mode;      /* CHNS_COEF_* */
     double force_amp;   /* Kolmogorov forcing F0 sin(kf y) x-hat on the flow; 0 = off.  Not in the reference */
     double force_k;     /* kf; kf*ly/(2 pi) must be an integer <= ny/2 */
+    int filter;         /* CHNS_FILTER_*: SHARP (default) or SMOOTH (the SMOOTH_FILTER build) */
 } chns_params;
 
 typedef struct chns_ctx chns_ctx;
@@ -99,10 +110,14 @@ int chns_destroy(chns_ctx *ctx);
  * e^{c dt}, z1, z2 of the phase fields (etd2rk.c:88-111,117-127 / 162-186,191-203,
  * per coef_mode; NS contexts: 1, dt, dt/2), in double;
  * chns_truncation_rows fills mrow[0..nx/2] with the largest |kx index| kept in
- * each ky row by the truncation (functions.c:47-84), -1 for an empty row.
- * Parameters are checked as by chns_create. */
+ * each ky row by the truncation (functions.c:47-84), -1 for an empty row (every
+ * row keeps nx/2 with the SMOOTH filter); chns_truncation_factor gives the factor
+ * f of one product of the truncation at mode (i, j): 1 or 0 for the SHARP cut,
+ * exp(-36 (k^2/k^2max)^18) for the SMOOTH filter (the mode is multiplied by it
+ * twice).  Parameters are checked as by chns_create. */
 int chns_etd_coefficients(const chns_params *p, int i, int j, double *out);
 int chns_truncation_rows(const chns_params *p, int *mrow);
+int chns_truncation_factor(const chns_params *p, int i, int j, double *f);
 
 /* Uses `stream` (a cudaStream_t) for all later work instead of the context's own. */
 int chns_set_stream(chns_ctx *ctx, void *stream);

@@ -95,6 +95,11 @@ CONFIGS = {
     # half-integer wavenumbers put some |k| exactly half-way between two shells)
     "nssh32": dict(model=0, n=32, lx="(2.0*pi)", dt="(1e-3)", nu="(0.01)", init="shell"),
     "binsh64": dict(_BIN_DEF, n=64, init="shell"),
+    # SMOOTH_FILTER (macro.h:15, functions.c:69-72): the smooth filter in place of the sharp cut
+    "nssf32": dict(model=0, n=32, lx="(2.0*pi)", dt="(1e-3)", nu="(0.01)", filter=True),
+    "binsf64": dict(_BIN, n=64, filter=True),
+    "tersf64": dict(_TER, n=64, filter=True),
+    "binsfdef64": dict(_BIN_DEF, n=64, filter=True),
 }
 
 _SUBST = {  # macro name -> key in the config dict
@@ -123,6 +128,8 @@ def _gen_macro_h(cfg: dict) -> str:
         lines.append("#define TG_INIT")
     elif init != "shell":  # "shell": neither macro, init.c's k-space branch
         lines.append("#define ZERO_INIT")
+    if cfg.get("filter"):
+        lines.append("#define SMOOTH_FILTER")
     if cfg["model"] == 1:
         lines.append("#define BINARY")
     elif cfg["model"] == 2:
@@ -208,7 +215,7 @@ def build(name: str, force: bool = False, dropin: bool = False) -> str:
 
 
 # configurations also built with the drop-in etd2rk (needs libchns_b200.so)
-DROPIN_CONFIGS = ["ns32", "bin32", "ter32", "bindef64", "terdef64"]
+DROPIN_CONFIGS = ["ns32", "bin32", "ter32", "bindef64", "terdef64", "binsf64"]
 
 
 def build_all(names=None, force=False, dropin: bool = True) -> list[str]:

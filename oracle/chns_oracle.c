@@ -21,6 +21,7 @@ struct orc_ctx {
     size_t nc;       /* complex modes nx*ny2 */
     size_t nd;       /* doubles per buffer = 2*nc = nx*(ny+2) */
     double factor_x, factor_y, dealias;
+    double ksqrmax;  /* kxmax^2 + kymax^2 (functions.c:54, main.c:57-58) */
     double gamma1, gamma2, gamma3, del;
     double *kx, *ky;
     fftc_plan *plan;
@@ -56,13 +57,23 @@ static void ifft(orc_ctx *c, double *a)
 
 static void copy(const orc_ctx *c, const double *in, double *out) { memcpy(out, in, c->nd * sizeof(double)); }
 
-/* functions.c:47-84 (the sharp cut; SMOOTH_FILTER is not part of the step's configuration) */
+/* functions.c:47-84: the sharp cut k^2 > dealias (:74-79), or with SMOOTH_FILTER
+ * (:69-72) every mode scaled by exp(-36 (k^2/k^2max)^18), applied twice with a
+ * rounding after each product */
 static void truncation(orc_ctx *c, double *a)
 {
     for (int i = 0; i < c->nx; i++)
         for (int j = 0; j < c->ny2; j++) {
             size_t k = (size_t)i * c->ny2 + j;
-            if (ksq(c, i, j) > c->dealias) { RE(a, k) = 0.0; IM(a, k) = 0.0; }
+            double ksqr = ksq(c, i, j);
+            if (c->p.filter) {
+                double pp = ksqr / c->ksqrmax;
+                double f = exp(-36.0 * pow(pp, 18));
+                RE(a, k) *= f; IM(a, k) *= f;
+                RE(a, k) *= f; IM(a, k) *= f;
+            } else if (ksqr > c->dealias) {
+                RE(a, k) = 0.0; IM(a, k) = 0.0;
+            }
         }
 }
 
@@ -470,6 +481,10 @@ orc_ctx *orc_create(const orc_params *p, int nthreads)
     {   /* functions.c:56-59: only the x extent enters the cut */
         double dax = (c->nx / c->p.dealias_div) * c->factor_x;
         c->dealias = dax * dax;
+    }
+    {   /* main.c:57-58, functions.c:54 */
+        double kxmax = (c->nx / 2.0) * c->factor_x, kymax = (c->ny / 2.0) * c->factor_y;
+        c->ksqrmax = (double)(kxmax * kxmax + kymax * kymax);
     }
     if (p->model == 2) { /* main.c:166-170 */
         c->gamma1 = (p->sigma12 - p->sigma23 + p->sigma13);

@@ -35,6 +35,7 @@ typedef struct orc_params {
     int coef_mode;      /* 0: reference's direct phi-functions (etd2rk.c:88-206); 1: series/expm1 */
     double force_amp;   /* Kolmogorov forcing F0 sin(kf y) x-hat; 0 = off (not in the reference) */
     double force_k;     /* kf */
+    int filter;         /* 0: the sharp cut; 1: SMOOTH_FILTER (functions.c:69-72, macro.h:15) */
 } orc_params;
 
 typedef struct orc_ctx orc_ctx;

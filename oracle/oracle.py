@@ -35,6 +35,7 @@ class OrcParams(ctypes.Structure):
         ("sigma12", ctypes.c_double), ("sigma13", ctypes.c_double), ("sigma23", ctypes.c_double),
         ("xlambda", ctypes.c_double), ("dealias_div", ctypes.c_double),
         ("coef_mode", ctypes.c_int), ("force_amp", ctypes.c_double), ("force_k", ctypes.c_double),
+        ("filter", ctypes.c_int),
     ]
 
 
@@ -102,7 +103,7 @@ class Oracle:
                       sigma13=p.get("sigma13", 0.0), sigma23=p.get("sigma23", 0.0),
                       xlambda=p.get("xlambda", 2.0), dealias_div=p.get("dealias_div", 4.0),
                       coef_mode=p.get("coef_mode", 0), force_amp=p.get("force_amp", 0.0),
-                      force_k=p.get("force_k", 0.0))
+                      force_k=p.get("force_k", 0.0), filter=p.get("filter", 0))
         self._h = L.orc_create(ctypes.byref(s), nthreads)
         if not self._h:
             raise ValueError("oracle: bad parameters")
@@ -216,6 +217,8 @@ def ref_config_params(name: str) -> dict:
         p["sigma13"] = eval_ref_expr(cfg["s13"], n)
         p["sigma23"] = eval_ref_expr(cfg["s23"], n)
         p["xlambda"] = eval_ref_expr(cfg["xlam"], n)
+    if cfg.get("filter"):
+        p["filter"] = 1
     return p
 
 

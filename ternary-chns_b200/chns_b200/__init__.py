@@ -27,6 +27,8 @@ LIB_PATH = os.environ.get("CHNS_B200_LIB") or os.path.join(PKG, "lib", "libchns_
 MODEL_NS, MODEL_BINARY, MODEL_TERNARY = 0, 1, 2
 FP64, FP32, FP32_STATE64 = 0, 1, 2
 COEF_REFERENCE, COEF_ACCURATE = 0, 1
+# truncation: the sharp cut, or the reference's SMOOTH_FILTER build (functions.c:69-72)
+FILTER_SHARP, FILTER_SMOOTH = 0, 1
 HOST, DEVICE = 0, 1
 INIT_W_ZERO, INIT_W_TAYLOR_GREEN, INIT_W_SHELL = 0, 1, 2
 INIT_C_DROP, INIT_C_NOISE = 0, 1
@@ -49,7 +51,7 @@ class Params(ctypes.Structure):
         ("lam", ctypes.c_double), ("sigma", ctypes.c_double), ("epsilon", ctypes.c_double),
         ("sigma12", ctypes.c_double), ("sigma13", ctypes.c_double), ("sigma23", ctypes.c_double),
         ("xlambda", ctypes.c_double), ("dealias_div", ctypes.c_double), ("coef_mode", ctypes.c_int),
-        ("force_amp", ctypes.c_double), ("force_k", ctypes.c_double),
+        ("force_amp", ctypes.c_double), ("force_k", ctypes.c_double), ("filter", ctypes.c_int),
     ]
 
 
@@ -164,6 +166,7 @@ def make_params(p: dict) -> Params:
     s.coef_mode = int(p.get("coef_mode", COEF_REFERENCE))
     s.force_amp = float(p.get("force_amp", 0.0))
     s.force_k = float(p.get("force_k", 0.0))
+    s.filter = int(p.get("filter", FILTER_SHARP))
     return s
 
 

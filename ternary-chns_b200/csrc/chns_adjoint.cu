@@ -715,6 +715,8 @@ extern "C" int chns_adjoint(chns_ctx* c, int nsteps, int ckpt, const double* los
   if (c->p.model == CHNS_MODEL_NS) return CHNS_ERR_UNSUPPORTED;
   // the checkpoints hold the float state; a double state would not be restored
   if (c->st64) return CHNS_ERR_UNSUPPORTED;
+  // the transposed passes implement the sharp cut's mask only
+  if (c->p.filter != CHNS_FILTER_SHARP) return CHNS_ERR_UNSUPPORTED;
   const double dflt[3] = {1.0, 1.0, 1.0};
   const double* lw = loss_w ? loss_w : dflt;
   if (c->p.model == CHNS_MODEL_BINARY)

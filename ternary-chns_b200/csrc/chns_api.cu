@@ -159,6 +159,10 @@ double mode_ksq(double fx, double fy, int m, int j) {
 // the last row with a kept mode.
 int truncation_rows(const chns_params& p, double fx, double fy, int* mrow) {
   const int n = p.nx, nr = p.nx / 2 + 1;
+  if (p.filter == CHNS_FILTER_SMOOTH) {  // functions.c:69-72: no mode is zeroed
+    for (int j = 0; j < nr; j++) mrow[j] = n / 2;
+    return n / 2;
+  }
   const double dax = (p.nx / p.dealias_div) * fx;
   const double dealias = dax * dax;
   int jt = -1;
@@ -174,6 +178,15 @@ int truncation_rows(const chns_params& p, double fx, double fy, int* mrow) {
   return jt;
 }
 
+// SMOOTH_FILTER factor of the mode (|kx index| m, ky index j), functions.c:53-54,69-72
+// with kxmax, kymax of main.c:57-58: exp(-36 (k^2/k^2max)^18) by the host's libm
+double filter_factor(const chns_params& p, double fx, double fy, int m, int j) {
+  const double kxmax = (p.nx / 2.0) * fx, kymax = (p.ny / 2.0) * fy;
+  const double ksqrmax = (double)(kxmax * kxmax + kymax * kymax);
+  const double pp = mode_ksq(fx, fy, m, j) / ksqrmax;
+  return ::exp(-36.0 * ::pow(pp, 18.0));
+}
+
 int validate(const chns_params* p) {
   if (!p) return CHNS_ERR_ARG;
   if (p->model < 0 || p->model > 2) return CHNS_ERR_ARG;
@@ -183,7 +196,9 @@ int validate(const chns_params* p) {
   const int l = ilog2_exact(p->nx);
   if (l < 5 || l > 12) return CHNS_ERR_UNSUPPORTED;
   if (!(p->lx > 0) || !(p->ly > 0) || !(p->dt > 0) || !(p->nu >= 0)) return CHNS_ERR_ARG;
-  if (!(p->dealias_div > 2.0)) return CHNS_ERR_ARG;  // the truncated band must stay below the Nyquist row
+  if (p->filter != CHNS_FILTER_SHARP && p->filter != CHNS_FILTER_SMOOTH) return CHNS_ERR_ARG;
+  // the sharp cut's band must stay below the Nyquist row
+  if (p->filter == CHNS_FILTER_SHARP && !(p->dealias_div > 2.0)) return CHNS_ERR_ARG;
   if (p->model != CHNS_MODEL_NS && !(p->epsilon > 0)) return CHNS_ERR_ARG;
   if (p->coef_mode != CHNS_COEF_REFERENCE && p->coef_mode != CHNS_COEF_ACCURATE) return CHNS_ERR_ARG;
   if (p->force_amp != 0.0) {
@@ -200,7 +215,8 @@ void free_all(chns_ctx* c) {
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   void* ptrs[] = {c->state[0], c->state[1], c->state[2], c->saved[0], c->saved[1], c->saved[2], c->nw,
                   c->coef, c->mrow, c->tw, c->k0, c->stage, c->realbuf, c->realdbl, c->red, c->redscratch,
-                  c->statelo[0], c->statelo[1], c->statelo[2], c->tma_err};
+                  c->statelo[0], c->statelo[1], c->statelo[2], c->tma_err, c->filt,
+                  (void*)c->filtd == c->filt ? nullptr : (void*)c->filtd};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (void* q : c->g)
@@ -392,7 +408,7 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
   c->fy = (2 * M_PI) / p.ly;
   std::vector<int> mrow(nr, -1);
   c->jt = truncation_rows(p, c->fx, c->fy, mrow.data());
-  if (c->jt < 0 || c->jt >= n / 2) {
+  if (c->jt < 0 || (c->jt >= n / 2 && p.filter == CHNS_FILTER_SHARP)) {
     free_all(c);
     return CHNS_ERR_UNSUPPORTED;
   }
@@ -462,7 +478,26 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
   if (rc == CHNS_OK) rc = dmalloc((void**)&c->red, 16 * sizeof(double));
   if (rc == CHNS_OK) rc = dmalloc(&c->redscratch, (size_t)(n / 2 + 1) * 8 * sizeof(double));
   if (rc == CHNS_OK) rc = dmalloc((void**)&c->tma_err, sizeof(unsigned int));
+  std::vector<double> filt;
+  if (rc == CHNS_OK && p.filter == CHNS_FILTER_SMOOTH) {
+    filt.resize(tsz);
+    for (int j = 0; j < nr; j++)
+      for (int m = 0; m < nr; m++) filt[(size_t)j * nr + m] = filter_factor(p, c->fx, c->fy, m, j);
+    rc = dmalloc(&c->filt, tsz * c->rsz);
+    if (rc == CHNS_OK && c->f32) rc = dmalloc((void**)&c->filtd, tsz * sizeof(double));
+    if (rc == CHNS_OK && !c->f32) c->filtd = (double*)c->filt;
+  }
   if (rc == CHNS_OK) rc = build_tma(c);
+  // the row kernels' shared memory grows with the G rows (all of them with the
+  // smooth filter): refuse a context whose kernels would not launch
+  if (rc == CHNS_OK) {
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+      rc = CHNS_ERR_CUDA;
+    else if (c->L->step_smem(c) > (size_t)optin)
+      rc = CHNS_ERR_UNSUPPORTED;
+  }
   if (rc != CHNS_OK) {
     free_all(c);
     return rc;
@@ -490,6 +525,12 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
     if (e == cudaSuccess) e = cudaMemcpy(c->tw, twd.data(), twd.size() * 8, cudaMemcpyHostToDevice);
   }
   if (e == cudaSuccess) e = cudaMemcpy(c->mrow, mrow.data(), nr * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && c->filtd)
+    e = cudaMemcpy(c->filtd, filt.data(), tsz * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && c->filt && c->f32) {
+    std::vector<float> ff(filt.begin(), filt.end());
+    e = cudaMemcpy(c->filt, ff.data(), tsz * sizeof(float), cudaMemcpyHostToDevice);
+  }
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     free_all(c);
@@ -513,6 +554,21 @@ int chns_truncation_rows(const chns_params* p, int* mrow) {
   if (rc != CHNS_OK) return rc;
   if (!mrow) return CHNS_ERR_ARG;
   truncation_rows(*p, (2 * M_PI) / p->lx, (2 * M_PI) / p->ly, mrow);
+  return CHNS_OK;
+}
+
+int chns_truncation_factor(const chns_params* p, int i, int j, double* f) {
+  const int rc = validate(p);
+  if (rc != CHNS_OK) return rc;
+  if (!f || i < 0 || i >= p->nx || j < 0 || j > p->nx / 2) return CHNS_ERR_ARG;
+  const int m = i <= p->nx / 2 ? i : p->nx - i;
+  const double fx = (2 * M_PI) / p->lx, fy = (2 * M_PI) / p->ly;
+  if (p->filter == CHNS_FILTER_SMOOTH) {
+    *f = filter_factor(*p, fx, fy, m, j);
+  } else {
+    const double dax = (p->nx / p->dealias_div) * fx;
+    *f = mode_ksq(fx, fy, m, j) > dax * dax ? 0.0 : 1.0;
+  }
   return CHNS_OK;
 }
 
@@ -633,7 +689,8 @@ static int set_field(chns_ctx* c, int f, const double* src, int where) {
     const dim3 grid((c->nr + 31) / 32, (c->n + 31) / 32);
     k_fftw_to_hilo<<<grid, dim3(32, 8), 0, c->stream>>>((const double2*)c->stage, (float2*)c->state[f],
                                                          (float2*)c->statelo[f], c->n);
-    c->L->truncate(c, c->statelo[f]);  // low parts only inside the truncation disc
+    // low parts only inside the sharp cut's disc (the smooth filter keeps every mode)
+    if (c->p.filter == CHNS_FILTER_SHARP) c->L->truncate(c, c->statelo[f]);
   } else {
     c->L->from_fftw(c, c->stage, c->state[f]);
   }

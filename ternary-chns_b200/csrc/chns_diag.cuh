@@ -38,7 +38,8 @@ __device__ __forceinline__ void row_c2r_direct(cx<R>* v, RowSrc<R> s, int jt, bo
   fft<N, +1>(v, sh, t, tw);
 }
 
-template <int N, class R, int GPC, int MODEL>
+// FILT: SMOOTH_FILTER truncation (P.filt), a variant of its own as in P3
+template <int N, class R, int GPC, int MODEL, bool FILT = false>
 __global__ void __launch_bounds__(GPC * (N / 16)) k_diag_spec(const Bufs<R> B, const Par<R> P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
@@ -80,8 +81,10 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_diag_spec(const Bufs<R> B, c
       // truncated c for the phase masks (kinetic_energy.c:23-32)
       if (tr) {
 #pragma unroll
-        for (int m = 0; m < 16; m++)
+        for (int m = 0; m < 16; m++) {
           v[m] = amask<N>(t, m) <= mlim ? mk<R>(in[m].x * sc, in[m].y * sc) : czero<R>();
+          if (FILT && amask<N>(t, m) <= mlim) v[m] = smooth2(v[m], P.filt[(size_t)row * NR + amask<N>(t, m)]);
+        }
         fft<N, +1>(v, sh, t, TW);
         if (row <= P.jt) {
           if (MODEL == MODEL_BINARY) store_row<N>(v, B.g[GCT], row, live, t);
@@ -101,6 +104,7 @@ __global__ void __launch_bounds__(GPC * (N / 16)) k_diag_spec(const Bufs<R> B, c
         R a = (R)0, b = (R)0;
         if (ks > (R)1e-12 && amask<N>(t, m) <= mlim) { a = rdiv(in[m].x, ks); b = rdiv(in[m].y, ks); }
         v[m] = d == 0 ? mk<R>(-rmul(ky, b) * sc, rmul(ky, a) * sc) : mk<R>(rmul(kx, b) * sc, -rmul(kx, a) * sc);
+        if (FILT && amask<N>(t, m) <= mlim) v[m] = smooth2(v[m], P.filt[(size_t)row * NR + amask<N>(t, m)]);
       }
       fft<N, +1>(v, sh, t, TW);
       if (row <= P.jt) store_row_pair<N>(v, B.g[GUV], row, d, live, t);

@@ -28,6 +28,7 @@ struct SpecArgs {
   int n, jt, nshell, nph;
   double fx, fy, dk, scale2;
   const int* mrow;
+  const double* filt;  // SMOOTH_FILTER factors [row][|m|] in double (null: the sharp cut)
   const double* k0;  // FP32 contexts: k = 0 modes in double, else null
   double* out;       // ek, ensk, phase spectra (nph x nshell), ekx, eky
 };
@@ -61,7 +62,11 @@ __global__ void k_spectrum(const chns::cx<R>* __restrict__ w, const chns::cx<R>*
     double wr, wi;
     load_mode(w, idx, wr, wi);
     const double pr = wr / ksqr, pi_ = wi / ksqr;
-    const double uxr = -ky * pi_, uxi = ky * pr, uyr = kx * pi_, uyi = -kx * pr;
+    double uxr = -ky * pi_, uxi = ky * pr, uyr = kx * pi_, uyi = -kx * pr;
+    if (A.filt) {  // functions.c:69-72
+      const double f = A.filt[(size_t)row * (n / 2 + 1) + am];
+      uxr = (uxr * f) * f; uxi = (uxi * f) * f; uyr = (uyr * f) * f; uyi = (uyi * f) * f;
+    }
     eu = (uxr * uxr + uxi * uxi) + (uyr * uyr + uyi * uyi);
   }
   eu *= A.scale2;
@@ -93,6 +98,10 @@ __global__ void k_spectrum(const chns::cx<R>* __restrict__ w, const chns::cx<R>*
         br = A.k0[4];
         bi = A.k0[5];
       }
+    }
+    if (A.filt) {
+      const double f = A.filt[(size_t)row * (n / 2 + 1) + am];
+      ar = (ar * f) * f; ai = (ai * f) * f; br = (br * f) * f; bi = (bi * f) * f;
     }
     const double e1 = (ar * ar + ai * ai) * A.scale2;
     atomicAdd(sph + ik, wp * e1);
@@ -156,6 +165,7 @@ int chns_spectrum(chns_ctx* c, double* out) {
   const double scale = 1.0 / ((double)c->p.nx * (double)c->p.ny);
   A.scale2 = scale * scale;
   A.mrow = c->mrow;
+  A.filt = c->filtd;
   A.k0 = c->f32 ? c->k0 : nullptr;
   A.out = dev;
   const int blocks = (int)(((size_t)n * c->nr + 255) / 256);

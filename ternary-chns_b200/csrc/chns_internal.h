@@ -35,7 +35,7 @@ constexpr int kNumG = 6, kNumH = 4;
 struct Launchers {
   // one ETD2RK stage (1 or 2) of the context's model; returns launches enqueued
   int (*stage)(chns_ctx* c, int stage);
-  // S-layout field -> truncated in place
+  // S-layout field -> truncated in place (the sharp cut, or the smooth filter's two products)
   int (*truncate)(chns_ctx* c, void* s);
   // device real (R, nx*ny) -> S-layout spectrum (unnormalised r2c)
   int (*dfft)(chns_ctx* c, const void* real, void* s);
@@ -50,6 +50,8 @@ struct Launchers {
   // (complex elements); scratch holds nb n x (n/2+1) complex fields
   int (*dfftb)(chns_ctx* c, const void* real, size_t rs, void* s, size_t ss, int nb, void* scratch);
   int (*ifftb)(chns_ctx* c, const void* s, size_t ss, void* real, size_t rs, int nb, void* scratch);
+  // the largest dynamic shared memory a step kernel of the context needs (bytes)
+  size_t (*step_smem)(const chns_ctx* c);
 };
 
 const Launchers* launchers_f64(int logn);
@@ -77,6 +79,8 @@ struct chns_ctx {
   void* tmag;         // chns::TmaG (host): tensor maps of the G slots for the row kernels' TMA tiles
   unsigned int* tma_err;  // device word the row kernels flag a timed-out tile wait in
   int* mrow;
+  void* filt;       // SMOOTH filter factors [nx/2+1 rows][nx/2+1 |m|] in the context precision (else null)
+  double* filtd;    // the same in double (FP64 contexts: filt itself)
   void* tw;
   double* k0;       // [12] k = 0 modes (FP32 contexts)
   double* stage;    // FFTW-layout double staging, n * nr complex

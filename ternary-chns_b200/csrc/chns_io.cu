@@ -84,7 +84,7 @@ int chns_read_phase(chns_ctx* c, const char* path1, const char* path2) {
 
 // checkpoint file: magic, the chns_params the context was created with (padding
 // zeroed), then the spectral fields (FFTW layout, FP64) of the model
-static const char kCkptMagic[8] = {'C', 'H', 'N', 'S', 'C', 'K', 'P', '1'};
+static const char kCkptMagic[8] = {'C', 'H', 'N', 'S', 'C', 'K', 'P', '2'};
 
 static chns_params canonical(const chns_params& a) {
   chns_params q;
@@ -108,6 +108,7 @@ static chns_params canonical(const chns_params& a) {
   q.coef_mode = a.coef_mode;
   q.force_amp = a.force_amp;
   q.force_k = a.force_k;
+  q.filter = a.filter;
   return q;
 }
 

@@ -59,6 +59,7 @@ template <class R> struct Par {
   R force_hat;             // its spectral amplitude, added to N_w at (0, force_j)
   double k0coef[6];        // ETD coefficients at k = 0 (double)
   const int* mrow;         // [n/2+1] largest |m| kept by the truncation per row (-1: none)
+  const R* filt;           // SMOOTH_FILTER factors [n/2+1 rows][n/2+1 |m|] (null: the sharp cut)
   const R* coef;           // [6][n/2+1][n/2+1] ETD coefficients at (row, |m|); with a
                            // double-float state, slots 0 and 3 hold e - 1 (expm1) instead of e
   const cx<R>* tw;         // tw[q] = exp(-2 pi i q / n)
@@ -113,6 +114,13 @@ template <class R> __device__ __forceinline__ cx<R> czero() { return mk<R>((R)0,
 template <int N> __device__ __forceinline__ int sidx(int i) { return i <= N / 2 ? i : i - N; }
 
 template <class R> __device__ __forceinline__ R ksq(R kx, R ky) { return radd(rmul(kx, kx), rmul(ky, ky)); }
+
+// SMOOTH_FILTER's truncation of one mode (functions.c:69-72): two products by the
+// filter factor f, each rounded
+template <class R> __device__ __forceinline__ cx<R> smooth2(cx<R> a, R f) {
+  a = mk<R>(rmul(a.x, f), rmul(a.y, f));
+  return mk<R>(rmul(a.x, f), rmul(a.y, f));
+}
 
 // ---------------------------------------------------------------------------
 // asynchronous tile copies (cp.async, 16 bytes each) into shared memory
@@ -555,6 +563,14 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_spec_inv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
 #pragma unroll
       for (int m = 0; m < 16; m++)
         in[m] = ((inmask >> m) & 1) ? src[(size_t)row * N + t + NT * m] : czero<R>();
+      // SMOOTH_FILTER: every output of this field is truncated once, so the loaded
+      // row is filtered once (the products by f commute with the derivative and
+      // velocity factors up to rounding)
+      if (P.filt && live) {
+        const R* fr = P.filt + (size_t)row * (N / 2 + 1);
+#pragma unroll
+        for (int m = 0; m < 16; m++) in[m] = smooth2(in[m], fr[amask<N>(t, m)]);
+      }
       loaded = true;
     }
     const int q = o < 4 ? o : 4 + (o - 4) % 3;  // 0 u, 1 v, 2 dx, 3 dy (w); 4 c_t, 5 dx, 6 dy (c)
@@ -972,7 +988,9 @@ __device__ __forceinline__ cxf split_k0(const double* st, cxf* lo) {
 // modes outside it never reach a right-hand side (every product's inputs are
 // truncated), so their float rounding is not amplified; they are updated in
 // float with their low part left at zero.
-template <int N, class R, int GPC, int MODEL, int STAGE, bool S64>
+// FILT: the context's truncation is SMOOTH_FILTER's (P.filt), a variant of its own
+// so that the sharp cut's kernel carries none of the filter's registers
+template <int N, class R, int GPC, int MODEL, int STAGE, bool S64, bool FILT = false>
 CHNS_STAGE_KERNEL(N, R, GPC) k_spec_fwd_c(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
@@ -1053,6 +1071,7 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_spec_fwd_c(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
             const R q = rmul(fld == 0 ? P.mu1 : P.mu2, ks);
             v[m] = mk<R>(radd(f[m].x, rmul(q, c[m].x)) * P.scale, radd(f[m].y, rmul(q, c[m].y)) * P.scale);
           }
+          if constexpr (FILT) v[m] = smooth2(v[m], P.filt[(size_t)row * NR + amask<N>(t, m)]);
         } else {
           v[m] = czero<R>();
         }

@@ -46,6 +46,14 @@ template <int N, class R> constexpr size_t spec_smem(bool prefetch) {
   return Sizes<N, R>::FFT_SMEM + (prefetch && sizeof(R) == 4 ? prefetch_smem<N, R, Sizes<N, R>::GPC>() : 0);
 }
 
+// the P3 variant of a context: double-float state (FP32 only) and SMOOTH_FILTER
+template <int N, class R, int GPC, int MODEL, int STAGE>
+static auto spec_fwd_c_kernel(bool s64, bool filt) {
+  constexpr bool F32 = sizeof(R) == 4;
+  return s64 ? (filt ? k_spec_fwd_c<N, R, GPC, MODEL, STAGE, F32, true> : k_spec_fwd_c<N, R, GPC, MODEL, STAGE, F32>)
+             : (filt ? k_spec_fwd_c<N, R, GPC, MODEL, STAGE, false, true> : k_spec_fwd_c<N, R, GPC, MODEL, STAGE, false>);
+}
+
 template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   using S = Sizes<N, R>;
   constexpr int GPC = S::GPC;
@@ -120,26 +128,15 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   }
 
   // P3: x forward transforms, mu, N_c, ETD of c
-  if (model == CHNS_MODEL_BINARY) {
-    if (stage == 1) {
-      auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1, F32> : k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 1, false>;
-      set_smem(k, spec_smem<N, R>(model == CHNS_MODEL_BINARY));
-      k<<<rows_all, S::THREADS, spec_smem<N, R>(model == CHNS_MODEL_BINARY), st>>>(B, P);
-    } else {
-      auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 2, F32> : k_spec_fwd_c<N, R, GPC, MODEL_BINARY, 2, false>;
-      set_smem(k, spec_smem<N, R>(model == CHNS_MODEL_BINARY));
-      k<<<rows_all, S::THREADS, spec_smem<N, R>(model == CHNS_MODEL_BINARY), st>>>(B, P);
-    }
-  } else {
-    if (stage == 1) {
-      auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 1, F32> : k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 1, false>;
-      set_smem(k, spec_smem<N, R>(model == CHNS_MODEL_BINARY));
-      k<<<rows_all, S::THREADS, spec_smem<N, R>(model == CHNS_MODEL_BINARY), st>>>(B, P);
-    } else {
-      auto k = s64 ? k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 2, F32> : k_spec_fwd_c<N, R, GPC, MODEL_TERNARY, 2, false>;
-      set_smem(k, spec_smem<N, R>(model == CHNS_MODEL_BINARY));
-      k<<<rows_all, S::THREADS, spec_smem<N, R>(model == CHNS_MODEL_BINARY), st>>>(B, P);
-    }
+  {
+    const bool bin = model == CHNS_MODEL_BINARY;
+    const bool filt = c->filt != nullptr;
+    auto k = bin ? (stage == 1 ? spec_fwd_c_kernel<N, R, GPC, MODEL_BINARY, 1>(s64, filt)
+                               : spec_fwd_c_kernel<N, R, GPC, MODEL_BINARY, 2>(s64, filt))
+                 : (stage == 1 ? spec_fwd_c_kernel<N, R, GPC, MODEL_TERNARY, 1>(s64, filt)
+                               : spec_fwd_c_kernel<N, R, GPC, MODEL_TERNARY, 2>(s64, filt));
+    set_smem(k, spec_smem<N, R>(bin));
+    k<<<rows_all, S::THREADS, spec_smem<N, R>(bin), st>>>(B, P);
   }
   launches++;
   mark(c, KIND_SPEC_FWD_C);
@@ -175,19 +172,41 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   return launches;
 }
 
-template <class R> __global__ void k_truncate(cx<R>* s, const int* __restrict__ mrow, int n) {
+// truncation (functions.c:47-84) of an S-layout field in place: the sharp cut
+// zeroes |m| > mrow[row]; with filt (SMOOTH_FILTER, :69-72) every mode is
+// multiplied by its factor twice
+template <class R>
+__global__ void k_truncate(cx<R>* s, const int* __restrict__ mrow, const R* __restrict__ filt, int n) {
   const int row = blockIdx.y;
   const int lim = mrow[row];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int ms = i <= n / 2 ? i : n - i;
-    if (ms > lim) s[(size_t)row * n + i] = czero<R>();
+    const size_t idx = (size_t)row * n + i;
+    if (filt) s[idx] = smooth2(s[idx], filt[(size_t)row * (n / 2 + 1) + ms]);
+    else if (ms > lim) s[idx] = czero<R>();
   }
 }
 
 template <int N, class R> int truncate_impl(chns_ctx* c, void* s) {
   dim3 grid((N + 255) / 256, N / 2 + 1);
-  k_truncate<R><<<grid, 256, 0, c->stream>>>((cx<R>*)s, c->mrow, N);
+  k_truncate<R><<<grid, 256, 0, c->stream>>>((cx<R>*)s, c->mrow, (const R*)c->filt, N);
   return 1;
+}
+
+// the largest dynamic shared memory of the step's kernels (P2 / P4 grow with the G rows)
+template <int N, class R> size_t step_smem_impl(const chns_ctx* c) {
+  using S = Sizes<N, R>;
+  constexpr int GPC = S::GPC;
+  const TmaG& TG = *static_cast<const TmaG*>(c->tmag);
+  const bool tma = TG.use != 0;
+  const int model = c->p.model;
+  int frags = model == CHNS_MODEL_BINARY    ? row_adv_frags<MODEL_BINARY>()
+              : model == CHNS_MODEL_TERNARY ? row_adv_frags<MODEL_TERNARY>()
+                                            : row_adv_frags<MODEL_NS>();
+  if (model != CHNS_MODEL_NS && row_force_frags<MODEL_BINARY>() > frags) frags = row_force_frags<MODEL_BINARY>();
+  const size_t m = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, c->jt, TG.boxr, TG.nbox, frags);
+  const size_t sp = spec_smem<N, R>(true);
+  return m > sp ? m : sp;
 }
 
 // batched plain transforms: nb fields at strides (in elements of their type);
@@ -254,21 +273,21 @@ template <int N, class R> int diag_impl(chns_ctx* c) {
   const int pairs = S::grid_rows(N / 2);
   double* part = (double*)c->redscratch;
   if (model == CHNS_MODEL_NS) {
-    auto k1 = k_diag_spec<N, R, S::GPC, MODEL_NS>;
+    auto k1 = c->filt ? k_diag_spec<N, R, S::GPC, MODEL_NS, true> : k_diag_spec<N, R, S::GPC, MODEL_NS>;
     set_smem(k1, S::FFT_SMEM);
     k1<<<rows, S::THREADS, S::FFT_SMEM, c->stream>>>(B, P);
     auto k2 = k_diag_row<N, R, S::GPC, MODEL_NS>;
     set_smem(k2, sm);
     k2<<<pairs, S::THREADS, sm, c->stream>>>(B, P, part);
   } else if (model == CHNS_MODEL_BINARY) {
-    auto k1 = k_diag_spec<N, R, S::GPC, MODEL_BINARY>;
+    auto k1 = c->filt ? k_diag_spec<N, R, S::GPC, MODEL_BINARY, true> : k_diag_spec<N, R, S::GPC, MODEL_BINARY>;
     set_smem(k1, S::FFT_SMEM);
     k1<<<rows, S::THREADS, S::FFT_SMEM, c->stream>>>(B, P);
     auto k2 = k_diag_row<N, R, S::GPC, MODEL_BINARY>;
     set_smem(k2, sm);
     k2<<<pairs, S::THREADS, sm, c->stream>>>(B, P, part);
   } else {
-    auto k1 = k_diag_spec<N, R, S::GPC, MODEL_TERNARY>;
+    auto k1 = c->filt ? k_diag_spec<N, R, S::GPC, MODEL_TERNARY, true> : k_diag_spec<N, R, S::GPC, MODEL_TERNARY>;
     set_smem(k1, S::FFT_SMEM);
     k1<<<rows, S::THREADS, S::FFT_SMEM, c->stream>>>(B, P);
     auto k2 = k_diag_row<N, R, S::GPC, MODEL_TERNARY>;
@@ -282,7 +301,8 @@ template <int N, class R> int diag_impl(chns_ctx* c) {
 template <int N, class R> const Launchers* make_launchers() {
   static const Launchers L = {stage_impl<N, R>,     truncate_impl<N, R>, dfft_impl<N, R>,
                               ifft_impl<N, R>,      from_fftw_impl<N, R>, to_fftw_impl<N, R>,
-                              diag_impl<N, R>,      dfftb_impl<N, R>,     ifftb_impl<N, R>};
+                              diag_impl<N, R>,      dfftb_impl<N, R>,     ifftb_impl<N, R>,
+                              step_smem_impl<N, R>};
   return &L;
 }
 

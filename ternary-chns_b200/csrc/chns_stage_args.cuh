@@ -43,6 +43,7 @@ template <class R> Par<R> make_par(const chns_ctx* c) {
   P.force_hat = (R)c->force_hat;
   for (int k = 0; k < 6; k++) P.k0coef[k] = c->k0coef[k];
   P.mrow = c->mrow;
+  P.filt = (const R*)c->filt;
   P.coef = (const R*)c->coef;
   P.tw = (const cx<R>*)c->tw;
   P.k0 = c->k0;

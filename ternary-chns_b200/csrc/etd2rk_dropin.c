@@ -77,6 +77,9 @@ static void dropin_init(void)
     p.dt = cfg_dt;
     p.nu = cfg_nu;
     p.dealias_div = 4.0;                 /* functions.c:56 */
+#ifdef SMOOTH_FILTER
+    p.filter = CHNS_FILTER_SMOOTH;       /* functions.c:69-72 */
+#endif
     p.coef_mode = CHNS_COEF_REFERENCE;   /* etd2rk.c's own phi-function formulas */
     rc = chns_create(&p, &dropin_ctx);
     if (rc != CHNS_OK) dropin_fail("chns_create", rc);

@@ -9,7 +9,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
 
-SMALL_CONFIGS = ["ns32", "bin32", "bin64", "ter32", "ter64", "bindef64", "terdef64"]
+SMALL_CONFIGS = ["ns32", "bin32", "bin64", "ter32", "ter64", "bindef64", "terdef64",
+                 "nssf32", "binsf64", "tersf64", "binsfdef64"]
 
 
 def load_small(name: str) -> dict:

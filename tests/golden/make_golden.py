@@ -14,8 +14,9 @@ the big grids (4096^2, 1024^2) store only the fingerprint.
 
 The reference's source folder is taken from CHNS_REFERENCE_DIR (oracle/build_ref.py).
 
-Usage:  python tests/golden/make_golden.py [--full] [--big] [--init] [--only]
-  (--init: only init_ref.npz; --only: skip the small fixtures and init_ref.npz)
+Usage:  python tests/golden/make_golden.py [--full] [--big] [--init] [--only] [--names a,b]
+  (--init: only init_ref.npz; --only: skip the small fixtures and init_ref.npz;
+  --names: only the named small fixtures)
 """
 from __future__ import annotations
 
@@ -41,6 +42,11 @@ SMALL = [
     ("ter64", 20, 2, 5, 6.0, 0.5),
     ("bindef64", 20, 4, 6, 3.0, 0.5),
     ("terdef64", 20, 4, 6, 3.0, 0.5),
+    # SMOOTH_FILTER builds of the reference
+    ("nssf32", 20, None, 3, 6.0, 1.0),
+    ("binsf64", 20, 1, 5, 6.0, 0.5),
+    ("tersf64", 20, 2, 5, 6.0, 0.5),
+    ("binsfdef64", 20, 4, 6, 3.0, 0.5),
 ]
 FULL = [
     # binary spinodal run: 256^2, omega = 0, c = (1 + U(+-0.05) - mean)/2, 1000 steps
@@ -108,8 +114,10 @@ def fingerprint_rel_err(fp_ref: dict, fp: dict) -> float:
     return float(max(e_low, e_proj, e_norm))
 
 
-def make_small(O):
+def make_small(O, names=None):
     for name, steps, ps, ws, kmax, rms in SMALL:
+        if names and name not in names:
+            continue
         p = O.ref_config_params(name)
         R = O.RefLib(name)
         n = p["nx"]
@@ -183,7 +191,9 @@ def make_init(O):
 if __name__ == "__main__":
     import oracle as O
     O.build_ref.build_all()
-    if "--init" in sys.argv:
+    if "--names" in sys.argv:
+        make_small(O, sys.argv[sys.argv.index("--names") + 1].split(","))
+    elif "--init" in sys.argv:
         make_init(O)
     elif "--only" not in sys.argv:
         make_small(O)

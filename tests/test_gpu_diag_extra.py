@@ -29,7 +29,7 @@ def chns():
 
 
 @pytest.mark.parametrize("prec", [0, 1])
-@pytest.mark.parametrize("name", ["ns32", "bin32", "ter32", "bindef64", "terdef64"])
+@pytest.mark.parametrize("name", ["ns32", "bin32", "ter32", "bindef64", "terdef64", "nssf32", "binsf64", "tersf64"])
 def test_spectrum_matches_reference(chns, name, prec):
     import oracle as O
 

@@ -124,7 +124,7 @@ def test_steps_match_reference(chns, name):
             assert rel_l2(a, b) <= 1e-11, (name, k, rel_l2(a, b))
 
 
-@pytest.mark.parametrize("name", ["bin32", "ter32", "bindef64", "terdef64"])
+@pytest.mark.parametrize("name", ["bin32", "ter32", "bindef64", "terdef64", "binsf64", "tersf64", "binsfdef64"])
 def test_diagnostics_match_reference(chns, name):
     g = load_small(name)
     with _ctx(chns, g["params"]) as c:
@@ -136,7 +136,7 @@ def test_diagnostics_match_reference(chns, name):
         assert np.allclose(ke[:nk], g["ke0"], rtol=1e-10, atol=1e-12)
 
 
-@pytest.mark.parametrize("name", ["bin64", "ter64"])
+@pytest.mark.parametrize("name", ["bin64", "ter64", "binsf64", "tersf64"])
 def test_phase_init_matches_reference(chns, name):
     """init.c INIT_READ_DATA path: dfft + truncation of the real phase fields."""
     g = load_small(name)

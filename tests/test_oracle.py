@@ -57,7 +57,7 @@ def test_restatement_matches_reference_golden(name):
     assert rel_l2(o.ifft(g["fft_dfft"]), g["fft_ifft"]) <= 1e-14
 
 
-@pytest.mark.parametrize("name", ["bin32", "ter32", "bindef64", "ns32"])
+@pytest.mark.parametrize("name", ["bin32", "ter32", "bindef64", "ns32", "nssf32", "binsf64", "tersf64"])
 def test_restatement_bitwise_vs_live_reference(name):
     if not os.path.isfile(O.build_ref.lib_path(name)):
         pytest.skip("oracle/_ref not built (reference sources absent)")
