@@ -306,6 +306,17 @@ int chns_tma_tiles(const chns_ctx *ctx);
  * has no TMA tiles (chns_tma_tiles). */
 int chns_debug_tile_waits(chns_ctx *ctx, int spins, int skip_copies);
 
+/* Autotuning hook (no reference counterpart): overrides, for contexts created
+ * afterwards in this process, a launch-shape choice of the tuned tables
+ * (ternary-chns_b200/csrc/chns_tuned.h).  knob CHNS_TUNE_TMA_BOX_ROWS: rows per
+ * TMA box of the row kernels' tiles, a multiple of 8 in 8..256;
+ * CHNS_TUNE_P1_SPLIT: 1 runs the spectral inverse pass with two CTAs per row, 0
+ * with one.  value -1 restores the table.  Results are bitwise the same under
+ * every choice; only the speed changes.  Not thread-safe: set before creating
+ * contexts. */
+enum { CHNS_TUNE_TMA_BOX_ROWS = 1, CHNS_TUNE_P1_SPLIT = 2 };
+int chns_tune_override(int knob, int value);
+
 /* Tracing: runs `reps` steps launching the kernels one by one (not from the
  * graph) with a CUDA event recorded after each launch on the context's stream;
  * writes the mean duration of every launch of one step to ms[] and its kind to

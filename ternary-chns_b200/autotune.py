@@ -1,41 +1,69 @@
 #!/usr/bin/env python3
-"""Autotuner of the CTA shape of the step and transform kernels (csrc/chns_tuned.h).
+"""Autotuner of the launch shapes of the step and transform kernels (csrc/chns_tuned.h).
 
-Every row and column kernel runs n/16 threads per transform of n points and
-packs several transforms into one CTA.  Few threads per CTA spread the rows of a
-small grid over all SMs; more threads share twiddles and give wider tile loads
-on large grids.  This script builds one library variant per candidate
-(-DCHNS_CTA_THREADS=T), times the forward binary and ternary steps of every grid
-size in both precisions with each variant (a fresh process per variant), and
-writes the header with the fastest candidate per size and precision (highest
-summed steps/s of the two models).  It needs a GPU:
+Three choices per grid size and precision, each timed on forward binary and
+ternary steps (the candidate with the highest summed steps/s wins):
 
-    python ternary-chns_b200/autotune.py --out ternary-chns_b200/csrc/chns_tuned.h
+* threads per CTA (``threads`` pass).  Every row and column kernel runs n/16
+  threads per transform of n points and packs several transforms into one CTA.
+  Few threads per CTA spread the rows of a small grid over all SMs; more threads
+  share twiddles and give wider tile loads on large grids.  The CTA shape is a
+  template argument, so this pass builds one library variant per candidate
+  (-DCHNS_CTA_THREADS=T) and times it in a fresh process.
+* rows per TMA box of the row kernels' tiles (``box`` pass, 64 / 128 / 256): a
+  tile is whole boxes, so smaller boxes fetch fewer zero rows beyond the cut and
+  take less shared memory, for more copies per tile.
+* the P1 split (``split`` pass): the spectral inverse pass with two CTAs per row
+  (half the outputs each) or one.
+
+The box and split choices are run-time (chns_tune_override, for contexts created
+afterwards), so those passes time one library.  A box or split candidate replaces
+the current table entry only when it is more than ``--margin`` (1%) faster, so
+that run-to-run noise does not flip choices.  Results are bitwise the same under
+every choice (tests/test_gpu_tuning.py).
+
+The transforms' radix order is not a knob: a thread holds 16 elements, so every
+stage but one is radix 16, the remaining radix-2/4/8 stage must come first (the
+last stage leaves the result in registers in natural order), and moving it
+changes the twiddle multiplies by at most one per thread and stage.
+
+Passes not run keep the values of the current header.  It needs a GPU:
+
+    python ternary-chns_b200/autotune.py --passes threads,box,split \\
+        --out ternary-chns_b200/csrc/chns_tuned.h --report autotune.json
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import re
 import subprocess
 import sys
 import tempfile
 import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CANDIDATES = [32, 64, 128, 256]
+TUNED = os.path.join(HERE, "csrc", "chns_tuned.h")
+THREADS = [32, 64, 128, 256]
+BOX_ROWS = [64, 128, 256]
+SPLIT = [0, 1]
 TIMED_SIZES = [256, 512, 1024, 2048, 4096]
 ALL_SIZES = [32, 64, 128, 256, 512, 1024, 2048, 4096]
+TABLES = ["kCtaThreads", "kTmaBoxRows", "kSpecInvSplit"]
 
 
-def time_variant(lib: str, steps_small: int = 200, steps_large: int = 40) -> dict:
-    """Steps/s of each (model, n, precision) with the library at `lib`."""
+def time_variant(lib: str, box: int = -1, split: int = -1, steps_small: int = 200, steps_large: int = 40) -> dict:
+    """Steps/s of each (model, n, precision) with the library at `lib` and the
+    given run-time overrides (-1: the tuned table)."""
     import numpy as np
 
     sys.path.insert(0, HERE)
     import chns_b200 as C
 
     C.load_library(lib)
+    C.tune_override(C.TUNE_TMA_BOX_ROWS, box)
+    C.tune_override(C.TUNE_P1_SPLIT, split)
     out = {}
     rng = np.random.default_rng(0)
     for model in (C.MODEL_BINARY, C.MODEL_TERNARY):
@@ -59,66 +87,134 @@ def time_variant(lib: str, steps_small: int = 200, steps_large: int = 40) -> dic
                         c.synchronize()
                         best = max(best, steps / (time.perf_counter() - t0))
                 out[f"{model}/{n}/{prec}"] = best
+    C.tune_override(C.TUNE_TMA_BOX_ROWS, -1)
+    C.tune_override(C.TUNE_P1_SPLIT, -1)
     return out
 
 
-def header(choice: dict) -> str:
-    f64 = ", ".join(str(choice[(n, 0)]) for n in ALL_SIZES)
-    f32 = ", ".join(str(choice[(n, 1)]) for n in ALL_SIZES)
-    return f"""// chns_tuned.h -- threads per CTA of the step and transform kernels for each
-// grid size and precision (index log2(n) - 5, n = 32 .. 4096).  Chosen by
-// ternary-chns_b200/autotune.py from forward-step timings of the binary and
-// ternary models on a B200: the candidate with the highest summed steps/s.
-// Each CTA runs threads / (n/16) transforms of n points side by side; small
-// grids want few threads per CTA so that the rows spread over all 148 SMs.
+def read_tables(path: str = TUNED) -> dict:
+    """{(table, prec): [8 values]} of a tuned header (prec 0 = F64, 1 = F32)."""
+    text = open(path).read()
+    out = {}
+    for name in TABLES:
+        for prec, suf in ((0, "F64"), (1, "F32")):
+            m = re.search(rf"{name}{suf}\[8\]\s*=\s*\{{([^}}]*)\}}", text)
+            out[(name, prec)] = [int(v) for v in m.group(1).split(",")]
+    return out
+
+
+def header(t: dict) -> str:
+    def row(name, prec):
+        return ", ".join(str(v) for v in t[(name, prec)])
+
+    return f"""// chns_tuned.h -- launch shapes of the step and transform kernels for each grid
+// size and precision (index log2(n) - 5, n = 32 .. 4096): threads per CTA, TMA box
+// rows and the P1 split.  Chosen by ternary-chns_b200/autotune.py from
+// forward-step timings of the binary and ternary models on a B200: the candidate
+// with the highest summed steps/s.  Each CTA runs threads / (n/16) transforms of
+// n points side by side; small grids want few threads per CTA so that the rows
+// spread over all 148 SMs.
 #pragma once
 
 namespace chns {{
 
-constexpr int kCtaThreadsF64[8] = {{{f64}}};
-constexpr int kCtaThreadsF32[8] = {{{f32}}};
+constexpr int kCtaThreadsF64[8] = {{{row("kCtaThreads", 0)}}};
+constexpr int kCtaThreadsF32[8] = {{{row("kCtaThreads", 1)}}};
+
+// Rows per TMA box of the row kernels' tiles (a tile is whole boxes, so smaller
+// boxes over-fetch fewer zero rows beyond the cut at the price of more copies).
+constexpr int kTmaBoxRowsF64[8] = {{{row("kTmaBoxRows", 0)}}};
+constexpr int kTmaBoxRowsF32[8] = {{{row("kTmaBoxRows", 1)}}};
+
+// P1 with two CTAs per row (each half of the outputs): 1 = on.
+constexpr int kSpecInvSplitF64[8] = {{{row("kSpecInvSplit", 0)}}};
+constexpr int kSpecInvSplitF32[8] = {{{row("kSpecInvSplit", 1)}}};
 
 }}  // namespace chns
 """
 
 
+def _time_in_process(lib: str, box: int = -1, split: int = -1) -> dict:
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--time", lib, "--box", str(box),
+                        "--split", str(split)], capture_output=True, text=True, check=True)
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def _score(res: dict, n: int, prec: int) -> float:
+    return sum(res[f"{m}/{n}/{prec}"] for m in (1, 2))
+
+
+def _pick(results: dict, table: list, prec: int, margin: float, allowed=lambda cand, n: True) -> list:
+    """New table: per timed size the best candidate, kept at the current value
+    unless the best beats it by more than `margin` (when the current value was timed)."""
+    out = list(table)
+    for n in TIMED_SIZES:
+        li = ALL_SIZES.index(n)
+        score = {cand: _score(res, n, prec) for cand, res in results.items() if allowed(cand, n)}
+        best = max(score, key=score.get)
+        cur = table[li]
+        if cur in score and score[best] <= score[cur] * (1 + margin):
+            best = cur
+        out[li] = best
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--passes", default="threads,box,split", help="comma list of threads, box, split")
     ap.add_argument("--out", required=False, help="header to write")
+    ap.add_argument("--report", help="also write the measured tables (JSON) here")
+    ap.add_argument("--margin", type=float, default=0.01, help="gain a box / split change needs")
+    ap.add_argument("--lib", help="library the box and split passes time (default: the in-tree build)")
     ap.add_argument("--time", help="(internal) time one library variant and print JSON")
-    ap.add_argument("--report", help="also write the measured table (JSON) here")
+    ap.add_argument("--box", type=int, default=-1, help="(internal) box-rows override of --time")
+    ap.add_argument("--split", type=int, default=-1, help="(internal) P1-split override of --time")
     a = ap.parse_args()
     if a.time:
-        print(json.dumps(time_variant(a.time)))
+        print(json.dumps(time_variant(a.time, a.box, a.split)))
         return
     sys.path.insert(0, HERE)
     import build as B
 
-    results = {}
-    with tempfile.TemporaryDirectory() as tmp:
-        for t in CANDIDATES:
-            lib = os.path.join(tmp, f"t{t}", "libchns_b200.so")
-            B.build(defines=(f"CHNS_CTA_THREADS={t}",), build_dir=os.path.join(tmp, f"b{t}"), lib=lib)
-            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--time", lib], capture_output=True,
-                               text=True, check=True)
-            results[t] = json.loads(r.stdout.strip().splitlines()[-1])
-            print(f"threads {t}:", json.dumps(results[t]), flush=True)
-    choice = {}
-    for n in ALL_SIZES:
+    passes = [p for p in a.passes.split(",") if p]
+    tables = read_tables()
+    report = {}
+    if "threads" in passes:
+        results = {}
+        with tempfile.TemporaryDirectory() as tmp:
+            for t in THREADS:
+                lib = os.path.join(tmp, f"t{t}", "libchns_b200.so")
+                B.build(defines=(f"CHNS_CTA_THREADS={t}",), build_dir=os.path.join(tmp, f"b{t}"), lib=lib)
+                results[t] = _time_in_process(lib)
+                print(f"threads {t}:", json.dumps(results[t]), flush=True)
         for prec in (0, 1):
-            if n not in TIMED_SIZES:
-                choice[(n, prec)] = 32
-                continue
-            score = {t: sum(results[t][f"{m}/{n}/{prec}"] for m in (1, 2)) for t in CANDIDATES
-                     if t >= n // 16 or t == CANDIDATES[-1]}
-            choice[(n, prec)] = max(score, key=score.get)
-    text = header(choice)
+            # a transform needs n/16 threads: a smaller candidate runs as one transform per CTA
+            tables[("kCtaThreads", prec)] = _pick(results, tables[("kCtaThreads", prec)], prec, 0.0,
+                                                  lambda t, n: t >= n // 16 or t == THREADS[-1])
+        report["threads"] = {str(k): v for k, v in results.items()}
+    lib = a.lib or B.LIB
+    if not os.path.isfile(lib):
+        raise SystemExit(f"{lib} is missing: build the library first (build.py)")
+    if "box" in passes:
+        results = {b: _time_in_process(lib, box=b) for b in BOX_ROWS}
+        for prec in (0, 1):
+            tables[("kTmaBoxRows", prec)] = _pick(results, tables[("kTmaBoxRows", prec)], prec, a.margin)
+        report["box"] = {str(k): v for k, v in results.items()}
+        print("box:", json.dumps(report["box"]), flush=True)
+    if "split" in passes:
+        results = {s: _time_in_process(lib, split=s) for s in SPLIT}
+        for prec in (0, 1):
+            tables[("kSpecInvSplit", prec)] = _pick(results, tables[("kSpecInvSplit", prec)], prec, a.margin)
+        report["split"] = {str(k): v for k, v in results.items()}
+        print("split:", json.dumps(report["split"]), flush=True)
+    text = header(tables)
     if a.out:
         with open(a.out, "w") as f:
             f.write(text)
     if a.report:
+        report["chosen"] = {f"{k[0]}/{k[1]}": v for k, v in tables.items()}
         with open(a.report, "w") as f:
-            json.dump({str(t): v for t, v in results.items()}, f, indent=1)
+            json.dump(report, f, indent=1)
     print(text)
 
 

@@ -125,10 +125,24 @@ def load_library(path: str = LIB_PATH):
     L.chns_ensemble_persistent.restype = ip
     L.chns_dfft_noalloc.argtypes = [vp, vp, ip, vp]
     L.chns_dfft_noalloc.restype = ip
+    L.chns_tune_override.argtypes = [ip, ip]
+    L.chns_tune_override.restype = ip
+    L.chns_truncation_factor.argtypes = [vp, ip, ip, vp]
+    L.chns_truncation_factor.restype = ip
     L.chns_status_string.restype = ctypes.c_char_p
     L.chns_status_string.argtypes = [ip]
     _lib = L
     return L
+
+
+# chns_tune_override knobs: rows per TMA box of the row kernels' tiles; P1 with two CTAs per row
+TUNE_TMA_BOX_ROWS, TUNE_P1_SPLIT = 1, 2
+
+
+def tune_override(knob: int, value: int) -> None:
+    """Overrides a launch-shape choice of the tuned tables for contexts created
+    afterwards in this process (value -1: the table); results stay bitwise the same."""
+    _check(load_library().chns_tune_override(int(knob), int(value)), "chns_tune_override")
 
 
 def default_params(model: int, n: int) -> dict:

@@ -18,6 +18,7 @@
 
 #include "chns_internal.h"
 #include "chns_kernels.cuh"
+#include "chns_tuned.h"
 
 namespace chns {
 #define CHNS_DECL(NN)                  \
@@ -235,6 +236,11 @@ void free_all(chns_ctx* c) {
 // unused, with cp.async tiles instead, when the driver's encoder is unavailable
 // or refuses a map).  Each G slot holds rows 0..jt; a tile is nbox boxes of
 // {2 complex, boxr rows}.
+// chns_tune_override's process-wide choices (-1: the tuned table)
+static int g_tune_box_rows = -1, g_tune_p1_split = -1;
+
+static int tuned_index(int n) { return ilog2_exact(n) - 5; }
+
 int build_tma(chns_ctx* c) {
   chns::TmaG* T = new (std::nothrow) chns::TmaG();
   if (!T) return CHNS_ERR_NOMEM;
@@ -242,7 +248,10 @@ int build_tma(chns_ctx* c) {
   T->use = 0;
   T->err = c->tma_err;
   const int rows = c->jt + 1;
-  T->boxr = rows >= 256 ? 256 : (rows + 7) / 8 * 8;
+  const int li = tuned_index(c->n);
+  const int cap = g_tune_box_rows > 0 ? g_tune_box_rows
+                                      : (c->f32 ? chns::kTmaBoxRowsF32[li] : chns::kTmaBoxRowsF64[li]);
+  T->boxr = rows >= cap ? cap : (rows + 7) / 8 * 8;
   T->nbox = (rows + T->boxr - 1) / T->boxr;
   T->ecx = c->f32 ? 1 : 2;
   void* fn = nullptr;
@@ -390,6 +399,11 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
   c->f32 = p.precision != CHNS_FP64;
   c->st64 = p.precision == CHNS_FP32_STATE64;
   c->rsz = c->f32 ? 4 : 8;
+  {
+    const int li = tuned_index(c->n);
+    c->p1_split = g_tune_p1_split >= 0 ? g_tune_p1_split != 0
+                                       : (c->f32 ? chns::kSpecInvSplitF32[li] : chns::kSpecInvSplitF64[li]) != 0;
+  }
   const int logn = ilog2_exact(c->n);
   c->L = c->f32 ? chns::launchers_f32(logn) : chns::launchers_f64(logn);
   if (!c->L) {
@@ -961,6 +975,20 @@ int chns_diagnostics(chns_ctx* c, double* out_fe, double* out_ke) {
 int chns_launches_per_step(const chns_ctx* c) { return c ? c->launches_per_step : 0; }
 
 int chns_tma_tiles(const chns_ctx* c) { return c && static_cast<const chns::TmaG*>(c->tmag)->use ? 1 : 0; }
+
+int chns_tune_override(int knob, int value) {
+  if (knob == CHNS_TUNE_TMA_BOX_ROWS) {
+    if (value != -1 && (value < 8 || value > 256 || value % 8 != 0)) return CHNS_ERR_ARG;
+    g_tune_box_rows = value;
+    return CHNS_OK;
+  }
+  if (knob == CHNS_TUNE_P1_SPLIT) {
+    if (value != -1 && value != 0 && value != 1) return CHNS_ERR_ARG;
+    g_tune_p1_split = value;
+    return CHNS_OK;
+  }
+  return CHNS_ERR_ARG;
+}
 
 int chns_debug_tile_waits(chns_ctx* c, int spins, int skip_copies) {
   if (!c || spins < 0) return CHNS_ERR_ARG;

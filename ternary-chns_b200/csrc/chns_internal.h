@@ -62,6 +62,7 @@ const Launchers* launchers_f32(int logn);
 struct chns_ctx {
   chns_params p;
   int n, nr, jt;
+  bool p1_split;  // P1 with two CTAs per row (chns_tuned.h or chns_tune_override)
   bool f32;
   bool st64;   // FP32 context with a double-float state (CHNS_FP32_STATE64)
   size_t rsz;  // bytes per real scalar (4 or 8)

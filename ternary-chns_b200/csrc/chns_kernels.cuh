@@ -513,10 +513,12 @@ template <int N> __device__ __forceinline__ int amask(int t, int m) {
 // nonlin.c:30-48, velocity.c:12-42, surface_tension.c:20-22,57-75,
 // nonlin.c:177-198,259-284, chem_potential.c:256-261
 // ---------------------------------------------------------------------------
-// P1 runs two CTAs per row (grid.y = 2) on grids up to 1024^2
+// SPLIT: P1 runs two CTAs per row (grid.y = 2), each with half of the outputs
+// (the launcher's choice per grid size, chns_tuned.h; this default is the
+// persistent ensemble kernel's)
 template <int N> constexpr bool spec_inv_split() { return N <= 1024; }
 
-template <int N, class R, int GPC, int MODEL>
+template <int N, class R, int GPC, int MODEL, bool SPLIT = spec_inv_split<N>()>
 CHNS_STAGE_KERNEL(N, R, GPC) k_spec_inv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
   constexpr int NT = N / 16;
   extern __shared__ __align__(16) unsigned char smem_all[];
@@ -543,14 +545,14 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_spec_inv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
   // One loop with one inverse transform keeps the kernel small.  The y derivative
   // of c commutes with the x transform (ky is constant along the row), so dy c is
   // i ky times the transformed c_t and gets no transform of its own.
-  // Grids up to 1024^2 split the outputs between the two CTAs of a row
-  // (CHNS_BY), half the transforms each: twice the CTAs for rows too few to
-  // fill the GPU (measured: 5-8% more steps/s at 256^2-1024^2; at 4096^2 the
-  // second read of the input row costs more than it gains).
+  // SPLIT divides the outputs between the two CTAs of a row (CHNS_BY), half
+  // the transforms each: twice the CTAs for rows too few to fill the GPU
+  // (measured: 5-8% more steps/s at 256^2-1024^2; at 4096^2 the second read of
+  // the input row costs more than it gains).
   // The vorticity's outputs run in the order dx w, dy w, u, v so that w can be
   // turned into psi = w / k^2 in place once (velocity.c:12-42) for both u and v.
   constexpr int NOUT = MODEL == MODEL_NS ? 4 : (MODEL == MODEL_BINARY ? 7 : 10);
-  constexpr int OSPLIT = spec_inv_split<N>() ? (MODEL == MODEL_NS ? 2 : (MODEL == MODEL_BINARY ? 3 : 4)) : NOUT;
+  constexpr int OSPLIT = SPLIT ? (MODEL == MODEL_NS ? 2 : (MODEL == MODEL_BINARY ? 3 : 4)) : NOUT;
   const int obeg = CHNS_BY == 0 ? 0 : OSPLIT, oend = CHNS_BY == 0 ? OSPLIT : NOUT;
   bool loaded = false;
 #pragma unroll 1

@@ -75,17 +75,17 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
 
   // P1: spectral fan-out and x inverse transforms
   if (model == CHNS_MODEL_NS) {
-    auto k = k_spec_inv<N, R, GPC, MODEL_NS>;
+    auto k = c->p1_split ? k_spec_inv<N, R, GPC, MODEL_NS, true> : k_spec_inv<N, R, GPC, MODEL_NS, false>;
     set_smem(k, S::FFT_SMEM);
-    k<<<dim3(rows_inv, spec_inv_split<N>() ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    k<<<dim3(rows_inv, c->p1_split ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
   } else if (model == CHNS_MODEL_BINARY) {
-    auto k = k_spec_inv<N, R, GPC, MODEL_BINARY>;
+    auto k = c->p1_split ? k_spec_inv<N, R, GPC, MODEL_BINARY, true> : k_spec_inv<N, R, GPC, MODEL_BINARY, false>;
     set_smem(k, S::FFT_SMEM);
-    k<<<dim3(rows_inv, spec_inv_split<N>() ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    k<<<dim3(rows_inv, c->p1_split ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
   } else {
-    auto k = k_spec_inv<N, R, GPC, MODEL_TERNARY>;
+    auto k = c->p1_split ? k_spec_inv<N, R, GPC, MODEL_TERNARY, true> : k_spec_inv<N, R, GPC, MODEL_TERNARY, false>;
     set_smem(k, S::FFT_SMEM);
-    k<<<dim3(rows_inv, spec_inv_split<N>() ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    k<<<dim3(rows_inv, c->p1_split ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
   }
   launches++;
   mark(c, KIND_SPEC_INV);

@@ -90,6 +90,16 @@ def test_truncation_factors_equal_the_restatement(chns, name):
         assert got[0, 0] == 1.0 and 0.0 < got.min() < 1e-30  # the corner (n/2, n/2): exp(-36)^2
 
 
+def test_tune_override_checks_its_arguments(chns):
+    C, L = chns
+    for knob, bad in ((C.TUNE_TMA_BOX_ROWS, (0, 4, 12, 264, -2)), (C.TUNE_P1_SPLIT, (2, -2)), (7, (1,))):
+        for v in bad:
+            assert L.chns_tune_override(knob, v) == -1, (knob, v)
+    for knob, good in ((C.TUNE_TMA_BOX_ROWS, (8, 64, 256, -1)), (C.TUNE_P1_SPLIT, (0, 1, -1))):
+        for v in good:
+            assert L.chns_tune_override(knob, v) == 0, (knob, v)
+
+
 def test_tables_reject_bad_arguments(chns):
     C, L = chns
     p = C.make_params(load_small("bin64")["params"])
