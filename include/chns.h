@@ -311,10 +311,12 @@ int chns_debug_tile_waits(chns_ctx *ctx, int spins, int skip_copies);
  * (ternary-chns_b200/csrc/chns_tuned.h).  knob CHNS_TUNE_TMA_BOX_ROWS: rows per
  * TMA box of the row kernels' tiles, a multiple of 8 in 8..256;
  * CHNS_TUNE_P1_SPLIT: 1 runs the spectral inverse pass with two CTAs per row, 0
- * with one.  value -1 restores the table.  Results are bitwise the same under
- * every choice; only the speed changes.  Not thread-safe: set before creating
- * contexts. */
-enum { CHNS_TUNE_TMA_BOX_ROWS = 1, CHNS_TUNE_P1_SPLIT = 2 };
+ * with one; CHNS_TUNE_P4_GRAD: 1 keeps grad c_i in real space from the advection
+ * pass for the force pass (one more device field per phase field), 0 has the force
+ * pass transform it again.  value -1 restores the table.  Results are bitwise the
+ * same under every choice; only the speed changes.  Not thread-safe: set before
+ * creating contexts. */
+enum { CHNS_TUNE_TMA_BOX_ROWS = 1, CHNS_TUNE_P1_SPLIT = 2, CHNS_TUNE_P4_GRAD = 3 };
 int chns_tune_override(int knob, int value);
 
 /* Tracing: runs `reps` steps launching the kernels one by one (not from the

@@ -216,7 +216,7 @@ void free_all(chns_ctx* c) {
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   void* ptrs[] = {c->state[0], c->state[1], c->state[2], c->saved[0], c->saved[1], c->saved[2], c->nw,
                   c->coef, c->mrow, c->tw, c->k0, c->stage, c->realbuf, c->realdbl, c->red, c->redscratch,
-                  c->statelo[0], c->statelo[1], c->statelo[2], c->tma_err, c->filt,
+                  c->statelo[0], c->statelo[1], c->statelo[2], c->tma_err, c->filt, c->gradr,
                   (void*)c->filtd == c->filt ? nullptr : (void*)c->filtd};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -237,7 +237,7 @@ void free_all(chns_ctx* c) {
 // or refuses a map).  Each G slot holds rows 0..jt; a tile is nbox boxes of
 // {2 complex, boxr rows}.
 // chns_tune_override's process-wide choices (-1: the tuned table)
-static int g_tune_box_rows = -1, g_tune_p1_split = -1;
+static int g_tune_box_rows = -1, g_tune_p1_split = -1, g_tune_p4_grad = -1;
 
 static int tuned_index(int n) { return ilog2_exact(n) - 5; }
 
@@ -403,6 +403,9 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
     const int li = tuned_index(c->n);
     c->p1_split = g_tune_p1_split >= 0 ? g_tune_p1_split != 0
                                        : (c->f32 ? chns::kSpecInvSplitF32[li] : chns::kSpecInvSplitF64[li]) != 0;
+    c->p4_grad = p.model != CHNS_MODEL_NS &&
+                 (g_tune_p4_grad >= 0 ? g_tune_p4_grad != 0
+                                      : (c->f32 ? chns::kP4GradF32[li] : chns::kP4GradF64[li]) != 0);
   }
   const int logn = ilog2_exact(c->n);
   c->L = c->f32 ? chns::launchers_f32(logn) : chns::launchers_f64(logn);
@@ -482,6 +485,7 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
   if (rc == CHNS_OK) rc = dmalloc(&c->nw, ncx * cxsz);
   for (int k = 0; k < chns::kNumG && rc == CHNS_OK; k++) rc = dmalloc(&c->g[k], ngx * cxsz);
   for (int k = 0; k < chns::kNumH && rc == CHNS_OK; k++) rc = dmalloc(&c->h[k], nhx * cxsz);
+  if (rc == CHNS_OK && c->p4_grad) rc = dmalloc(&c->gradr, (size_t)p.model * n * n * cxsz);
   if (rc == CHNS_OK) rc = dmalloc(&c->coef, 6 * tsz * c->rsz);
   if (rc == CHNS_OK) rc = dmalloc((void**)&c->mrow, nr * sizeof(int));
   if (rc == CHNS_OK) rc = dmalloc(&c->tw, (size_t)n * cxsz);
@@ -982,9 +986,9 @@ int chns_tune_override(int knob, int value) {
     g_tune_box_rows = value;
     return CHNS_OK;
   }
-  if (knob == CHNS_TUNE_P1_SPLIT) {
+  if (knob == CHNS_TUNE_P1_SPLIT || knob == CHNS_TUNE_P4_GRAD) {
     if (value != -1 && value != 0 && value != 1) return CHNS_ERR_ARG;
-    g_tune_p1_split = value;
+    (knob == CHNS_TUNE_P1_SPLIT ? g_tune_p1_split : g_tune_p4_grad) = value;
     return CHNS_OK;
   }
   return CHNS_ERR_ARG;

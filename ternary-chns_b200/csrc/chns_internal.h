@@ -63,6 +63,7 @@ struct chns_ctx {
   chns_params p;
   int n, nr, jt;
   bool p1_split;  // P1 with two CTAs per row (chns_tuned.h or chns_tune_override)
+  bool p4_grad;   // grad c_i from P2 in real space for P4 (chns_tuned.h or chns_tune_override)
   bool f32;
   bool st64;   // FP32 context with a double-float state (CHNS_FP32_STATE64)
   size_t rsz;  // bytes per real scalar (4 or 8)
@@ -76,6 +77,7 @@ struct chns_ctx {
   void* nw;
   void* g[12];
   void* h[7];
+  void* gradr;      // p4_grad: real-space grad c_i of a stage (P2 -> P4), model x n x n complex of the context precision
   void* coef;
   void* tmag;         // chns::TmaG (host): tensor maps of the G slots for the row kernels' TMA tiles
   unsigned int* tma_err;  // device word the row kernels flag a timed-out tile wait in

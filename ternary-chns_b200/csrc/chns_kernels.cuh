@@ -79,6 +79,7 @@ template <class R> struct Bufs {
   cx<R>* x2;
   cx<R>* nw;
   cx<R>* lo[3];  // FP32 contexts with a double-float state: low parts of w, c1, c2 (else null)
+  cx<R>* gr;     // (dx c_i, dy c_i) in real space, [field][x-row][y]: written by P2, read by P4
   cx<R>* g[NG];
   cx<R>* h[NH];
 };
@@ -683,7 +684,9 @@ __device__ __forceinline__ RowSrc<R> adv_src(const Bufs<R>& B, int it, int i0) {
   return RowSrc<R>{B.g[slot], 2 * N, 2 * (i0 + h), 2 * slot};
 }
 
-template <int N, class R, int GPC, int MODEL, bool JT4 = false>
+// GR: the stage keeps grad c_i in real space for P4 (Bufs::gr), which then
+// transforms only mu (the context's choice per grid size, chns_tuned.h)
+template <int N, class R, int GPC, int MODEL, bool JT4 = false, bool GR = false>
 CHNS_STAGE_KERNEL(N, R, GPC) k_row_adv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS_TMAG_PARAM T) {
   using Sc = AdvSchedule<MODEL>;
   constexpr int NT = N / 16;
@@ -744,6 +747,8 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_row_adv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS
         // one complex row and stored as a plain field, A at HAB, B behind it.  The
         // group thus writes both halves of each 16-byte pair of x-rows at once, and
         // P3 reads whole rows.
+        // GR: grad c of this x-row stays in real space for P4 (no second transform there)
+        if (GR && r == 2) store_row<N>(v, B.gr, i0 + h, live, t);
         Frag<N, R>& kp = r == 1 ? keep : keep2;
         if (h == 0) {
 #pragma unroll
@@ -768,12 +773,16 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_row_adv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS
           }
         }
       } else if (r == 2) {
-        // ternary: B1 = u dx c1 + v dy c1 (nonlin.c:292-293), stored with A as a pair field
+        // ternary: B1 = u dx c1 + v dy c1 (nonlin.c:292-293), stored with A as a pair field;
+        // GR: grad c1 of this x-row stays in real space for P4
+        if (GR) store_row<N>(v, B.gr, i0 + h, live, t);
 #pragma unroll
         for (int m = 0; m < 16; m++) v[m] = mk<R>(a[m], dot2(z[m], v[m]));
         dst = B.h[HAB]; stride = 2 * N; off = 2 * (i0 + h);
       } else {
-        // B2 = u dx c2 + v dy c2 (nonlin.c:334-335) of x-rows i0, i1, transformed together
+        // B2 = u dx c2 + v dy c2 (nonlin.c:334-335) of x-rows i0, i1, transformed together;
+        // GR: grad c2 of this x-row stays in real space for P4
+        if (GR) store_row<N>(v, B.gr + (size_t)N * N, i0 + h, live, t);
         if (h == 0) {
 #pragma unroll
           for (int m = 0; m < 16; m++) keep[m] = dot2(z[m], v[m]);
@@ -795,6 +804,9 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_row_adv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS
 // the reference are summed before the transform: F[a] + F[b] = F[a + b])
 // binary schedule: 0 mu_t (plain, x-rows i0, i1); 1 + h: (dx c, dy c) of x-row i0 + h
 // ternary schedule: per x-row 3h: (mu1, mu2); 3h + 1: grad c1; 3h + 2: grad c2
+// Every step is an inverse transform of its G rows, or with GR only the mu steps
+// are, grad c_i being P2's real-space copy (the same transform of the same G
+// rows, so the same values bit for bit).
 // ---------------------------------------------------------------------------
 template <int N, class R, int MODEL>
 __device__ __forceinline__ RowSrc<R> force_src(const Bufs<R>& B, int it, int i0) {
@@ -807,11 +819,11 @@ __device__ __forceinline__ RowSrc<R> force_src(const Bufs<R>& B, int it, int i0)
   return RowSrc<R>{B.g[slot], 2 * N, 2 * (i0 + h), 2 * slot};
 }
 
-template <int N, class R, int GPC, int MODEL, bool JT4 = false>
+template <int N, class R, int GPC, int MODEL, bool JT4 = false, bool GR = false>
 CHNS_STAGE_KERNEL(N, R, GPC) k_row_force(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS_TMAG_PARAM T) {
   constexpr int NT = N / 16;
-  constexpr int NIN = MODEL == MODEL_BINARY ? 3 : 6;      // inverse transforms
-  constexpr int STEPS = MODEL == MODEL_BINARY ? 4 : 6;    // binary: a last step only stores
+  constexpr int NIN = MODEL == MODEL_BINARY ? 3 : 6;      // steps with an input (binary: a last step only stores)
+  constexpr int STEPS = MODEL == MODEL_BINARY ? 4 : 6;
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
@@ -832,10 +844,21 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_row_force(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CH
   tile_start<N>(TL, T, S.tile, force_src<N, R, MODEL>(B, 0, i0), jt, live, t);
 #pragma unroll 1
   for (int it = 0; it < STEPS; it++) {
-    if (it < NIN) {
+    const bool mu_step = MODEL == MODEL_BINARY ? it == 0 : it % 3 == 0;
+    if (!GR && it < NIN) {
       const bool more = it + 1 < NIN;
       row_c2r_loaded<N, R, JT4>(v, S.tile, TL, T, more, force_src<N, R, MODEL>(B, more ? it + 1 : it, i0), jt, live,
                                 t, S.sh, TW);
+    } else if (GR && mu_step) {
+      // mu of the pair (binary) or of x-row i0 + it/3 (ternary: the copy of x-row i1's is in flight after it 0)
+      const bool more = MODEL == MODEL_TERNARY && it == 0;
+      row_c2r_loaded<N, R, JT4>(v, S.tile, TL, T, more, force_src<N, R, MODEL>(B, more ? 3 : it, i0), jt, live, t,
+                                S.sh, TW);
+    } else if (GR && it < NIN) {
+      // grad c (binary, x-row i0 + it - 1) or grad c_(it%3) (ternary, x-row i0 + it/3)
+      const int xr = MODEL == MODEL_BINARY ? i0 + it - 1 : i0 + it / 3;
+      const int f = MODEL == MODEL_BINARY ? 0 : it % 3 - 1;
+      load_row<N>(v, B.gr + (size_t)f * N * N, xr, live, t);
     }
     bool store = false;
     cx<R>* dst = B.h[HFF];

@@ -54,6 +54,23 @@ static auto spec_fwd_c_kernel(bool s64, bool filt) {
              : (filt ? k_spec_fwd_c<N, R, GPC, MODEL, STAGE, false, true> : k_spec_fwd_c<N, R, GPC, MODEL, STAGE, false>);
 }
 
+// the row kernels of a context: the square-box cut's compile-time tile reads
+// (JT4) and grad c_i kept in real space from P2 for P4 (GR; pure Navier-Stokes has none)
+template <int N, class R, int GPC, int MODEL>
+static auto row_adv_kernel(bool jt4, bool gr) {
+  if constexpr (MODEL == MODEL_NS) {
+    return jt4 ? k_row_adv<N, R, GPC, MODEL, true> : k_row_adv<N, R, GPC, MODEL, false>;
+  } else {
+    return jt4 ? (gr ? k_row_adv<N, R, GPC, MODEL, true, true> : k_row_adv<N, R, GPC, MODEL, true, false>)
+               : (gr ? k_row_adv<N, R, GPC, MODEL, false, true> : k_row_adv<N, R, GPC, MODEL, false, false>);
+  }
+}
+template <int N, class R, int GPC, int MODEL>
+static auto row_force_kernel(bool jt4, bool gr) {
+  return jt4 ? (gr ? k_row_force<N, R, GPC, MODEL, true, true> : k_row_force<N, R, GPC, MODEL, true, false>)
+             : (gr ? k_row_force<N, R, GPC, MODEL, false, true> : k_row_force<N, R, GPC, MODEL, false, false>);
+}
+
 template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   using S = Sizes<N, R>;
   constexpr int GPC = S::GPC;
@@ -94,17 +111,17 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   // square box (jt = N/4) has row kernels whose tile reads are fixed at compile time.
   const bool jt4 = jt == N / 4;
   if (model == CHNS_MODEL_NS) {
-    auto k = jt4 ? k_row_adv<N, R, GPC, MODEL_NS, true> : k_row_adv<N, R, GPC, MODEL_NS>;
+    auto k = row_adv_kernel<N, R, GPC, MODEL_NS>(jt4, c->p4_grad);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_NS>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   } else if (model == CHNS_MODEL_BINARY) {
-    auto k = jt4 ? k_row_adv<N, R, GPC, MODEL_BINARY, true> : k_row_adv<N, R, GPC, MODEL_BINARY>;
+    auto k = row_adv_kernel<N, R, GPC, MODEL_BINARY>(jt4, c->p4_grad);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_BINARY>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   } else {
-    auto k = jt4 ? k_row_adv<N, R, GPC, MODEL_TERNARY, true> : k_row_adv<N, R, GPC, MODEL_TERNARY>;
+    auto k = row_adv_kernel<N, R, GPC, MODEL_TERNARY>(jt4, c->p4_grad);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_TERNARY>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
@@ -143,12 +160,12 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
 
   // P4: surface-tension force
   if (model == CHNS_MODEL_BINARY) {
-    auto k = jt4 ? k_row_force<N, R, GPC, MODEL_BINARY, true> : k_row_force<N, R, GPC, MODEL_BINARY>;
+    auto k = row_force_kernel<N, R, GPC, MODEL_BINARY>(jt4, c->p4_grad);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_force_frags<MODEL_BINARY>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
   } else {
-    auto k = jt4 ? k_row_force<N, R, GPC, MODEL_TERNARY, true> : k_row_force<N, R, GPC, MODEL_TERNARY>;
+    auto k = row_force_kernel<N, R, GPC, MODEL_TERNARY>(jt4, c->p4_grad);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_force_frags<MODEL_TERNARY>());
     set_smem(k, sm);
     k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);

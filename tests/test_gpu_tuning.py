@@ -1,5 +1,6 @@
 """The autotuner's run-time launch-shape choices (chns_tune_override: rows per
-TMA box of the row kernels' tiles, the P1 split) change no result bit: every
+TMA box of the row kernels' tiles, the P1 split, P4's grad c from P2's real-space
+copy or from its own transform) change no result bit: every
 choice gives the state of the tuned default bit for bit, on grids whose tiles
 take one or several boxes, in both precisions and with the smooth filter."""
 import math
@@ -42,7 +43,8 @@ def test_launch_shapes_change_no_bit(chns, model, n, prec, filt):
     p1, p2, w = MG.initial_state(model, n, lx, 500 + n, 501 + n, 8.0, 0.1)
     ref = _run(chns, p, 3, (p1, p2), w)
     try:
-        for knob, values in ((chns.TUNE_TMA_BOX_ROWS, (64, 128, 256, 8)), (chns.TUNE_P1_SPLIT, (0, 1))):
+        for knob, values in ((chns.TUNE_TMA_BOX_ROWS, (64, 128, 256, 8)), (chns.TUNE_P1_SPLIT, (0, 1)),
+                             (chns.TUNE_P4_GRAD, (0, 1))):
             for v in values:
                 chns.tune_override(knob, v)
                 got = _run(chns, p, 3, (p1, p2), w)
@@ -52,3 +54,4 @@ def test_launch_shapes_change_no_bit(chns, model, n, prec, filt):
     finally:
         chns.tune_override(chns.TUNE_TMA_BOX_ROWS, -1)
         chns.tune_override(chns.TUNE_P1_SPLIT, -1)
+        chns.tune_override(chns.TUNE_P4_GRAD, -1)
