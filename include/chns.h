@@ -313,10 +313,12 @@ int chns_debug_tile_waits(chns_ctx *ctx, int spins, int skip_copies);
  * CHNS_TUNE_P1_SPLIT: 1 runs the spectral inverse pass with two CTAs per row, 0
  * with one; CHNS_TUNE_P4_GRAD: 1 keeps grad c_i in real space from the advection
  * pass for the force pass (one more device field per phase field), 0 has the force
- * pass transform it again.  value -1 restores the table.  Results are bitwise the
- * same under every choice; only the speed changes.  Not thread-safe: set before
- * creating contexts. */
-enum { CHNS_TUNE_TMA_BOX_ROWS = 1, CHNS_TUNE_P1_SPLIT = 2, CHNS_TUNE_P4_GRAD = 3 };
+ * pass transform it again; CHNS_TUNE_PDL: 1 launches the stage kernels as
+ * programmatic dependent launches (each scheduled while the one before drains,
+ * waiting on the device for its completion), 0 plainly.  value -1 restores the
+ * table.  Results are bitwise the same under every choice; only the speed changes.
+ * Not thread-safe: set before creating contexts. */
+enum { CHNS_TUNE_TMA_BOX_ROWS = 1, CHNS_TUNE_P1_SPLIT = 2, CHNS_TUNE_P4_GRAD = 3, CHNS_TUNE_PDL = 4 };
 int chns_tune_override(int knob, int value);
 
 /* Tracing: runs `reps` steps launching the kernels one by one (not from the

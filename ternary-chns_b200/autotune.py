@@ -18,8 +18,10 @@ ternary steps (the candidate with the highest summed steps/s wins):
 * P4's grad c (``grad`` pass): kept in real space by P2 (one more field written
   and read per phase field) or transformed again by P4 (two more transforms per
   x-row pair and phase field).
+* programmatic dependent launches of the stage kernels (``pdl`` pass): each kernel
+  scheduled while the one before drains, waiting on the device for it.
 
-The box, split and grad choices are run-time (chns_tune_override, for contexts
+The box, split, grad and pdl choices are run-time (chns_tune_override, for contexts
 created afterwards), so those passes time one library.  Such a candidate replaces
 the current table entry only when it is more than ``--margin`` (1%) faster, so
 that run-to-run noise does not flip choices.  Results are bitwise the same under
@@ -32,7 +34,7 @@ changes the twiddle multiplies by at most one per thread and stage.
 
 Passes not run keep the values of the current header.  It needs a GPU:
 
-    python ternary-chns_b200/autotune.py --passes threads,box,split,grad \\
+    python ternary-chns_b200/autotune.py --passes threads,box,split,grad,pdl \\
         --out ternary-chns_b200/csrc/chns_tuned.h --report autotune.json
 """
 from __future__ import annotations
@@ -52,12 +54,13 @@ THREADS = [32, 64, 128, 256]
 BOX_ROWS = [64, 128, 256]
 SPLIT = [0, 1]
 GRAD = [0, 1]
+PDL = [0, 1]
 TIMED_SIZES = [256, 512, 1024, 2048, 4096]
 ALL_SIZES = [32, 64, 128, 256, 512, 1024, 2048, 4096]
-TABLES = ["kCtaThreads", "kTmaBoxRows", "kSpecInvSplit", "kP4Grad"]
+TABLES = ["kCtaThreads", "kTmaBoxRows", "kSpecInvSplit", "kP4Grad", "kPdl"]
 
 
-def time_variant(lib: str, box: int = -1, split: int = -1, grad: int = -1, steps_small: int = 200,
+def time_variant(lib: str, box: int = -1, split: int = -1, grad: int = -1, pdl: int = -1, steps_small: int = 200,
                  steps_large: int = 40) -> dict:
     """Steps/s of each (model, n, precision) with the library at `lib` and the
     given run-time overrides (-1: the tuned table)."""
@@ -70,6 +73,7 @@ def time_variant(lib: str, box: int = -1, split: int = -1, grad: int = -1, steps
     C.tune_override(C.TUNE_TMA_BOX_ROWS, box)
     C.tune_override(C.TUNE_P1_SPLIT, split)
     C.tune_override(C.TUNE_P4_GRAD, grad)
+    C.tune_override(C.TUNE_PDL, pdl)
     out = {}
     rng = np.random.default_rng(0)
     for model in (C.MODEL_BINARY, C.MODEL_TERNARY):
@@ -96,6 +100,7 @@ def time_variant(lib: str, box: int = -1, split: int = -1, grad: int = -1, steps
     C.tune_override(C.TUNE_TMA_BOX_ROWS, -1)
     C.tune_override(C.TUNE_P1_SPLIT, -1)
     C.tune_override(C.TUNE_P4_GRAD, -1)
+    C.tune_override(C.TUNE_PDL, -1)
     return out
 
 
@@ -116,11 +121,12 @@ def header(t: dict) -> str:
 
     return f"""// chns_tuned.h -- launch shapes of the step and transform kernels for each grid
 // size and precision (index log2(n) - 5, n = 32 .. 4096): threads per CTA, TMA box
-// rows, the P1 split and the source of P4's grad c.  Chosen by
-// ternary-chns_b200/autotune.py from forward-step timings of the binary and
-// ternary models on a B200: the candidate with the highest summed steps/s.  Each
-// CTA runs threads / (n/16) transforms of n points side by side; small grids want
-// few threads per CTA so that the rows spread over all 148 SMs.
+// rows, the P1 split, the source of P4's grad c and programmatic dependent
+// launches of the stage kernels.  Chosen by ternary-chns_b200/autotune.py from
+// forward-step timings of the binary and ternary models on a B200: the candidate
+// with the highest summed steps/s.  Each CTA runs threads / (n/16) transforms of
+// n points side by side; small grids want few threads per CTA so that the rows
+// spread over all 148 SMs.
 #pragma once
 
 namespace chns {{
@@ -141,13 +147,18 @@ constexpr int kSpecInvSplitF32[8] = {{{row("kSpecInvSplit", 1)}}};
 constexpr int kP4GradF64[8] = {{{row("kP4Grad", 0)}}};
 constexpr int kP4GradF32[8] = {{{row("kP4Grad", 1)}}};
 
+// stage kernels launched as programmatic dependent launches (1), or plainly (0).
+constexpr int kPdlF64[8] = {{{row("kPdl", 0)}}};
+constexpr int kPdlF32[8] = {{{row("kPdl", 1)}}};
+
 }}  // namespace chns
 """
 
 
-def _time_in_process(lib: str, box: int = -1, split: int = -1, grad: int = -1) -> dict:
+def _time_in_process(lib: str, box: int = -1, split: int = -1, grad: int = -1, pdl: int = -1) -> dict:
     r = subprocess.run([sys.executable, os.path.abspath(__file__), "--time", lib, "--box", str(box),
-                        "--split", str(split), "--grad", str(grad)], capture_output=True, text=True, check=True)
+                        "--split", str(split), "--grad", str(grad), "--pdl", str(pdl)], capture_output=True,
+                       text=True, check=True)
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
@@ -172,18 +183,20 @@ def _pick(results: dict, table: list, prec: int, margin: float, allowed=lambda c
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--passes", default="threads,box,split,grad", help="comma list of threads, box, split, grad")
+    ap.add_argument("--passes", default="threads,box,split,grad,pdl",
+                    help="comma list of threads, box, split, grad, pdl")
     ap.add_argument("--out", required=False, help="header to write")
     ap.add_argument("--report", help="also write the measured tables (JSON) here")
-    ap.add_argument("--margin", type=float, default=0.01, help="gain a box / split / grad change needs")
+    ap.add_argument("--margin", type=float, default=0.01, help="gain a run-time choice's change needs")
     ap.add_argument("--lib", help="library the box and split passes time (default: the in-tree build)")
     ap.add_argument("--time", help="(internal) time one library variant and print JSON")
     ap.add_argument("--box", type=int, default=-1, help="(internal) box-rows override of --time")
     ap.add_argument("--split", type=int, default=-1, help="(internal) P1-split override of --time")
     ap.add_argument("--grad", type=int, default=-1, help="(internal) P4-grad override of --time")
+    ap.add_argument("--pdl", type=int, default=-1, help="(internal) PDL override of --time")
     a = ap.parse_args()
     if a.time:
-        print(json.dumps(time_variant(a.time, a.box, a.split, a.grad)))
+        print(json.dumps(time_variant(a.time, a.box, a.split, a.grad, a.pdl)))
         return
     sys.path.insert(0, HERE)
     import build as B
@@ -225,6 +238,12 @@ def main():
             tables[("kP4Grad", prec)] = _pick(results, tables[("kP4Grad", prec)], prec, a.margin)
         report["grad"] = {str(k): v for k, v in results.items()}
         print("grad:", json.dumps(report["grad"]), flush=True)
+    if "pdl" in passes:
+        results = {q: _time_in_process(lib, pdl=q) for q in PDL}
+        for prec in (0, 1):
+            tables[("kPdl", prec)] = _pick(results, tables[("kPdl", prec)], prec, a.margin)
+        report["pdl"] = {str(k): v for k, v in results.items()}
+        print("pdl:", json.dumps(report["pdl"]), flush=True)
     text = header(tables)
     if a.out:
         with open(a.out, "w") as f:

@@ -136,8 +136,8 @@ def load_library(path: str = LIB_PATH):
 
 
 # chns_tune_override knobs: rows per TMA box of the row kernels' tiles; P1 with two CTAs per
-# row; grad c kept in real space from P2 for P4
-TUNE_TMA_BOX_ROWS, TUNE_P1_SPLIT, TUNE_P4_GRAD = 1, 2, 3
+# row; grad c kept in real space from P2 for P4; stage kernels as programmatic dependent launches
+TUNE_TMA_BOX_ROWS, TUNE_P1_SPLIT, TUNE_P4_GRAD, TUNE_PDL = 1, 2, 3, 4
 
 
 def tune_override(knob: int, value: int) -> None:

@@ -237,7 +237,7 @@ void free_all(chns_ctx* c) {
 // or refuses a map).  Each G slot holds rows 0..jt; a tile is nbox boxes of
 // {2 complex, boxr rows}.
 // chns_tune_override's process-wide choices (-1: the tuned table)
-static int g_tune_box_rows = -1, g_tune_p1_split = -1, g_tune_p4_grad = -1;
+static int g_tune_box_rows = -1, g_tune_p1_split = -1, g_tune_p4_grad = -1, g_tune_pdl = -1;
 
 static int tuned_index(int n) { return ilog2_exact(n) - 5; }
 
@@ -406,6 +406,7 @@ int chns_create(const chns_params* pin, chns_ctx** out) {
     c->p4_grad = p.model != CHNS_MODEL_NS &&
                  (g_tune_p4_grad >= 0 ? g_tune_p4_grad != 0
                                       : (c->f32 ? chns::kP4GradF32[li] : chns::kP4GradF64[li]) != 0);
+    c->pdl = g_tune_pdl >= 0 ? g_tune_pdl != 0 : (c->f32 ? chns::kPdlF32[li] : chns::kPdlF64[li]) != 0;
   }
   const int logn = ilog2_exact(c->n);
   c->L = c->f32 ? chns::launchers_f32(logn) : chns::launchers_f64(logn);
@@ -986,9 +987,9 @@ int chns_tune_override(int knob, int value) {
     g_tune_box_rows = value;
     return CHNS_OK;
   }
-  if (knob == CHNS_TUNE_P1_SPLIT || knob == CHNS_TUNE_P4_GRAD) {
+  if (knob == CHNS_TUNE_P1_SPLIT || knob == CHNS_TUNE_P4_GRAD || knob == CHNS_TUNE_PDL) {
     if (value != -1 && value != 0 && value != 1) return CHNS_ERR_ARG;
-    (knob == CHNS_TUNE_P1_SPLIT ? g_tune_p1_split : g_tune_p4_grad) = value;
+    (knob == CHNS_TUNE_P1_SPLIT ? g_tune_p1_split : knob == CHNS_TUNE_P4_GRAD ? g_tune_p4_grad : g_tune_pdl) = value;
     return CHNS_OK;
   }
   return CHNS_ERR_ARG;

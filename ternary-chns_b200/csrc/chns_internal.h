@@ -64,6 +64,7 @@ struct chns_ctx {
   int n, nr, jt;
   bool p1_split;  // P1 with two CTAs per row (chns_tuned.h or chns_tune_override)
   bool p4_grad;   // grad c_i from P2 in real space for P4 (chns_tuned.h or chns_tune_override)
+  bool pdl;       // stage kernels as programmatic dependent launches (chns_tuned.h or chns_tune_override)
   bool f32;
   bool st64;   // FP32 context with a double-float state (CHNS_FP32_STATE64)
   size_t rsz;  // bytes per real scalar (4 or 8)

@@ -93,6 +93,19 @@ template <class R> struct Bufs {
 // virtual CTA: there CHNS_BX / CHNS_BY read that CTA's index from chns_vblock
 // (a shared int[2] that translation unit declares before the include and sets,
 // followed by a barrier, before each call) instead of blockIdx.
+// CHNS_GRID_DEP: a stage kernel launched with programmatic stream serialization
+// (the context's PDL choice) may be scheduled while the kernel before it ends;
+// every access to the step's buffers follows this wait for that kernel's
+// completion (a no-op for an ordinary launch).  The next kernel is released
+// when this one's CTAs exit (an earlier release, right after the wait, made the
+// waiting CTAs of the next kernel crowd the SMs: up to 34% slower at 512^2).
+// Only the twiddle table, never written by a kernel, is read before it.
+#ifdef CHNS_STAGE_BODIES
+#define CHNS_GRID_DEP() ((void)0)
+#else
+#define CHNS_GRID_DEP() asm volatile("griddepcontrol.wait;\n" ::: "memory")
+#endif
+
 #ifdef CHNS_STAGE_BODIES
 #define CHNS_STAGE_KERNEL(N, R, GPC) __device__ __forceinline__ void
 #define CHNS_TMAG_PARAM const TmaG&
@@ -525,6 +538,7 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_spec_inv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  CHNS_GRID_DEP();
   unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = CHNS_BX * GPC + g;
@@ -693,6 +707,7 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_row_adv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  CHNS_GRID_DEP();
   unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   const bool tma = tma_tiles_ok<N, R, GPC>(T, smem_raw);  // CTA-uniform
   if (tma) smem_raw = align128(smem_raw);
@@ -827,6 +842,7 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_row_force(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CH
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  CHNS_GRID_DEP();
   unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   const bool tma = tma_tiles_ok<N, R, GPC>(T, smem_raw);  // CTA-uniform
   if (tma) smem_raw = align128(smem_raw);
@@ -1023,6 +1039,7 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_spec_fwd_c(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  CHNS_GRID_DEP();
   unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = CHNS_BX * GPC + g;
@@ -1170,6 +1187,7 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_spec_curl_w(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) 
   extern __shared__ __align__(16) unsigned char smem_all[];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   const Tw<R> TW = tw_setup<N>(reinterpret_cast<cx<R>*>(smem_all), P.tw, t);
+  CHNS_GRID_DEP();
   unsigned char* smem_raw = smem_all + tw_smem_bytes<N, R>(blockDim.x);
   cx<R>* sh = reinterpret_cast<cx<R>*>(smem_raw) + g * FftShape<N>::SMEM;
   const int row = CHNS_BX * GPC + g;

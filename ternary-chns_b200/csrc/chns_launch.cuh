@@ -46,6 +46,29 @@ template <int N, class R> constexpr size_t spec_smem(bool prefetch) {
   return Sizes<N, R>::FFT_SMEM + (prefetch && sizeof(R) == 4 ? prefetch_smem<N, R, Sizes<N, R>::GPC>() : 0);
 }
 
+// launch of a stage kernel; with the context's PDL choice as a programmatic
+// dependent launch (the kernel's CHNS_GRID_DEP waits for its predecessor), so
+// that it is scheduled while the kernel before it drains
+template <class K, class... Args>
+static void launch_stage(const chns_ctx* c, K kern, dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                         const Args&... args) {
+  if (!c->pdl) {
+    kern<<<grid, block, smem, st>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // the P3 variant of a context: double-float state (FP32 only) and SMOOTH_FILTER
 template <int N, class R, int GPC, int MODEL, int STAGE>
 static auto spec_fwd_c_kernel(bool s64, bool filt) {
@@ -94,15 +117,15 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   if (model == CHNS_MODEL_NS) {
     auto k = c->p1_split ? k_spec_inv<N, R, GPC, MODEL_NS, true> : k_spec_inv<N, R, GPC, MODEL_NS, false>;
     set_smem(k, S::FFT_SMEM);
-    k<<<dim3(rows_inv, c->p1_split ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    launch_stage(c, k, dim3(rows_inv, c->p1_split ? 2 : 1), S::THREADS, S::FFT_SMEM, st, B, P);
   } else if (model == CHNS_MODEL_BINARY) {
     auto k = c->p1_split ? k_spec_inv<N, R, GPC, MODEL_BINARY, true> : k_spec_inv<N, R, GPC, MODEL_BINARY, false>;
     set_smem(k, S::FFT_SMEM);
-    k<<<dim3(rows_inv, c->p1_split ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    launch_stage(c, k, dim3(rows_inv, c->p1_split ? 2 : 1), S::THREADS, S::FFT_SMEM, st, B, P);
   } else {
     auto k = c->p1_split ? k_spec_inv<N, R, GPC, MODEL_TERNARY, true> : k_spec_inv<N, R, GPC, MODEL_TERNARY, false>;
     set_smem(k, S::FFT_SMEM);
-    k<<<dim3(rows_inv, c->p1_split ? 2 : 1), S::THREADS, S::FFT_SMEM, st>>>(B, P);
+    launch_stage(c, k, dim3(rows_inv, c->p1_split ? 2 : 1), S::THREADS, S::FFT_SMEM, st, B, P);
   }
   launches++;
   mark(c, KIND_SPEC_INV);
@@ -114,17 +137,17 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
     auto k = row_adv_kernel<N, R, GPC, MODEL_NS>(jt4, c->p4_grad);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_NS>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
+    launch_stage(c, k, pairs, S::THREADS, sm, st, B, P, TG);
   } else if (model == CHNS_MODEL_BINARY) {
     auto k = row_adv_kernel<N, R, GPC, MODEL_BINARY>(jt4, c->p4_grad);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_BINARY>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
+    launch_stage(c, k, pairs, S::THREADS, sm, st, B, P, TG);
   } else {
     auto k = row_adv_kernel<N, R, GPC, MODEL_TERNARY>(jt4, c->p4_grad);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_TERNARY>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
+    launch_stage(c, k, pairs, S::THREADS, sm, st, B, P, TG);
   }
   launches++;
   mark(c, KIND_ROW_ADV);
@@ -134,11 +157,11 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
     if (stage == 1) {
       auto k = s64 ? k_spec_curl_w<N, R, GPC, false, 1, F32> : k_spec_curl_w<N, R, GPC, false, 1, false>;
       set_smem(k, S::FFT_SMEM);
-      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+      launch_stage(c, k, rows_all, S::THREADS, S::FFT_SMEM, st, B, P);
     } else {
       auto k = s64 ? k_spec_curl_w<N, R, GPC, false, 2, F32> : k_spec_curl_w<N, R, GPC, false, 2, false>;
       set_smem(k, S::FFT_SMEM);
-      k<<<rows_all, S::THREADS, S::FFT_SMEM, st>>>(B, P);
+      launch_stage(c, k, rows_all, S::THREADS, S::FFT_SMEM, st, B, P);
     }
     mark(c, KIND_SPEC_CURL_W);
     return launches + 1;
@@ -153,7 +176,7 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
                  : (stage == 1 ? spec_fwd_c_kernel<N, R, GPC, MODEL_TERNARY, 1>(s64, filt)
                                : spec_fwd_c_kernel<N, R, GPC, MODEL_TERNARY, 2>(s64, filt));
     set_smem(k, spec_smem<N, R>(bin));
-    k<<<rows_all, S::THREADS, spec_smem<N, R>(bin), st>>>(B, P);
+    launch_stage(c, k, rows_all, S::THREADS, spec_smem<N, R>(bin), st, B, P);
   }
   launches++;
   mark(c, KIND_SPEC_FWD_C);
@@ -163,12 +186,12 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
     auto k = row_force_kernel<N, R, GPC, MODEL_BINARY>(jt4, c->p4_grad);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_force_frags<MODEL_BINARY>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
+    launch_stage(c, k, pairs, S::THREADS, sm, st, B, P, TG);
   } else {
     auto k = row_force_kernel<N, R, GPC, MODEL_TERNARY>(jt4, c->p4_grad);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_force_frags<MODEL_TERNARY>());
     set_smem(k, sm);
-    k<<<pairs, S::THREADS, sm, st>>>(B, P, TG);
+    launch_stage(c, k, pairs, S::THREADS, sm, st, B, P, TG);
   }
   launches++;
   mark(c, KIND_ROW_FORCE);
@@ -182,7 +205,7 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
                  : (s64 ? (bin ? k_spec_curl_w<N, R, GPC, true, 2, F32, true> : k_spec_curl_w<N, R, GPC, true, 2, F32>)
                         : (bin ? k_spec_curl_w<N, R, GPC, true, 2, false, true> : k_spec_curl_w<N, R, GPC, true, 2, false>));
     set_smem(k, spec_smem<N, R>(bin));
-    k<<<rows_all, S::THREADS, spec_smem<N, R>(bin), st>>>(B, P);
+    launch_stage(c, k, rows_all, S::THREADS, spec_smem<N, R>(bin), st, B, P);
   }
   launches++;
   mark(c, KIND_SPEC_CURL_W);

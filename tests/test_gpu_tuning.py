@@ -1,6 +1,7 @@
 """The autotuner's run-time launch-shape choices (chns_tune_override: rows per
 TMA box of the row kernels' tiles, the P1 split, P4's grad c from P2's real-space
-copy or from its own transform) change no result bit: every
+copy or from its own transform, programmatic dependent launches) change no result
+bit: every
 choice gives the state of the tuned default bit for bit, on grids whose tiles
 take one or several boxes, in both precisions and with the smooth filter."""
 import math
@@ -44,7 +45,7 @@ def test_launch_shapes_change_no_bit(chns, model, n, prec, filt):
     ref = _run(chns, p, 3, (p1, p2), w)
     try:
         for knob, values in ((chns.TUNE_TMA_BOX_ROWS, (64, 128, 256, 8)), (chns.TUNE_P1_SPLIT, (0, 1)),
-                             (chns.TUNE_P4_GRAD, (0, 1))):
+                             (chns.TUNE_P4_GRAD, (0, 1)), (chns.TUNE_PDL, (0, 1))):
             for v in values:
                 chns.tune_override(knob, v)
                 got = _run(chns, p, 3, (p1, p2), w)
@@ -55,3 +56,4 @@ def test_launch_shapes_change_no_bit(chns, model, n, prec, filt):
         chns.tune_override(chns.TUNE_TMA_BOX_ROWS, -1)
         chns.tune_override(chns.TUNE_P1_SPLIT, -1)
         chns.tune_override(chns.TUNE_P4_GRAD, -1)
+        chns.tune_override(chns.TUNE_PDL, -1)

@@ -93,11 +93,11 @@ def test_truncation_factors_equal_the_restatement(chns, name):
 def test_tune_override_checks_its_arguments(chns):
     C, L = chns
     for knob, bad in ((C.TUNE_TMA_BOX_ROWS, (0, 4, 12, 264, -2)), (C.TUNE_P1_SPLIT, (2, -2)),
-                      (C.TUNE_P4_GRAD, (2, -2)), (7, (1,))):
+                      (C.TUNE_P4_GRAD, (2, -2)), (C.TUNE_PDL, (2, -2)), (7, (1,))):
         for v in bad:
             assert L.chns_tune_override(knob, v) == -1, (knob, v)
     for knob, good in ((C.TUNE_TMA_BOX_ROWS, (8, 64, 256, -1)), (C.TUNE_P1_SPLIT, (0, 1, -1)),
-                       (C.TUNE_P4_GRAD, (0, 1, -1))):
+                       (C.TUNE_P4_GRAD, (0, 1, -1)), (C.TUNE_PDL, (0, 1, -1))):
         for v in good:
             assert L.chns_tune_override(knob, v) == 0, (knob, v)
 
