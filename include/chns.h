@@ -243,13 +243,16 @@ int chns_read_phase(chns_ctx *ctx, const char *path1, const char *path2);
  * free_energy.c:3-157 (loss_w = NULL: all weights 1):
  *   binary  J = w[0] E_bulk + w[1] E_grad + w[2] <|grad phi|^2>,  phi = 2c - 1
  *   ternary J = w[0] E_bulk + w[1] E_grad + w[2] <|grad c1|^2 + |grad c2|^2>
+ *   pure Navier-Stokes J = w[0] <|u|^2 / 2> + w[1] <w_t^2 / 2>, of the truncated
+ *           velocity (kinetic_energy.c:17-21,43-49,89) and vorticity (w[2] unused)
  * Outputs: *J; dJ/d(omega_hat_0) in g_w and dJ/d(c_hat_0) (binary) or dJ/d(c1_hat_0)
  * followed by dJ/d(c2_hat_0) (ternary) in g_c, FFTW layout (gradients with respect
- * to the stored real and imaginary parts; g_w / g_c may be NULL); g_params =
- * dJ/d(nu, lambda, sigma) (binary, 3 values) or dJ/d(nu, lambda, sigma_12,
- * sigma_13, sigma_23) (ternary, 5 values).  The state is kept every `ckpt` steps
- * and recomputed in between; it is unchanged on return.  Pure Navier-Stokes
- * contexts and CHNS_FP32_STATE64 contexts return CHNS_ERR_UNSUPPORTED. */
+ * to the stored real and imaginary parts; g_w / g_c may be NULL; g_c is not written
+ * for pure Navier-Stokes); g_params = dJ/d(nu, lambda, sigma) (binary, 3 values;
+ * pure Navier-Stokes: nu, 0, 0) or dJ/d(nu, lambda, sigma_12, sigma_13, sigma_23)
+ * (ternary, 5 values).  The state is kept every `ckpt` steps and recomputed in
+ * between; it is unchanged on return.  CHNS_FP32_STATE64 contexts return
+ * CHNS_ERR_UNSUPPORTED. */
 int chns_adjoint(chns_ctx *ctx, int nsteps, int ckpt, const double *loss_w, double *J, double *g_w,
                  double *g_c, double *g_params, int where);
 

@@ -353,11 +353,13 @@ class Context:
         return fe, ke, rc
 
     def adjoint(self, nsteps: int, ckpt: int = 20, loss_w=(1.0, 1.0, 1.0)):
-        """Discrete adjoint of `nsteps` ETD2RK steps from the current state (binary or
-        ternary).  Returns (J, dJ/d omega_hat_0, dJ/d c_hat_0, dJ/d params): for the
-        binary model dJ/d c_hat_0 is one array and the parameters are (nu, lambda,
-        sigma); for the ternary model it is a pair (c1, c2) and the parameters are
-        (nu, lambda, sigma_12, sigma_13, sigma_23).  The state is unchanged."""
+        """Discrete adjoint of `nsteps` ETD2RK steps from the current state.  Returns
+        (J, dJ/d omega_hat_0, dJ/d c_hat_0, dJ/d params): for the binary model
+        dJ/d c_hat_0 is one array and the parameters are (nu, lambda, sigma); for the
+        ternary model it is a pair (c1, c2) and the parameters are (nu, lambda,
+        sigma_12, sigma_13, sigma_23); for pure Navier-Stokes (loss_w[0] kinetic
+        energy, loss_w[1] enstrophy) it is None and the parameters are (nu, 0, 0).
+        The state is unchanged."""
         lw = np.ascontiguousarray(loss_w, np.float64)
         if lw.shape != (3,):
             raise ValueError("loss_w: three weights")
@@ -365,9 +367,11 @@ class Context:
         gw = np.empty(self.shape, np.complex128)
         nc = max(self.model, 1)
         gc = np.empty((nc,) + self.shape, np.complex128)
-        gp = np.zeros(3 if self.model == MODEL_BINARY else 5)
+        gp = np.zeros(5 if self.model == MODEL_TERNARY else 3)
         _check(self.L.chns_adjoint(self._h, int(nsteps), int(ckpt), _ptr(lw), _ptr(J), _ptr(gw), _ptr(gc),
                                    _ptr(gp), HOST), "chns_adjoint")
+        if self.model == MODEL_NS:
+            return float(J[0]), gw, None, gp
         return float(J[0]), gw, (gc[0] if self.model == MODEL_BINARY else (gc[0], gc[1])), gp
 
     def launches_per_step(self) -> int:

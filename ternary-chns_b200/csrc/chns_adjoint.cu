@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "chns_adjoint.cuh"
+#include "chns_adjoint_ns.cuh"
 #include "chns_adjoint_t.cuh"
 #include "chns_internal.h"
 
@@ -261,6 +262,135 @@ template <class R> struct Adj {
       fields(st, 1, S(CUW), S(CUC));
     }
     transpose_rhs(1, S(CUC), S(SNBAW), S(SNBAC), gw, gc);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// pure Navier-Stokes: state w.  Two field sets as in the binary model (0: u*,
+// 1: u_n), each with the batch of the four forward spectra (u, v, wx, wy) and
+// their physical fields.
+// ---------------------------------------------------------------------------
+namespace nsadj {
+constexpr int SSET = 4;                        // spectral fields per set (the batch of 4)
+enum {
+  SA = 2 * SSET,                               // A_bar spectrum
+  SNB,                                         // N*_bar
+  SNA,                                         // N(u_n)_bar
+  SG,                                          // running gradient
+  CUR,                                         // current step: u_n, u*, N(u_n), N(u*)
+  NSPEC = CUR + 4
+};
+constexpr int PSET = 4;                        // u, v, wx, wy per set
+enum { PA = 2 * PSET, PXB, NPHYS = PXB + 4 };  // A_bar, then the batch of 4 adjoints
+}  // namespace nsadj
+
+template <class R> struct AdjNS {
+  static constexpr int NF = 1, NSPEC_ = nsadj::NSPEC, NPHYS_ = nsadj::NPHYS, NBSCR = 4, NDCOEF = 3;
+  chns_ctx* c;
+  chns_adj* a;
+  AdjPar<R> P;
+  cudaStream_t st;
+  size_t ncx, nn;
+  int blocks_s, blocks_p;
+
+  cx<R>* S(int k) const { return (cx<R>*)a->spec + (size_t)k * ncx; }
+  R* F(int k) const { return (R*)a->phys + (size_t)k * nn; }
+  cx<R>* SS(int set, int k) const { return S(set * nsadj::SSET + k); }
+  R* FS(int set, int k) const { return F(set * nsadj::PSET + k); }
+  void* scratch(int set) const { return (char*)a->bscr + (size_t)set * NBSCR * ncx * sizeof(cx<R>); }
+  int cur0() const { return nsadj::CUR; }
+  cx<R>* grad(int) const { return S(nsadj::SG); }
+
+  void setup() {
+    P.n = c->n;
+    P.jt = c->jt;
+    P.fx = c->fx;
+    P.fy = c->fy;
+    P.s1 = P.s2 = P.lam = (R)0;
+    P.ds1 = P.ds2 = 0.0;
+    P.mrow = c->mrow;
+  }
+  // d/dnu of the w coefficients (e, z1, z2)
+  static void dcoef_tables(const chns_ctx* c, std::vector<double>& d) {
+    const int nr = c->nr;
+    const size_t t = (size_t)nr * nr;
+    d.assign(NDCOEF * t, 0.0);
+    for (int j = 0; j < nr; j++)
+      for (int m = 0; m < nr; m++) {
+        const double kx = c->fx * m, ky = c->fy * j, ks = kx * kx + ky * ky;
+        double o[3];
+        dcoef_dc(-c->p.nu * ks, c->p.dt, o);
+        for (int q = 0; q < 3; q++) d[q * t + (size_t)j * nr + m] = -ks * o[q];
+      }
+  }
+  void ifft(cudaStream_t s, int set, const cx<R>* in, R* x, int nb) {
+    c->stream = s;
+    c->L->ifftb(c, in, ncx, x, nn, nb, scratch(set));
+    c->stream = st;
+  }
+  void dfft(cudaStream_t s, int set, const R* x, cx<R>* out, int nb) {
+    c->stream = s;
+    c->L->dfftb(c, x, nn, out, ncx, nb, scratch(set));
+    c->stream = st;
+  }
+  // loss at the final state (w[0] kinetic energy, w[1] enstrophy, both of the
+  // truncated fields) and its gradient
+  void loss(const double* lw) {
+    using namespace nsadj;
+    k_adjns_loss_prep3<R><<<blocks_s, 256, 0, st>>>(P, (const cx<R>*)c->state[0], SS(0, 0), ncx);
+    ifft(st, 0, SS(0, 0), FS(0, 0), 3);
+    const double inv = 1.0 / ((double)c->n * (double)c->n);
+    k_adjns_loss<R><<<kLossBlocks, 256, 0, st>>>(FS(0, 0), FS(0, 1), FS(0, 2), F(PXB), F(PXB + 1), F(PXB + 2), nn,
+                                                 lw[0] * inv, lw[1] * inv, a->acc + kAcc);
+    k_sum_parts<<<1, 32, 0, st>>>(a->acc + kAcc, kLossBlocks, a->acc);
+    dfft(st, 0, F(PXB), SS(0, 0), 3);
+    k_adjns_loss_acc3<R><<<blocks_s, 256, 0, st>>>(P, SS(0, 0), S(SG), ncx);
+  }
+  // g_par = dJ/d(nu, lambda, sigma): only nu acts on a pure Navier-Stokes run
+  void params(const double* h, double* g_par) const {
+    g_par[0] = h[4];
+    g_par[1] = 0.0;
+    g_par[2] = 0.0;
+  }
+  void fields(cudaStream_t s, int set, const cx<R>* w) {
+    k_adjns_prep4<R><<<blocks_s, 256, 0, s>>>(P, w, SS(set, 0), ncx);
+    ifft(s, set, SS(set, 0), FS(set, 0), 4);
+  }
+  // gw += J_N(state)^T nbw with the forward fields of set `set`.  Scratch of set 0.
+  void transpose_rhs(int set, const cx<R>* nbw, cx<R>* gw) {
+    using namespace nsadj;
+    k_adjns_tail1<R><<<blocks_s, 256, 0, st>>>(P, nbw, S(SA));
+    ifft(st, 0, S(SA), F(PA), 1);
+    k_adjns_products<R><<<blocks_p, 256, 0, st>>>(FS(set, 0), FS(set, 1), FS(set, 2), FS(set, 3), F(PA), F(PXB),
+                                                  F(PXB + 1), F(PXB + 2), F(PXB + 3), nn);
+    dfft(st, 0, F(PXB), SS(0, 0), 4);
+    k_adjns_acc4<R><<<blocks_s, 256, 0, st>>>(P, SS(0, 0), gw, ncx);
+  }
+  // one reversed step from the current-step slots (u_n, u*, N(u_n), N(u*))
+  void reverse_step(const R* coef, const double* dcoef, cudaStream_t fork) {
+    using namespace nsadj;
+    double* pacc = a->acc + 4;
+    cx<R>* gw = S(SG);
+    const cx<R>* un = S(CUR);
+    const cx<R>* us = S(CUR + 1);
+    const cx<R>* nn_ = S(CUR + 2);
+    const cx<R>* ns_ = S(CUR + 3);
+    if (fork) {
+      cudaEventRecord(a->ev_fork, st);
+      cudaStreamWaitEvent(fork, a->ev_fork, 0);
+      fields(fork, 1, un);
+      cudaEventRecord(a->ev_join, fork);
+    }
+    k_adjns_etd2<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, ns_, nn_, S(SNB), S(SNA), pacc);
+    fields(st, 0, us);
+    transpose_rhs(0, S(SNB), gw);
+    k_adjns_etd1<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, un, nn_, S(SNA), pacc);
+    if (fork) {
+      cudaStreamWaitEvent(st, a->ev_join, 0);
+    } else {
+      fields(st, 1, un);
+    }
+    transpose_rhs(1, S(SNA), gw);
   }
 };
 
@@ -712,13 +842,15 @@ void chns_adj_free(chns_ctx* c) {
 extern "C" int chns_adjoint(chns_ctx* c, int nsteps, int ckpt, const double* loss_w, double* J, double* g_w,
                             double* g_c, double* g_par, int where) {
   if (!c || nsteps < 1 || ckpt < 1) return CHNS_ERR_ARG;
-  if (c->p.model == CHNS_MODEL_NS) return CHNS_ERR_UNSUPPORTED;
   // the checkpoints hold the float state; a double state would not be restored
   if (c->st64) return CHNS_ERR_UNSUPPORTED;
   // the transposed passes implement the sharp cut's mask only
   if (c->p.filter != CHNS_FILTER_SHARP) return CHNS_ERR_UNSUPPORTED;
   const double dflt[3] = {1.0, 1.0, 1.0};
   const double* lw = loss_w ? loss_w : dflt;
+  if (c->p.model == CHNS_MODEL_NS)
+    return c->f32 ? adjoint_impl<float, AdjNS<float>>(c, nsteps, ckpt, lw, J, g_w, g_c, g_par, where)
+                  : adjoint_impl<double, AdjNS<double>>(c, nsteps, ckpt, lw, J, g_w, g_c, g_par, where);
   if (c->p.model == CHNS_MODEL_BINARY)
     return c->f32 ? adjoint_impl<float, Adj<float>>(c, nsteps, ckpt, lw, J, g_w, g_c, g_par, where)
                   : adjoint_impl<double, Adj<double>>(c, nsteps, ckpt, lw, J, g_w, g_c, g_par, where);
