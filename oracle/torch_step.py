@@ -2,14 +2,15 @@
 infrastructure only.
 
 This module restates, with torch operations on the host, the same arithmetic as
-oracle/chns_oracle.c: the ETD2RK step of the binary and ternary models
-(etd2rk.c:14-224 with coef_mode 1: expm1 / series coefficients), the right-hand
-sides of nonlin.c:13-381, surface_tension.c:13-227 and chem_potential.c:12-94, and
-the final-time loss built from free_energy.c:3-157.  torch's reverse mode then
+oracle/chns_oracle.c: the ETD2RK step of the pure Navier-Stokes, binary and
+ternary models (etd2rk.c:14-224 with coef_mode 1: expm1 / series coefficients), the
+right-hand sides of nonlin.c:13-381, surface_tension.c:13-227 and
+chem_potential.c:12-94, and the final-time loss built from free_energy.c:3-157
+(pure Navier-Stokes: the kinetic energy of kinetic_energy.c and the enstrophy).  torch's reverse mode then
 gives the exact gradient of the discrete map, which is the checker of the
 hand-written discrete adjoint (chns_adjoint): same loss, same gradients with
 respect to the stored real and imaginary parts of the initial spectral state and
-to the parameters (nu, lambda, sigma) or (nu, lambda, sigma_12, sigma_13, sigma_23).
+to the parameters (nu), (nu, lambda, sigma) or (nu, lambda, sigma_12, sigma_13, sigma_23).
 
 It is pinned on the CPU against the C restatement (forward, to round-off) and
 against central differences of the C restatement (gradients), and it writes the
@@ -40,8 +41,8 @@ class TorchStep:
     def __init__(self, p: dict):
         if p.get("coef_mode", 0) != 1:
             raise ValueError("the differentiable step restates coef_mode 1 (expm1 / series coefficients)")
-        if p["model"] not in (1, 2):
-            raise ValueError("binary (1) or ternary (2) model")
+        if p["model"] not in (0, 1, 2):
+            raise ValueError("pure Navier-Stokes (0), binary (1) or ternary (2) model")
         self.p = dict(p)
         self.model = p["model"]
         nx, ny = p["nx"], p["ny"]
@@ -54,8 +55,15 @@ class TorchStep:
         dax = (nx / p.get("dealias_div", 4.0)) * fx  # functions.c:56-59: only the x extent
         self.keep = (self.ks <= dax * dax).to(DT)
         self.dt = float(p["dt"])
-        self.eps = float(p["epsilon"])
+        self.eps = float(p.get("epsilon", 0.0))
         self.xlambda = float(p.get("xlambda", 2.0))
+        # vorticity of the Kolmogorov forcing F0 sin(kf y) x-hat, -F0 kf cos(kf y),
+        # transformed like any field (the C restatement's extension)
+        self.forc = None
+        if p.get("force_amp", 0.0) != 0.0:
+            y = torch.arange(ny, dtype=DT) * (p["ly"] / ny)
+            row = -p["force_amp"] * p["force_k"] * torch.cos(p["force_k"] * y)
+            self.forc = torch.fft.rfft2(row[None, :].expand(nx, ny).contiguous())
 
     # --- transforms and spectral helpers (fft.c, functions.c, velocity.c, curl.c)
     def dfft(self, x):
@@ -101,11 +109,15 @@ class TorchStep:
         """N(omega), N(c1)[, N(c2)] (potential() + nonlin(), etd2rk.c:28,40-51)."""
         T, ifft, dfft = self.T, self.ifft, self.dfft
         eps, ks = self.eps, self.ks
-        lam = q["lambda"]
         ux, uy = self.velocity(w)
         uxr, uyr = ifft(T(ux)), ifft(T(uy))
         # -(u . grad) omega  (nonlin.c:30-101)
         nw = -dfft(uxr * ifft(T(self.ikx(w))) + uyr * ifft(T(self.iky(w))))
+        if self.forc is not None:
+            nw = nw + self.forc
+        if self.model == 0:
+            return nw, None, None
+        lam = q["lambda"]
         if self.model == 1:
             sg = q["sigma"]
             cr = ifft(T(c1))
@@ -168,6 +180,8 @@ class TorchStep:
         dt, ks = self.dt, self.ks
         zw = (-q["nu"] * ks) * dt
         eta = torch.exp(-q["nu"] * dt * ks)
+        if self.model == 0:
+            return eta, self._phi1(zw), self._phi2(zw), None, None, None
         if self.model == 1:
             cc = -1.5 * q["lambda"] * q["sigma"] * self.eps * ks * ks
         else:
@@ -176,9 +190,15 @@ class TorchStep:
         return eta, self._phi1(zw), self._phi2(zw), torch.exp(dt * cc), self._phi1(zc), self._phi2(zc)
 
     def step(self, state, q):
+        eta, z1w, z2w, beta, z1c, z2c = self.coefs(q)
+        if self.model == 0:
+            w = state[0]
+            nw0 = self.rhs(w, None, None, q)[0]
+            w1 = w * eta + nw0 * z1w
+            nw1 = self.rhs(w1, None, None, q)[0]
+            return [w1 + (nw1 - nw0) * z2w]
         w, c1 = state[0], state[1]
         c2 = state[2] if self.model == 2 else None
-        eta, z1w, z2w, beta, z1c, z2c = self.coefs(q)
         nw0, n10, n20 = self.rhs(w, c1, c2, q)
         w1 = w * eta + nw0 * z1w
         c11 = c1 * beta + n10 * z1c
@@ -199,6 +219,13 @@ class TorchStep:
         q = self.params(prm)
         eps = self.eps
         ifft = self.ifft
+        if self.model == 0:
+            # kinetic energy of the truncated velocity (kinetic_energy.c:17-21,43-49,89)
+            # and the enstrophy of the truncated vorticity
+            ux, uy = self.velocity(state[0])
+            u, v = ifft(self.T(ux)), ifft(self.T(uy))
+            wt = ifft(self.T(state[0]))
+            return weights[0] * torch.mean(0.5 * (u * u + v * v)) + weights[1] * torch.mean(0.5 * wt * wt)
         if self.model == 1:
             ch = state[1]
             c = ifft(ch)
@@ -221,7 +248,7 @@ class TorchStep:
         return weights[0] * eb + weights[1] * eg + weights[2] * gp
 
 
-PARAM_NAMES = {1: ("nu", "lambda", "sigma"), 2: ("nu", "lambda", "sigma12", "sigma13", "sigma23")}
+PARAM_NAMES = {0: ("nu",), 1: ("nu", "lambda", "sigma"), 2: ("nu", "lambda", "sigma12", "sigma13", "sigma23")}
 
 
 def forward(p: dict, state, nsteps: int):

@@ -981,6 +981,16 @@ int chns_launches_per_step(const chns_ctx* c) { return c ? c->launches_per_step 
 
 int chns_tma_tiles(const chns_ctx* c) { return c && static_cast<const chns::TmaG*>(c->tmag)->use ? 1 : 0; }
 
+int chns_tune_value(int knob) {
+  switch (knob) {
+    case CHNS_TUNE_TMA_BOX_ROWS: return g_tune_box_rows;
+    case CHNS_TUNE_P1_SPLIT: return g_tune_p1_split;
+    case CHNS_TUNE_P4_GRAD: return g_tune_p4_grad;
+    case CHNS_TUNE_PDL: return g_tune_pdl;
+    default: return -1;
+  }
+}
+
 int chns_tune_override(int knob, int value) {
   if (knob == CHNS_TUNE_TMA_BOX_ROWS) {
     if (value != -1 && (value < 8 || value > 256 || value % 8 != 0)) return CHNS_ERR_ARG;

@@ -112,6 +112,10 @@ int chns_ensemble_create(const chns_params* members, int count, chns_ensemble** 
       release(e);
       return rc;
     }
+    // P1's two CTAs per row fill the GPU for a lone small grid; in an ensemble the
+    // members' branches fill it, and one CTA per row was 1.7% faster on the
+    // 64-member ternary ensemble (unless chns_tune_override chose the split)
+    if (chns_tune_value(CHNS_TUNE_P1_SPLIT) < 0) e->m[i]->p1_split = false;
     if (cudaEventCreateWithFlags(&e->ev[i], cudaEventDisableTiming) != cudaSuccess) {
       release(e);
       return CHNS_ERR_CUDA;

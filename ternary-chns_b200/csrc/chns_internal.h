@@ -25,6 +25,8 @@ extern "C" int chns_field_to_realdbl(chns_ctx* c, int f, int truncate);
 // chns_set_state has written its float part (zero, and at k = 0 the rest of the
 // double k = 0 mode)
 extern "C" int chns_statelo_reset(chns_ctx* c, int f);
+// the value chns_tune_override set for a knob (-1: the tuned table)
+extern "C" int chns_tune_value(int knob);
 
 namespace chns {
 // intermediate buffers of a step: G slots (rows 0..jt) and H slots (rows

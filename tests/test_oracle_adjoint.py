@@ -1,5 +1,5 @@
 """CPU tests of the adjoint's checker: oracle/torch_step.py restates the reference step
-(binary and ternary, coef_mode 1) in torch so that reverse mode gives the exact
+(pure Navier-Stokes, binary and ternary, coef_mode 1) in torch so that reverse mode gives the exact
 gradient of the discrete map.  Pinned here against the C restatement:
 
 * forward: 12 steps from the golden initial states equal the C restatement's to
@@ -75,13 +75,14 @@ def test_gradients_equal_central_differences_of_c_restatement(name):
     for k, g in enumerate([gw] + gcs):
         d = rng.standard_normal(init[k].shape) + 1j * rng.standard_normal(init[k].shape)
         d *= np.abs(init[k]).max() / np.abs(d).max()
-        h = 1e-2 if k == 0 else 1e-6
+        # the phase-field losses are nearly linear in omega; the pure Navier-Stokes one is not
+        h = 1e-2 if k == 0 and p["model"] != 0 else 1e-6
         plus = [s + h * d if i == k else s for i, s in enumerate(init)]
         minus = [s - h * d if i == k else s for i, s in enumerate(init)]
         fd = (_loss_of_c_oracle(p, plus, MA.STEPS) - _loss_of_c_oracle(p, minus, MA.STEPS)) / (2 * h)
         assert abs(_rdot(g, d) - fd) <= 1e-6 * abs(fd), (name, k, _rdot(g, d), fd)
     for i, nm in enumerate(TS.PARAM_NAMES[p["model"]]):
-        h = (1e-1 if nm == "nu" else 1e-6) * abs(p[nm])
+        h = (1e-4 if p["model"] == 0 else 1e-1 if nm == "nu" else 1e-6) * abs(p[nm])
         fd = (_loss_of_c_oracle(dict(p, **{nm: p[nm] + h}), init, MA.STEPS)
               - _loss_of_c_oracle(dict(p, **{nm: p[nm] - h}), init, MA.STEPS)) / (2 * h)
         assert abs(gp[i] - fd) <= 1e-6 * abs(fd), (name, nm, gp[i], fd)
