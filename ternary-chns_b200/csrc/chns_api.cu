@@ -318,6 +318,39 @@ __global__ void k_real_r2d_f32(const float* __restrict__ a, double* __restrict__
     b[i] = (double)a[i];
 }
 // FP32 contexts keep the k = 0 modes in double: copy (0,0) of FFTW staging <-> k0
+// block sums of n doubles (fixed order within and across blocks: reproducible)
+__global__ void k_sum_blocks(const double* __restrict__ a, size_t n, double* part) {
+  __shared__ double red[32];
+  double s = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) s += a[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    part[blockIdx.x] = t;
+  }
+}
+// k0[2 slot] = the field's sum (its unnormalised k = 0 mode), k0[2 slot + 1] = 0
+__global__ void k_sum_finish(const double* __restrict__ part, int nb, double* k0, int slot) {
+  double t = 0.0;
+  for (int b = 0; b < nb; b++) t += part[b];
+  k0[2 * slot] = t;
+  k0[2 * slot + 1] = 0.0;
+}
+// b = (float)(a - sum / n): the field without its mean
+__global__ void k_real_d2r_f32_dev(const double* __restrict__ a, float* __restrict__ b, size_t n,
+                                   const double* __restrict__ k0, int slot) {
+  const double mean = k0[2 * slot] / (double)n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (float)(a[i] - mean);
+}
+// the float k = 0 mode of an S-layout field from the double one
+__global__ void k_k0_to_state(const double* __restrict__ k0, float2* s, int slot) {
+  s[0] = make_float2((float)k0[2 * slot], (float)k0[2 * slot + 1]);
+}
+
 __global__ void k_k0_set(double* k0, const double* st, int slot) {
   k0[2 * slot] = st[0];
   k0[2 * slot + 1] = st[1];
@@ -781,14 +814,25 @@ int chns_realdbl_to_realbuf(chns_ctx* c) {
 // phase field f (0: c / c1, 1: c2) from the real field in c->realdbl: dfft and
 // truncation (init.c:221-225, 253-262); FP32 contexts take its k = 0 mode in double
 int chns_phase_from_realdbl(chns_ctx* c, int f) {
-  int rc = chns_realdbl_to_realbuf(c);
-  if (rc) return rc;
-  c->L->dfft(c, c->realbuf, c->state[1 + f]);
-  c->L->truncate(c, c->state[1 + f]);
   if (c->f32) {
-    // the k = 0 mode in double comes from the same FP32 transform
-    c->L->to_fftw(c, c->state[1 + f], c->stage);
-    k_k0_set<<<1, 1, 0, c->stream>>>(c->k0, c->stage, 1 + f);
+    // FP32: the mean (the k = 0 mode) summed in double and kept there; the float
+    // transform takes the field without it, so that its rounding is relative to the
+    // fluctuations (a spinodal field is a mean of 1/3 or 1/2 with fluctuations of a
+    // few per cent: transformed whole, the fluctuations' spectrum carried errors
+    // ~1e-5 of itself, the mean's rounding spread over every mode)
+    const size_t nn = (size_t)c->n * c->n;
+    const int nb = 128;  // c->redscratch holds (n/2+1) 8 >= 136 doubles
+    k_sum_blocks<<<nb, 256, 0, c->stream>>>(c->realdbl, nn, (double*)c->redscratch);
+    k_sum_finish<<<1, 1, 0, c->stream>>>((const double*)c->redscratch, nb, c->k0, 1 + f);
+    k_real_d2r_f32_dev<<<1024, 256, 0, c->stream>>>(c->realdbl, (float*)c->realbuf, nn, c->k0, 1 + f);
+    c->L->dfft(c, c->realbuf, c->state[1 + f]);
+    c->L->truncate(c, c->state[1 + f]);
+    k_k0_to_state<<<1, 1, 0, c->stream>>>(c->k0, (float2*)c->state[1 + f], 1 + f);
+  } else {
+    int rc = chns_realdbl_to_realbuf(c);
+    if (rc) return rc;
+    c->L->dfft(c, c->realbuf, c->state[1 + f]);
+    c->L->truncate(c, c->state[1 + f]);
   }
   CK(cudaGetLastError());
   return chns_statelo_reset(c, 1 + f);
