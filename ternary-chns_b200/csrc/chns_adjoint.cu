@@ -93,7 +93,7 @@ struct chns_adj {
   void* spec;
   void* phys;
   void* bscr;
-  cudaGraphExec_t rev;  // one reverse step (fixed buffers), or null
+  cudaGraphExec_t rev[2];  // one reverse step per current-step buffer (fixed buffers), or null
   bool rev_tried;
   size_t ncx, nn;
 };
@@ -119,10 +119,14 @@ constexpr int PSET = 9;                                    // physical fields pe
 enum { PU = 0, PV, PWX, PWY, PCT, PCX, PCY, PMU, PFT };     // forward fields, f(c_t)
 enum { PFB = 2 * PSET, PAB, PBB, PFXB, PFYB, PUB, PVB, PWXB, PWYB, PCTB, PCXB, PCYB, NPHYS };
 constexpr int kLossBlocks = 1024;  // blocks of the loss reduction
+constexpr int kWork = 4;           // field-set index of the transposes' work buffers
 constexpr int kAcc = 32;           // accumulators; the loss reduction's per-block partials follow
 
 template <class R> struct Adj {
   static constexpr int NF = 2, NSPEC_ = NSPEC, NPHYS_ = NPHYS, NBSCR = FOP_N, NDCOEF = 9;
+  // allocation: field sets 2 and 3 and the work set after the named fields, then the
+  // second current-step buffer; scratch for sets 0-3 and the work set
+  static constexpr int NSPEC_ALL = NSPEC + 3 * SSET + 4 * NF, NPHYS_ALL = NPHYS + 2 * PSET, NSCR = 5;
   chns_ctx* c;
   chns_adj* a;
   AdjPar<R> P;
@@ -130,7 +134,8 @@ template <class R> struct Adj {
   size_t ncx, nn;
   int blocks_s, blocks_p;
 
-  int cur0() const { return CUW; }
+  int cb = CUW;  // current-step buffer of the step being reversed
+  int curbase(int par) const { return par == 0 ? CUW : NSPEC + 3 * SSET; }
   cx<R>* grad(int f) const { return S(SGW + f); }
   void setup() {
     const chns_params& p = c->p;
@@ -189,8 +194,9 @@ template <class R> struct Adj {
 
   cx<R>* S(int k) const { return (cx<R>*)a->spec + (size_t)k * ncx; }
   R* F(int k) const { return (R*)a->phys + (size_t)k * nn; }
-  cx<R>* SS(int set, int k) const { return S(set * SSET + k); }
-  R* FS(int set, int k) const { return F(set * PSET + k); }
+  // field sets 0, 1 (step of parity 0: u*, u_n), 2, 3 (parity 1), 4: transposes' work
+  cx<R>* SS(int set, int k) const { return set < 2 ? S(set * SSET + k) : S(NSPEC + (set - 2) * SSET + k); }
+  R* FS(int set, int k) const { return set < 2 ? F(set * PSET + k) : F(NPHYS + (set - 2) * PSET + k); }
   void* scratch(int set) const { return (char*)a->bscr + (size_t)set * FOP_N * ncx * sizeof(cx<R>); }
 
   // batched transforms on stream s with the scratch of a field set
@@ -220,48 +226,57 @@ template <class R> struct Adj {
   void transpose_rhs(int set, const cx<R>* cc, const cx<R>* nbw, const cx<R>* nbc, cx<R>* gw, cx<R>* gc) {
     double* pacc = a->acc + 4;
     // transposed spectral tail -> A_bar, B_bar, Fx_bar, Fy_bar
-    k_adj_tail4<R><<<blocks_s, 256, 0, st>>>(P, nbw, nbc, SS(0, SB), ncx);
-    ifft(st, 0, SS(0, SB), F(PAB), 4);
+    k_adj_tail4<R><<<blocks_s, 256, 0, st>>>(P, nbw, nbc, SS(kWork, SB), ncx);
+    ifft(st, kWork, SS(kWork, SB), F(PAB), 4);
     // mu_bar -> c_bar (s1 k^2), f_bar, lambda and sigma partials
     k_adj_mubar<R><<<blocks_p, 256, 0, st>>>(F(PFXB), F(PFYB), FS(set, PCX), FS(set, PCY), F(PUB), nn);
-    dfft(st, 0, F(PUB), SS(0, SXo), 1);
-    k_adj_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(0, SXo), cc, SS(set, SFFo), nbc, gc, S(SY), pacc);
-    ifft(st, 0, S(SY), F(PFB), 1);
+    dfft(st, kWork, F(PUB), SS(kWork, SXo), 1);
+    k_adj_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(kWork, SXo), cc, SS(set, SFFo), nbc, gc, S(SY), pacc);
+    ifft(st, kWork, S(SY), F(PFB), 1);
     // products, then C^T of the seven forward fields
     PhysFields<R> pf{FS(set, PU), FS(set, PV), FS(set, PWX), FS(set, PWY), FS(set, PCT), FS(set, PCX),
                      FS(set, PCY), FS(set, PMU)};
     PhysAdj<R> pa{F(PAB), F(PBB), F(PFXB), F(PFYB), F(PFB), F(PUB), F(PVB), F(PWXB), F(PWYB), F(PCTB), F(PCXB),
                   F(PCYB)};
     k_adj_products<R><<<blocks_p, 256, 0, st>>>(pf, pa, nn);
-    dfft(st, 0, F(PUB), SS(0, SB), FOP_N);
-    k_adj_acc7<R><<<blocks_s, 256, 0, st>>>(P, SS(0, SB), gw, gc, ncx);
+    dfft(st, kWork, F(PUB), SS(kWork, SB), FOP_N);
+    k_adj_acc7<R><<<blocks_s, 256, 0, st>>>(P, SS(kWork, SB), gw, gc, ncx);
   }
 
-  // one reversed step from the current-step slots (CUW..CXC): the transposed
-  // stage 2, right-hand side at u*, stage 1 and right-hand side at u_n.  With a
-  // fork stream the forward fields at u_n are built on a parallel branch.
-  void reverse_step(const R* coef, const double* dcoef, cudaStream_t fork) {
+  // one reversed step from current-step buffer `par` (u_n, u*, N(u_n), N(u*)), whose
+  // forward fields (sets 2 par, 2 par + 1) were built before it: the transposed
+  // stage 2, right-hand side at u*, stage 1 and right-hand side at u_n.  The forward
+  // fields of the next step to reverse (current-step buffer 1 - par) are built on the
+  // fork stream meanwhile, off the chain of dependent kernels.
+  void reverse_step(const R* coef, const double* dcoef, cudaStream_t fork, int par) {
     double* pacc = a->acc + 4;
     cx<R>* gw = S(SGW);
     cx<R>* gc = S(SGC);
+    cb = curbase(par);
+    const int s0 = 2 * par, s1 = 2 * par + 1;
     if (fork) {
       cudaEventRecord(a->ev_fork, st);
       cudaStreamWaitEvent(fork, a->ev_fork, 0);
-      fields(fork, 1, S(CUW), S(CUC));
+      prime(fork, 1 - par);
       cudaEventRecord(a->ev_join, fork);
     }
-    k_adj_etd2<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(CXW), S(CXC), S(CNW), S(CNC), S(SNBW),
-                                            S(SNBC), S(SNBAW), S(SNBAC), pacc);
-    fields(st, 0, S(CSW), S(CSC));
-    transpose_rhs(0, S(CSC), S(SNBW), S(SNBC), gw, gc);
-    k_adj_etd1<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(CUW), S(CUC), S(CNW), S(CNC), S(SNBAW),
-                                            S(SNBAC), pacc);
+    k_adj_etd2<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(cb + 6), S(cb + 7), S(cb + 4), S(cb + 5),
+                                            S(SNBW), S(SNBC), S(SNBAW), S(SNBAC), pacc);
+    transpose_rhs(s0, S(cb + 3), S(SNBW), S(SNBC), gw, gc);
+    k_adj_etd1<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(cb + 0), S(cb + 1), S(cb + 4), S(cb + 5),
+                                            S(SNBAW), S(SNBAC), pacc);
+    transpose_rhs(s1, S(cb + 1), S(SNBAW), S(SNBAC), gw, gc);
     if (fork) {
       cudaStreamWaitEvent(st, a->ev_join, 0);
     } else {
-      fields(st, 1, S(CUW), S(CUC));
+      prime(st, 1 - par);
     }
-    transpose_rhs(1, S(CUC), S(SNBAW), S(SNBAC), gw, gc);
+  }
+  // forward fields of current-step buffer `par` into sets 2 par (at u*), 2 par + 1 (at u_n)
+  void prime(cudaStream_t s, int par) {
+    const int b = curbase(par);
+    fields(s, 2 * par, S(b + 2), S(b + 3));
+    fields(s, 2 * par + 1, S(b + 0), S(b + 1));
   }
 };
 
@@ -286,6 +301,7 @@ enum { PA = 2 * PSET, PXB, NPHYS = PXB + 4 };  // A_bar, then the batch of 4 adj
 
 template <class R> struct AdjNS {
   static constexpr int NF = 1, NSPEC_ = nsadj::NSPEC, NPHYS_ = nsadj::NPHYS, NBSCR = 4, NDCOEF = 3;
+  static constexpr int NSPEC_ALL = NSPEC_ + 3 * nsadj::SSET + 4 * NF, NPHYS_ALL = NPHYS_ + 2 * nsadj::PSET, NSCR = 5;
   chns_ctx* c;
   chns_adj* a;
   AdjPar<R> P;
@@ -295,10 +311,13 @@ template <class R> struct AdjNS {
 
   cx<R>* S(int k) const { return (cx<R>*)a->spec + (size_t)k * ncx; }
   R* F(int k) const { return (R*)a->phys + (size_t)k * nn; }
-  cx<R>* SS(int set, int k) const { return S(set * nsadj::SSET + k); }
-  R* FS(int set, int k) const { return F(set * nsadj::PSET + k); }
+  // field sets 0, 1 (parity 0: u*, u_n), 2, 3 (parity 1), 4: the transposes' work
+  cx<R>* SS(int set, int k) const {
+    return set < 2 ? S(set * nsadj::SSET + k) : S(NSPEC_ + (set - 2) * nsadj::SSET + k);
+  }
+  R* FS(int set, int k) const { return set < 2 ? F(set * nsadj::PSET + k) : F(NPHYS_ + (set - 2) * nsadj::PSET + k); }
   void* scratch(int set) const { return (char*)a->bscr + (size_t)set * NBSCR * ncx * sizeof(cx<R>); }
-  int cur0() const { return nsadj::CUR; }
+  int curbase(int par) const { return par == 0 ? nsadj::CUR : NSPEC_ + 3 * nsadj::SSET; }
   cx<R>* grad(int) const { return S(nsadj::SG); }
 
   void setup() {
@@ -360,37 +379,43 @@ template <class R> struct AdjNS {
   void transpose_rhs(int set, const cx<R>* nbw, cx<R>* gw) {
     using namespace nsadj;
     k_adjns_tail1<R><<<blocks_s, 256, 0, st>>>(P, nbw, S(SA));
-    ifft(st, 0, S(SA), F(PA), 1);
+    ifft(st, kWork, S(SA), F(PA), 1);
     k_adjns_products<R><<<blocks_p, 256, 0, st>>>(FS(set, 0), FS(set, 1), FS(set, 2), FS(set, 3), F(PA), F(PXB),
                                                   F(PXB + 1), F(PXB + 2), F(PXB + 3), nn);
-    dfft(st, 0, F(PXB), SS(0, 0), 4);
-    k_adjns_acc4<R><<<blocks_s, 256, 0, st>>>(P, SS(0, 0), gw, ncx);
+    dfft(st, kWork, F(PXB), SS(kWork, 0), 4);
+    k_adjns_acc4<R><<<blocks_s, 256, 0, st>>>(P, SS(kWork, 0), gw, ncx);
   }
-  // one reversed step from the current-step slots (u_n, u*, N(u_n), N(u*))
-  void reverse_step(const R* coef, const double* dcoef, cudaStream_t fork) {
+  // one reversed step from current-step buffer `par` (u_n, u*, N(u_n), N(u*)), whose
+  // forward fields were built before it; the next step's are built on the fork
+  void reverse_step(const R* coef, const double* dcoef, cudaStream_t fork, int par) {
     using namespace nsadj;
     double* pacc = a->acc + 4;
     cx<R>* gw = S(SG);
-    const cx<R>* un = S(CUR);
-    const cx<R>* us = S(CUR + 1);
-    const cx<R>* nn_ = S(CUR + 2);
-    const cx<R>* ns_ = S(CUR + 3);
+    const int b = curbase(par);
+    const cx<R>* un = S(b);
+    const cx<R>* nn_ = S(b + 2);
+    const cx<R>* ns_ = S(b + 3);
     if (fork) {
       cudaEventRecord(a->ev_fork, st);
       cudaStreamWaitEvent(fork, a->ev_fork, 0);
-      fields(fork, 1, un);
+      prime(fork, 1 - par);
       cudaEventRecord(a->ev_join, fork);
     }
     k_adjns_etd2<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, ns_, nn_, S(SNB), S(SNA), pacc);
-    fields(st, 0, us);
-    transpose_rhs(0, S(SNB), gw);
+    transpose_rhs(2 * par, S(SNB), gw);
     k_adjns_etd1<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, un, nn_, S(SNA), pacc);
+    transpose_rhs(2 * par + 1, S(SNA), gw);
     if (fork) {
       cudaStreamWaitEvent(st, a->ev_join, 0);
     } else {
-      fields(st, 1, un);
+      prime(st, 1 - par);
     }
-    transpose_rhs(1, S(SNA), gw);
+  }
+  // forward fields of current-step buffer `par` into sets 2 par (at u*), 2 par + 1 (at u_n)
+  void prime(cudaStream_t s, int par) {
+    const int b = curbase(par);
+    fields(s, 2 * par, S(b + 1));
+    fields(s, 2 * par + 1, S(b));
   }
 };
 
@@ -415,6 +440,8 @@ enum { PTAIL = 2 * PSET, PMUB = PTAIL + 5, PMFB = PMUB + 2, PXB = PMFB + 2, NPHY
 
 template <class R> struct AdjT3 {
   static constexpr int NF = 3, NSPEC_ = tern::NSPEC, NPHYS_ = tern::NPHYS, NBSCR = T_N, NDCOEF = 6;
+  static constexpr int NSPEC_ALL = NSPEC_ + 3 * tern::SSET + 4 * NF, NPHYS_ALL = NPHYS_ + 2 * tern::PSET, NSCR = 5;
+  int cb = tern::CUR;  // current-step buffer of the step being reversed
   chns_ctx* c;
   chns_adj* a;
   AdjParT<R> P;
@@ -424,15 +451,18 @@ template <class R> struct AdjT3 {
 
   cx<R>* S(int k) const { return (cx<R>*)a->spec + (size_t)k * ncx; }
   R* F(int k) const { return (R*)a->phys + (size_t)k * nn; }
-  cx<R>* SS(int set, int k) const { return S(set * tern::SSET + k); }
-  R* FS(int set, int k) const { return F(set * tern::PSET + k); }
+  // field sets 0, 1 (parity 0: u*, u_n), 2, 3 (parity 1), 4: the transposes' work
+  cx<R>* SS(int set, int k) const {
+    return set < 2 ? S(set * tern::SSET + k) : S(NSPEC_ + (set - 2) * tern::SSET + k);
+  }
+  R* FS(int set, int k) const { return set < 2 ? F(set * tern::PSET + k) : F(NPHYS_ + (set - 2) * tern::PSET + k); }
   void* scratch(int set) const { return (char*)a->bscr + (size_t)set * T_N * ncx * sizeof(cx<R>); }
-  int cur0() const { return tern::CUR; }
+  int curbase(int par) const { return par == 0 ? tern::CUR : NSPEC_ + 3 * tern::SSET; }
   cx<R>* grad(int f) const { return S(tern::SG + f); }
-  cx<R>* cu(int f) const { return S(tern::CUR + f); }      // u_n
-  cx<R>* cs(int f) const { return S(tern::CUR + 3 + f); }  // u*
-  cx<R>* cn(int f) const { return S(tern::CUR + 6 + f); }  // N(u_n)
-  cx<R>* cx_(int f) const { return S(tern::CUR + 9 + f); } // N(u*)
+  cx<R>* cu(int f) const { return S(cb + f); }       // u_n
+  cx<R>* cs(int f) const { return S(cb + 3 + f); }   // u*
+  cx<R>* cn(int f) const { return S(cb + 6 + f); }   // N(u_n)
+  cx<R>* cx_(int f) const { return S(cb + 9 + f); }  // N(u*)
 
   void ifft(cudaStream_t s, int set, const cx<R>* in, R* x, int nb) {
     c->stream = s;
@@ -501,29 +531,32 @@ template <class R> struct AdjT3 {
   // parameter sums into acc[8 + 2 ..]
   void transpose_rhs(int set, const cx<R>* c1, const cx<R>* c2, const cx<R>* nw, const cx<R>* n1, const cx<R>* n2) {
     double* pacc = a->acc + 8;
-    k_adj3_tail<R><<<blocks_s, 256, 0, st>>>(P, nw, n1, n2, SS(0, tern::SB), ncx);
-    ifft(st, 0, SS(0, tern::SB), F(tern::PTAIL), 5);
+    k_adj3_tail<R><<<blocks_s, 256, 0, st>>>(P, nw, n1, n2, SS(kWork, tern::SB), ncx);
+    ifft(st, kWork, SS(kWork, tern::SB), F(tern::PTAIL), 5);
     const int b = tern::PF;
     PhysT<R> pf{FS(set, b + T_U),   FS(set, b + T_V),   FS(set, b + T_WX),  FS(set, b + T_WY),  FS(set, b + T_C1X),
                 FS(set, b + T_C1Y), FS(set, b + T_C2X), FS(set, b + T_C2Y), FS(set, tern::PMU), FS(set, tern::PMU + 1)};
     AdjT5<R> at{F(tern::PTAIL), F(tern::PTAIL + 1), F(tern::PTAIL + 2), F(tern::PTAIL + 3), F(tern::PTAIL + 4)};
     k_adj3_products<R><<<blocks_p, 256, 0, st>>>(P, pf, at, F(tern::PXB), F(tern::PMUB), nn, pacc + 2);
-    dfft(st, 0, F(tern::PMUB), SS(0, tern::SX), 2);
-    k_adj3_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(0, tern::SX), c1, c2, SS(set, tern::SFF), n1, n2, grad(1), grad(2),
+    dfft(st, kWork, F(tern::PMUB), SS(kWork, tern::SX), 2);
+    k_adj3_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(kWork, tern::SX), c1, c2, SS(set, tern::SFF), n1, n2, grad(1), grad(2),
                                            S(tern::SYB), ncx, pacc + 6);
-    ifft(st, 0, S(tern::SYB), F(tern::PMFB), 2);
+    ifft(st, kWork, S(tern::SYB), F(tern::PMFB), 2);
     k_adj3_bulk_bar<R><<<blocks_p, 256, 0, st>>>(P, FS(set, b + T_C1), FS(set, b + T_C2), F(tern::PMFB),
                                                  F(tern::PXB), nn, pacc + 10);
-    dfft(st, 0, F(tern::PXB), SS(0, tern::SB), T_N);
-    k_adj3_acc<R><<<blocks_s, 256, 0, st>>>(P, SS(0, tern::SB), grad(0), grad(1), grad(2), ncx);
+    dfft(st, kWork, F(tern::PXB), SS(kWork, tern::SB), T_N);
+    k_adj3_acc<R><<<blocks_s, 256, 0, st>>>(P, SS(kWork, tern::SB), grad(0), grad(1), grad(2), ncx);
   }
 
-  void reverse_step(const R* coef, const double* dcoef, cudaStream_t fork) {
+  // one reversed step from current-step buffer `par`, whose forward fields were
+  // built before it; the next step's (buffer 1 - par) are built on the fork
+  void reverse_step(const R* coef, const double* dcoef, cudaStream_t fork, int par) {
     double* pacc = a->acc + 8;
+    cb = curbase(par);
     if (fork) {
       cudaEventRecord(a->ev_fork, st);
       cudaStreamWaitEvent(fork, a->ev_fork, 0);
-      fields(fork, 1, cu(0), cu(1), cu(2));
+      prime(fork, 1 - par);
       cudaEventRecord(a->ev_join, fork);
     }
     CFields3<R> g{{grad(0), grad(1), grad(2)}};
@@ -532,18 +565,22 @@ template <class R> struct AdjT3 {
     Fields3<R> nba{{S(tern::SNA), S(tern::SNA + 1), S(tern::SNA + 2)}};
     Fields3<R> gm{{grad(0), grad(1), grad(2)}};
     k_adj3_etd2<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, g, nst, nnn, nbs, nba, pacc);
-    fields(st, 0, cs(0), cs(1), cs(2));
-    transpose_rhs(0, cs(1), cs(2), S(tern::SNB), S(tern::SNB + 1), S(tern::SNB + 2));
+    transpose_rhs(2 * par, cs(1), cs(2), S(tern::SNB), S(tern::SNB + 1), S(tern::SNB + 2));
     k_adj3_etd1<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gm, un, nnn, nba, pacc);
+    transpose_rhs(2 * par + 1, cu(1), cu(2), S(tern::SNA), S(tern::SNA + 1), S(tern::SNA + 2));
     if (fork) {
       cudaStreamWaitEvent(st, a->ev_join, 0);
     } else {
-      fields(st, 1, cu(0), cu(1), cu(2));
+      prime(st, 1 - par);
     }
-    transpose_rhs(1, cu(1), cu(2), S(tern::SNA), S(tern::SNA + 1), S(tern::SNA + 2));
+  }
+  // forward fields of current-step buffer `par` into sets 2 par (at u*), 2 par + 1 (at u_n)
+  void prime(cudaStream_t s, int par) {
+    const int b = curbase(par);
+    fields(s, 2 * par, S(b + 3), S(b + 4), S(b + 5));
+    fields(s, 2 * par + 1, S(b + 0), S(b + 1), S(b + 2));
   }
 
-  // loss (free_energy.c ternary, untruncated c_i and gradients) and its gradient
   void loss(const double* lw) {
     const chns_params& p = c->p;
     k_adj3_loss_prep<R><<<blocks_s, 256, 0, st>>>(P, (const cx<R>*)c->state[1], (const cx<R>*)c->state[2],
@@ -631,9 +668,9 @@ template <class A> int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
   a->ncx = ncx;
   a->nn = nn;
   if (!a->dcoef) {
-    if (cudaMalloc(&a->spec, A::NSPEC_ * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
-    if (cudaMalloc(&a->phys, A::NPHYS_ * nn * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
-    if (cudaMalloc(&a->bscr, 2 * (size_t)A::NBSCR * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->spec, A::NSPEC_ALL * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->phys, A::NPHYS_ALL * nn * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->bscr, (size_t)A::NSCR * A::NBSCR * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMalloc((void**)&a->acc, (kAcc + 4 * kLossBlocks) * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
     std::vector<double> d;
     A::dcoef_tables(c, d);
@@ -724,15 +761,27 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
     if (rc) return rc;
   }
   ad.loss(lw);
-  // the reversed step as a CUDA graph on its fixed buffers (eager if capture fails)
-  if (!a->rev && !a->rev_tried) {
+  // the reversed step as a CUDA graph per current-step buffer, on fixed buffers
+  // (eager if a capture fails)
+  if (!a->rev[0] && !a->rev_tried) {
     a->rev_tried = true;
-    cudaGraph_t g = nullptr;
-    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      ad.reverse_step(coef, dcoef, a->fork);
-      if (cudaStreamEndCapture(st, &g) == cudaSuccess && g) {
-        if (cudaGraphInstantiate(&a->rev, g, 0) != cudaSuccess) a->rev = nullptr;
-        cudaGraphDestroy(g);
+    bool ok = true;
+    for (int par = 0; par < 2 && ok; par++) {
+      cudaGraph_t g = nullptr;
+      ok = false;
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        ad.reverse_step(coef, dcoef, a->fork, par);
+        if (cudaStreamEndCapture(st, &g) == cudaSuccess && g) {
+          ok = cudaGraphInstantiate(&a->rev[par], g, 0) == cudaSuccess;
+          cudaGraphDestroy(g);
+        }
+      }
+      if (!ok) a->rev[par] = nullptr;
+    }
+    if (!ok) {
+      for (int par = 0; par < 2; par++) {
+        if (a->rev[par]) cudaGraphExecDestroy(a->rev[par]);
+        a->rev[par] = nullptr;
       }
     }
     cudaGetLastError();
@@ -757,16 +806,24 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
     ACK(cudaEventRecord(a->ev_ready[b], side));
     return CHNS_OK;
   };
+  // Steps alternate between two current-step buffers: while step k (buffer k & 1) is
+  // reversed, step k - 1 is already in the other buffer and its forward fields are
+  // built on the graph's parallel branch, so no reversed step waits for its own.
   auto reverse = [&](int s) -> int {
     const int b = s % nbuf, len = (s * ckpt + ckpt <= nsteps) ? ckpt : nsteps - s * ckpt;
     if (s != nseg - 1) ACK(cudaStreamWaitEvent(st, a->ev_ready[b], 0));
+    auto slot_of = [&](int k) { return segbase + ((size_t)b * ckpt + k) * slot; };
+    const int p0 = (len - 1) & 1;
+    ACK(cudaMemcpyAsync(ad.S(ad.curbase(p0)), slot_of(len - 1), slot, cudaMemcpyDeviceToDevice, st));
+    ad.prime(st, p0);
     for (int k = len - 1; k >= 0; k--) {
-      ACK(cudaMemcpyAsync(ad.S(ad.cur0()), segbase + ((size_t)b * ckpt + k) * slot, slot, cudaMemcpyDeviceToDevice,
-                          st));
-      if (a->rev) {
-        ACK(cudaGraphLaunch(a->rev, st));
+      const int par = k & 1;
+      if (k > 0)
+        ACK(cudaMemcpyAsync(ad.S(ad.curbase(1 - par)), slot_of(k - 1), slot, cudaMemcpyDeviceToDevice, st));
+      if (a->rev[par]) {
+        ACK(cudaGraphLaunch(a->rev[par], st));
       } else {
-        ad.reverse_step(coef, dcoef, nullptr);
+        ad.reverse_step(coef, dcoef, nullptr, par);
       }
     }
     ACK(cudaEventRecord(a->ev_free[b], st));
@@ -810,7 +867,8 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
 void chns_adj_free(chns_ctx* c) {
   chns_adj* a = c->adj;
   if (!a) return;
-  if (a->rev) cudaGraphExecDestroy(a->rev);
+  for (int p = 0; p < 2; p++)
+    if (a->rev[p]) cudaGraphExecDestroy(a->rev[p]);
   if (a->side) {
     cudaStreamSynchronize(a->side);
     cudaStreamDestroy(a->side);
