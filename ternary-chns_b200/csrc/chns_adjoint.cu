@@ -94,16 +94,17 @@ struct chns_adj {
   void* phys;
   void* bscr;
   cudaGraphExec_t rev[2];  // one reverse step per current-step buffer (fixed buffers), or null
+  void* rf;                // RecFields of the step being reversed (binary: recorded forward fields)
   bool rev_tried;
   size_t ncx, nn;
 };
 
 namespace {
 
-// Two field sets (0: the state u*, 1: the state u_n of a reversed step), each
-// with its own spectral batch, scratch and F[f(c_t)] and its own physical
-// forward fields, so that the forward fields at u_n are computed on a branch
-// parallel to the transposed right-hand side at u*.
+// Binary buffers: two field sets of a spectral batch, scratch and F[f] and of
+// physical fields (set 0: the loss; set 1: the transposes' work buffers; the
+// transposes read the forward fields the forward step recorded), the named
+// spectral fields and one current-step buffer.
 constexpr int SSET = 9;                      // spectral fields per set
 enum { SB = 0, SXo = 7, SFFo = 8 };           // batch of 7, scratch, F[f]
 enum {
@@ -124,9 +125,12 @@ constexpr int kAcc = 32;           // accumulators; the loss reduction's per-blo
 
 template <class R> struct Adj {
   static constexpr int NF = 2, NSPEC_ = NSPEC, NPHYS_ = NPHYS, NBSCR = FOP_N, NDCOEF = 9;
-  // allocation: field sets 2 and 3 and the work set after the named fields, then the
-  // second current-step buffer; scratch for sets 0-3 and the work set
-  static constexpr int NSPEC_ALL = NSPEC + 3 * SSET + 4 * NF, NPHYS_ALL = NPHYS + 2 * PSET, NSCR = 5;
+  static constexpr int NSPEC_ALL = NSPEC, NPHYS_ALL = NPHYS, NSCR = 2;
+  static constexpr int kW = 1;  // field set of the transposes' work buffers
+  // the forward step records what the transposes need (REC kernels): per right-hand
+  // side REC_REAL real fields and one spectral field, kept with each segment slot
+  static constexpr bool REC = true;
+  static constexpr int REC_REAL = 8;
   chns_ctx* c;
   chns_adj* a;
   AdjPar<R> P;
@@ -135,7 +139,7 @@ template <class R> struct Adj {
   int blocks_s, blocks_p;
 
   int cb = CUW;  // current-step buffer of the step being reversed
-  int curbase(int par) const { return par == 0 ? CUW : NSPEC + 3 * SSET; }
+  int curbase(int) const { return CUW; }
   cx<R>* grad(int f) const { return S(SGW + f); }
   void setup() {
     const chns_params& p = c->p;
@@ -194,9 +198,8 @@ template <class R> struct Adj {
 
   cx<R>* S(int k) const { return (cx<R>*)a->spec + (size_t)k * ncx; }
   R* F(int k) const { return (R*)a->phys + (size_t)k * nn; }
-  // field sets 0, 1 (step of parity 0: u*, u_n), 2, 3 (parity 1), 4: transposes' work
-  cx<R>* SS(int set, int k) const { return set < 2 ? S(set * SSET + k) : S(NSPEC + (set - 2) * SSET + k); }
-  R* FS(int set, int k) const { return set < 2 ? F(set * PSET + k) : F(NPHYS + (set - 2) * PSET + k); }
+  cx<R>* SS(int set, int k) const { return S(set * SSET + k); }
+  R* FS(int set, int k) const { return F(set * PSET + k); }
   void* scratch(int set) const { return (char*)a->bscr + (size_t)set * FOP_N * ncx * sizeof(cx<R>); }
 
   // batched transforms on stream s with the scratch of a field set
@@ -211,73 +214,43 @@ template <class R> struct Adj {
     c->stream = st;
   }
 
-  // forward fields of the right-hand side at (w, cc) into field set `set`
-  void fields(cudaStream_t s, int set, const cx<R>* w, const cx<R>* cc) {
-    k_adj_fwd_prep7<R><<<blocks_s, 256, 0, s>>>(P, w, cc, SS(set, SB), ncx);
-    ifft(s, set, SS(set, SB), FS(set, PU), FOP_N);
-    k_adj_bulk<R><<<blocks_p, 256, 0, s>>>(FS(set, PCT), FS(set, PFT), nn);
-    dfft(s, set, FS(set, PFT), SS(set, SFFo), 1);
-    k_adj_mu_prep<R><<<blocks_s, 256, 0, s>>>(P, cc, SS(set, SFFo), SS(set, SXo));
-    ifft(s, set, SS(set, SXo), FS(set, PMU), 1);
-  }
-
-  // (gw, gc) += J_N(state)^T (nbw, nbc) with the forward fields of set `set`
-  // (c_hat of the state: cc); parameter partials into acc[4..6].  Scratch of set 0.
-  void transpose_rhs(int set, const cx<R>* cc, const cx<R>* nbw, const cx<R>* nbc, cx<R>* gw, cx<R>* gc) {
+  // (gw, gc) += J_N(state)^T (nbw, nbc) with the recorded forward fields a->rf[r]
+  // (c_hat of the state: cc); parameter partials into acc[4..6]
+  void transpose_rhs(int r, const cx<R>* cc, const cx<R>* nbw, const cx<R>* nbc, cx<R>* gw, cx<R>* gc) {
+    const RecFields<R>* rf = static_cast<const RecFields<R>*>(a->rf) + r;
     double* pacc = a->acc + 4;
     // transposed spectral tail -> A_bar, B_bar, Fx_bar, Fy_bar
-    k_adj_tail4<R><<<blocks_s, 256, 0, st>>>(P, nbw, nbc, SS(kWork, SB), ncx);
-    ifft(st, kWork, SS(kWork, SB), F(PAB), 4);
+    k_adj_tail4<R><<<blocks_s, 256, 0, st>>>(P, nbw, nbc, SS(kW, SB), ncx);
+    ifft(st, kW, SS(kW, SB), F(PAB), 4);
     // mu_bar -> c_bar (s1 k^2), f_bar, lambda and sigma partials
-    k_adj_mubar<R><<<blocks_p, 256, 0, st>>>(F(PFXB), F(PFYB), FS(set, PCX), FS(set, PCY), F(PUB), nn);
-    dfft(st, kWork, F(PUB), SS(kWork, SXo), 1);
-    k_adj_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(kWork, SXo), cc, SS(set, SFFo), nbc, gc, S(SY), pacc);
-    ifft(st, kWork, S(SY), F(PFB), 1);
+    k_adj_mubar<R><<<blocks_p, 256, 0, st>>>(F(PFXB), F(PFYB), rf, F(PUB), nn);
+    dfft(st, kW, F(PUB), SS(kW, SXo), 1);
+    k_adj_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(kW, SXo), cc, rf, nbc, gc, S(SY), pacc);
+    ifft(st, kW, S(SY), F(PFB), 1);
     // products, then C^T of the seven forward fields
-    PhysFields<R> pf{FS(set, PU), FS(set, PV), FS(set, PWX), FS(set, PWY), FS(set, PCT), FS(set, PCX),
-                     FS(set, PCY), FS(set, PMU)};
     PhysAdj<R> pa{F(PAB), F(PBB), F(PFXB), F(PFYB), F(PFB), F(PUB), F(PVB), F(PWXB), F(PWYB), F(PCTB), F(PCXB),
                   F(PCYB)};
-    k_adj_products<R><<<blocks_p, 256, 0, st>>>(pf, pa, nn);
-    dfft(st, kWork, F(PUB), SS(kWork, SB), FOP_N);
-    k_adj_acc7<R><<<blocks_s, 256, 0, st>>>(P, SS(kWork, SB), gw, gc, ncx);
+    k_adj_products<R><<<blocks_p, 256, 0, st>>>(rf, pa, nn);
+    dfft(st, kW, F(PUB), SS(kW, SB), FOP_N);
+    k_adj_acc7<R><<<blocks_s, 256, 0, st>>>(P, SS(kW, SB), gw, gc, ncx);
   }
 
-  // one reversed step from current-step buffer `par` (u_n, u*, N(u_n), N(u*)), whose
-  // forward fields (sets 2 par, 2 par + 1) were built before it: the transposed
-  // stage 2, right-hand side at u*, stage 1 and right-hand side at u_n.  The forward
-  // fields of the next step to reverse (current-step buffer 1 - par) are built on the
-  // fork stream meanwhile, off the chain of dependent kernels.
-  void reverse_step(const R* coef, const double* dcoef, cudaStream_t fork, int par) {
+  // one reversed step from the current-step buffer (u_n, u*, N(u_n), N(u*)) with the
+  // forward fields recorded for it (a->rf[0] at u*, a->rf[1] at u_n): the transposed
+  // stage 2, right-hand side at u*, stage 1 and right-hand side at u_n
+  void reverse_step(const R* coef, const double* dcoef, cudaStream_t, int) {
     double* pacc = a->acc + 4;
     cx<R>* gw = S(SGW);
     cx<R>* gc = S(SGC);
-    cb = curbase(par);
-    const int s0 = 2 * par, s1 = 2 * par + 1;
-    if (fork) {
-      cudaEventRecord(a->ev_fork, st);
-      cudaStreamWaitEvent(fork, a->ev_fork, 0);
-      prime(fork, 1 - par);
-      cudaEventRecord(a->ev_join, fork);
-    }
+    cb = curbase(0);
     k_adj_etd2<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(cb + 6), S(cb + 7), S(cb + 4), S(cb + 5),
                                             S(SNBW), S(SNBC), S(SNBAW), S(SNBAC), pacc);
-    transpose_rhs(s0, S(cb + 3), S(SNBW), S(SNBC), gw, gc);
+    transpose_rhs(0, S(cb + 3), S(SNBW), S(SNBC), gw, gc);
     k_adj_etd1<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(cb + 0), S(cb + 1), S(cb + 4), S(cb + 5),
                                             S(SNBAW), S(SNBAC), pacc);
-    transpose_rhs(s1, S(cb + 1), S(SNBAW), S(SNBAC), gw, gc);
-    if (fork) {
-      cudaStreamWaitEvent(st, a->ev_join, 0);
-    } else {
-      prime(st, 1 - par);
-    }
+    transpose_rhs(1, S(cb + 1), S(SNBAW), S(SNBAC), gw, gc);
   }
-  // forward fields of current-step buffer `par` into sets 2 par (at u*), 2 par + 1 (at u_n)
-  void prime(cudaStream_t s, int par) {
-    const int b = curbase(par);
-    fields(s, 2 * par, S(b + 2), S(b + 3));
-    fields(s, 2 * par + 1, S(b + 0), S(b + 1));
-  }
+  void prime(cudaStream_t, int) {}  // the forward fields are recorded, not rebuilt
 };
 
 // ---------------------------------------------------------------------------
@@ -302,6 +275,8 @@ enum { PA = 2 * PSET, PXB, NPHYS = PXB + 4 };  // A_bar, then the batch of 4 adj
 template <class R> struct AdjNS {
   static constexpr int NF = 1, NSPEC_ = nsadj::NSPEC, NPHYS_ = nsadj::NPHYS, NBSCR = 4, NDCOEF = 3;
   static constexpr int NSPEC_ALL = NSPEC_ + 3 * nsadj::SSET + 4 * NF, NPHYS_ALL = NPHYS_ + 2 * nsadj::PSET, NSCR = 5;
+  static constexpr bool REC = false;
+  static constexpr int REC_REAL = 0;
   chns_ctx* c;
   chns_adj* a;
   AdjPar<R> P;
@@ -441,6 +416,8 @@ enum { PTAIL = 2 * PSET, PMUB = PTAIL + 5, PMFB = PMUB + 2, PXB = PMFB + 2, NPHY
 template <class R> struct AdjT3 {
   static constexpr int NF = 3, NSPEC_ = tern::NSPEC, NPHYS_ = tern::NPHYS, NBSCR = T_N, NDCOEF = 6;
   static constexpr int NSPEC_ALL = NSPEC_ + 3 * tern::SSET + 4 * NF, NPHYS_ALL = NPHYS_ + 2 * tern::PSET, NSCR = 5;
+  static constexpr bool REC = false;
+  static constexpr int REC_REAL = 0;
   int cb = tern::CUR;  // current-step buffer of the step being reversed
   chns_ctx* c;
   chns_adj* a;
@@ -626,17 +603,22 @@ template <class R> struct AdjT3 {
 };
 
 // one forward step that also records u_n, u*, N(u_n) and N(u*) (nf fields each)
-// into a segment slot
-int record_step(chns_ctx* c, char* slot, size_t fbytes, int nf) {
+// into a segment slot; with recb > 0 (binary) the stages' REC kernels also record the
+// forward fields of the right-hand sides at u_n and at u* (recb bytes each) behind them
+int record_step(chns_ctx* c, char* slot, size_t fbytes, int nf, size_t recb) {
   cudaStream_t st = c->stream;
   for (int f = 0; f < nf; f++) ACK(cudaMemcpyAsync(slot + f * fbytes, c->state[f], fbytes, cudaMemcpyDeviceToDevice, st));
+  char* rec = slot + 4 * (size_t)nf * fbytes;
+  c->rec = recb ? rec : nullptr;
   c->L->stage(c, 1);
+  c->rec = recb ? rec + recb : nullptr;
   for (int f = 0; f < nf; f++) {
     ACK(cudaMemcpyAsync(slot + (nf + f) * fbytes, c->state[f], fbytes, cudaMemcpyDeviceToDevice, st));
     ACK(cudaMemcpyAsync(slot + (2 * nf + f) * fbytes, c->saved[f], fbytes, cudaMemcpyDeviceToDevice, st));
     c->nstar[f] = slot + (3 * nf + f) * fbytes;
   }
   c->L->stage(c, 2);
+  c->rec = nullptr;
   for (int f = 0; f < 3; f++) c->nstar[f] = nullptr;
   return CHNS_OK;
 }
@@ -656,6 +638,16 @@ int snapshot_load(chns_ctx* c, const void* src, const double* srck0) {
   return CHNS_OK;
 }
 
+// bytes of one recorded forward right-hand side (binary) and of one segment slot
+template <class A> size_t rec_bytes(const chns_ctx* c) {
+  if (!A::REC) return 0;
+  const size_t nn = (size_t)c->n * c->n;
+  return A::REC_REAL * nn * c->rsz + (size_t)c->n * c->nr * 2 * c->rsz;
+}
+template <class A> size_t slot_bytes(const chns_ctx* c) {
+  return 4 * (size_t)A::NF * c->n * c->nr * 2 * c->rsz + 2 * rec_bytes<A>(c);
+}
+
 template <class A> int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
   if (!c->adj) {
     c->adj = (chns_adj*)calloc(1, sizeof(chns_adj));
@@ -672,6 +664,7 @@ template <class A> int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
     if (cudaMalloc(&a->phys, A::NPHYS_ALL * nn * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMalloc(&a->bscr, (size_t)A::NSCR * A::NBSCR * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMalloc((void**)&a->acc, (kAcc + 4 * kLossBlocks) * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->rf, 2 * sizeof(RecFields<double>)) != cudaSuccess) return CHNS_ERR_NOMEM;
     std::vector<double> d;
     A::dcoef_tables(c, d);
     if (cudaMalloc(&a->dcoef, d.size() * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
@@ -695,11 +688,12 @@ template <class A> int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
     a->seg = nullptr;
     a->cap_states = 0;
     a->seg_len = 0;
-    if (cudaMalloc(&a->seg, 4 * A::NF * fbytes * 2 * (size_t)seglen) == cudaSuccess) {
+    const size_t slot = slot_bytes<A>(c);
+    if (cudaMalloc(&a->seg, slot * 2 * (size_t)seglen) == cudaSuccess) {
       a->cap_states = 2 * seglen;
     } else {
       cudaGetLastError();
-      if (cudaMalloc(&a->seg, 4 * A::NF * fbytes * (size_t)seglen) != cudaSuccess) return CHNS_ERR_NOMEM;
+      if (cudaMalloc(&a->seg, slot * (size_t)seglen) != cudaSuccess) return CHNS_ERR_NOMEM;
       a->cap_states = seglen;
     }
     a->seg_len = seglen;
@@ -751,13 +745,14 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
   // forward sweep with checkpoints (checkpoint nseg keeps u_0 for restoring);
   // the last segment is recorded on the way
   char* segbase = (char*)a->seg;
-  const size_t slot = 4 * (size_t)A::NF * bytes;
+  const size_t cur = 4 * (size_t)A::NF * bytes;  // u_n, u*, N(u_n), N(u*)
+  const size_t recb = rec_bytes<A>(c), slot = slot_bytes<A>(c);
   const int nlast = (nseg - 1) * ckpt;
   const size_t lastbuf = a->cap_states >= 2 * ckpt ? (size_t)((nseg - 1) % 2) * ckpt : 0;
   if ((rc = snapshot_save(c, a->ckpt[nseg], a->ckptk0[nseg]))) return rc;
   for (int n = 0; n < nsteps; n++) {
     if (n % ckpt == 0 && (rc = snapshot_save(c, a->ckpt[n / ckpt], a->ckptk0[n / ckpt]))) return rc;
-    rc = n >= nlast ? record_step(c, segbase + (lastbuf + n - nlast) * slot, bytes, A::NF) : chns_step(c, 1);
+    rc = n >= nlast ? record_step(c, segbase + (lastbuf + n - nlast) * slot, bytes, A::NF, recb) : chns_step(c, 1);
     if (rc) return rc;
   }
   ad.loss(lw);
@@ -766,7 +761,7 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
   if (!a->rev[0] && !a->rev_tried) {
     a->rev_tried = true;
     bool ok = true;
-    for (int par = 0; par < 2 && ok; par++) {
+    for (int par = 0; par < (A::REC ? 1 : 2) && ok; par++) {
       cudaGraph_t g = nullptr;
       ok = false;
       if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
@@ -800,7 +795,7 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
     c->stream = side;
     int r = snapshot_load(c, a->ckpt[s], a->ckptk0[s]);
     for (int k = 0; k < len && !r; k++)
-      r = record_step(c, segbase + ((size_t)b * ckpt + k) * slot, bytes, A::NF);
+      r = record_step(c, segbase + ((size_t)b * ckpt + k) * slot, bytes, A::NF, recb);
     c->stream = st;
     if (r) return r;
     ACK(cudaEventRecord(a->ev_ready[b], side));
@@ -813,13 +808,28 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
     const int b = s % nbuf, len = (s * ckpt + ckpt <= nsteps) ? ckpt : nsteps - s * ckpt;
     if (s != nseg - 1) ACK(cudaStreamWaitEvent(st, a->ev_ready[b], 0));
     auto slot_of = [&](int k) { return segbase + ((size_t)b * ckpt + k) * slot; };
+    if (A::REC) {  // one current-step buffer; the step's forward fields were recorded with it
+      for (int k = len - 1; k >= 0; k--) {
+        char* sk = slot_of(k);
+        ACK(cudaMemcpyAsync(ad.S(ad.curbase(0)), sk, cur, cudaMemcpyDeviceToDevice, st));
+        k_adj_set_rec<R><<<1, 1, 0, st>>>(static_cast<RecFields<R>*>(a->rf), (const R*)(sk + cur + recb),
+                                          (const R*)(sk + cur), a->nn);
+        if (a->rev[0]) {
+          ACK(cudaGraphLaunch(a->rev[0], st));
+        } else {
+          ad.reverse_step(coef, dcoef, nullptr, 0);
+        }
+      }
+      ACK(cudaEventRecord(a->ev_free[b], st));
+      return CHNS_OK;
+    }
     const int p0 = (len - 1) & 1;
-    ACK(cudaMemcpyAsync(ad.S(ad.curbase(p0)), slot_of(len - 1), slot, cudaMemcpyDeviceToDevice, st));
+    ACK(cudaMemcpyAsync(ad.S(ad.curbase(p0)), slot_of(len - 1), cur, cudaMemcpyDeviceToDevice, st));
     ad.prime(st, p0);
     for (int k = len - 1; k >= 0; k--) {
       const int par = k & 1;
       if (k > 0)
-        ACK(cudaMemcpyAsync(ad.S(ad.curbase(1 - par)), slot_of(k - 1), slot, cudaMemcpyDeviceToDevice, st));
+        ACK(cudaMemcpyAsync(ad.S(ad.curbase(1 - par)), slot_of(k - 1), cur, cudaMemcpyDeviceToDevice, st));
       if (a->rev[par]) {
         ACK(cudaGraphLaunch(a->rev[par], st));
       } else {
@@ -882,6 +892,7 @@ void chns_adj_free(chns_ctx* c) {
     }
   }
   if (a->spec) cudaFree(a->spec);
+  if (a->rf) cudaFree(a->rf);
   if (a->phys) cudaFree(a->phys);
   if (a->bscr) cudaFree(a->bscr);
   for (int k = 0; k < a->nckpt_cap; k++) {

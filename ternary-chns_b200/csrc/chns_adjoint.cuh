@@ -197,14 +197,43 @@ __global__ void k_adj_tail4(const AdjPar<R> P, const cx<R>* __restrict__ nw, con
   out[3 * ncx + idx] = cscale(mul_mik(a, m.kx), sc);  // conj(i kx) = -i kx
 }
 
+// The forward fields of one right-hand side that its transpose needs, as recorded by
+// the forward step's REC kernels (n x n real fields and F[f(c_t)] in the S layout).
+// Device-resident, so that a captured reversed step reads the record of whichever
+// step it reverses.
+template <class R> struct RecFields {
+  const R *u, *v, *wx, *wy, *ct, *gx, *gy, *mu;  // gx, gy: grad c
+  const cx<R>* ff;
+};
+
+// rf[0], rf[1] from two records laid out as the REC kernels write them: c_t, u, v,
+// wx, wy, cx, cy, mu (n x n each), then F[f(c_t)]
+template <class R>
+__global__ void k_adj_set_rec(RecFields<R>* rf, const R* rec0, const R* rec1, size_t nn) {
+  for (int s = 0; s < 2; s++) {
+    const R* b = s == 0 ? rec0 : rec1;
+    RecFields<R>& r = rf[s];
+    r.ct = b;
+    r.u = b + nn;
+    r.v = b + 2 * nn;
+    r.wx = b + 3 * nn;
+    r.wy = b + 4 * nn;
+    r.gx = b + 5 * nn;
+    r.gy = b + 6 * nn;
+    r.mu = b + 7 * nn;
+    r.ff = reinterpret_cast<const cx<R>*>(b + 8 * nn);
+  }
+}
+
 // mu_bar_hat = T[(w_j / n^2) dfft(mu_bar)]; c_bar += s1 k^2 mu_bar_hat; the
 // spectrum of F[f]'s adjoint, s2 mu_bar_hat - lambda s2 k^2 Nc_bar, scaled
 // n^2 / w_j for F^T; lambda_bar and sigma_bar from the mu terms and from
 // N_c = -F[B] - lambda s2 k^2 F[f] (nonlin.c:240, 251).
 template <class R>
 __global__ void k_adj_mu(const AdjPar<R> P, const cx<R>* __restrict__ mub_hat_raw, const cx<R>* __restrict__ c,
-                         const cx<R>* __restrict__ Ff, const cx<R>* __restrict__ nc, cx<R>* __restrict__ gc,
+                         const RecFields<R>* rf, const cx<R>* __restrict__ nc, cx<R>* __restrict__ gc,
                          cx<R>* __restrict__ fbar_spec, double* acc) {
+  const cx<R>* __restrict__ Ff = rf->ff;
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
   double dl = 0.0, ds = 0.0;
@@ -231,8 +260,10 @@ __global__ void k_adj_mu(const AdjPar<R> P, const cx<R>* __restrict__ mub_hat_ra
 // physical adjoints of the products (nonlin.c:62, 207; surface_tension.c:87-88):
 // mu_bar = Fx_bar cx + Fy_bar cy
 template <class R>
-__global__ void k_adj_mubar(const R* __restrict__ fxb, const R* __restrict__ fyb, const R* __restrict__ cxp,
-                            const R* __restrict__ cyp, R* __restrict__ mub, size_t nn) {
+__global__ void k_adj_mubar(const R* __restrict__ fxb, const R* __restrict__ fyb, const RecFields<R>* rf,
+                            R* __restrict__ mub, size_t nn) {
+  const R* __restrict__ cxp = rf->gx;
+  const R* __restrict__ cyp = rf->gy;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x)
     mub[k] = fxb[k] * cxp[k] + fyb[k] * cyp[k];
 }
@@ -240,20 +271,18 @@ __global__ void k_adj_mubar(const R* __restrict__ fxb, const R* __restrict__ fyb
 // (Ab, Bb, Fxb, Fyb, fb) -> (u_bar, v_bar, wx_bar, wy_bar, ct_bar, cx_bar, cy_bar)
 //   u_bar = Ab wx + Bb cx, v_bar = Ab wy + Bb cy, wx_bar = Ab u, wy_bar = Ab v,
 //   cx_bar = Bb u + Fxb mu, cy_bar = Bb v + Fyb mu, ct_bar = fb f'(ct)
-template <class R> struct PhysFields {
-  R *u, *v, *wx, *wy, *ct, *cx, *cy, *mu;
-};
 template <class R> struct PhysAdj {
   R *ab, *bb, *fxb, *fyb, *fb;         // inputs
   R *ub, *vb, *wxb, *wyb, *ctb, *cxb, *cyb;  // outputs
 };
 template <class R>
-__global__ void k_adj_products(const PhysFields<R> F, const PhysAdj<R> A, size_t nn) {
+__global__ void k_adj_products(const RecFields<R>* rf, const PhysAdj<R> A, size_t nn) {
+  const RecFields<R> F = *rf;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
     const R ab = A.ab[k], bb = A.bb[k], fxb = A.fxb[k], fyb = A.fyb[k], fb = A.fb[k];
     const R u = F.u[k], v = F.v[k], ct = F.ct[k], mu = F.mu[k];
-    A.ub[k] = ab * F.wx[k] + bb * F.cx[k];
-    A.vb[k] = ab * F.wy[k] + bb * F.cy[k];
+    A.ub[k] = ab * F.wx[k] + bb * F.gx[k];
+    A.vb[k] = ab * F.wy[k] + bb * F.gy[k];
     A.wxb[k] = ab * u;
     A.wyb[k] = ab * v;
     A.cxb[k] = bb * u + fxb * mu;

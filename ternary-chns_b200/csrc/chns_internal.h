@@ -77,6 +77,8 @@ struct chns_ctx {
   void* statelo[3]; // CHNS_FP32_STATE64: the low float of the state (S layout): state = state[] + statelo[]
   void* saved[3];
   void* nstar[3];   // when set, stage 2 also stores N(u*) there (adjoint recording)
+  void* rec;        // when set (binary), the stage also records the forward fields its
+                    // adjoint transposes there (chns_kernels.cuh, Bufs::rec)
   void* nw;
   void* g[12];
   void* h[7];

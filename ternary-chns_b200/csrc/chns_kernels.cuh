@@ -80,6 +80,8 @@ template <class R> struct Bufs {
   cx<R>* nw;
   cx<R>* lo[3];  // FP32 contexts with a double-float state: low parts of w, c1, c2 (else null)
   cx<R>* gr;     // (dx c_i, dy c_i) in real space, [field][x-row][y]: written by P2, read by P4
+  R* rec;        // binary REC kernels: the adjoint's record of this right-hand side, n x n real
+                 // fields c_t, u, v, wx, wy, cx, cy, mu, then F[f(c_t)] in the S layout
   cx<R>* g[NG];
   cx<R>* h[NH];
 };
@@ -517,6 +519,16 @@ __device__ __forceinline__ void store_row_pair(const cx<R>* v, cx<R>* __restrict
   }
 }
 
+// REC: x-row xr of recorded real field k (the real or imaginary parts of v)
+template <int N, class R>
+__device__ __forceinline__ void rec_row(R* rec, int k, int xr, const cx<R>* v, bool im, bool live, int t) {
+  constexpr int NT = N / 16;
+  if (!live) return;
+  R* d = rec + (size_t)k * N * N + (size_t)xr * N + t;
+#pragma unroll
+  for (int m = 0; m < 16; m++) d[NT * m] = im ? v[m].y : v[m].x;
+}
+
 template <int N> __device__ __forceinline__ int amask(int t, int m) {
   const int ms = sidx<N>(t + (N / 16) * m);
   return ms < 0 ? -ms : ms;
@@ -742,7 +754,8 @@ __device__ __forceinline__ RowSrc<R> adv_src(const Bufs<R>& B, int it, int i0) {
 
 // GR: the stage keeps grad c_i in real space for P4 (Bufs::gr), which then
 // transforms only mu (the context's choice per grid size, chns_tuned.h)
-template <int N, class R, int GPC, int MODEL, bool JT4 = false, bool GR = false>
+// REC (binary): also store the real fields the discrete adjoint transposes (Bufs::rec)
+template <int N, class R, int GPC, int MODEL, bool JT4 = false, bool GR = false, bool REC = false>
 CHNS_STAGE_KERNEL(N, R, GPC) k_row_adv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS_TMAG_PARAM T) {
   using Sc = AdvSchedule<MODEL>;
   constexpr int NT = N / 16;
@@ -776,8 +789,11 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_row_adv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS
     int stride = 0, off = 0;
     if (it < Sc::PRE) {
       if (MODEL == MODEL_BINARY) {
-        // f(c_t) of x-rows i0, i1 (surface_tension.c:30-31, nonlin.c:225); FP32 from
-        // the deviation c_t - cb (P1 left the mean out; cb from the double k = 0 mode)
+        if constexpr (REC) {
+          rec_row<N>(B.rec, 0, i0, v, false, live, t);
+          rec_row<N>(B.rec, 0, i0 + 1, v, true, live, t);
+        }
+        // f(c_t) of x-rows i0, i1 (surface_tension.c:30-31, nonlin.c:225)
 #pragma unroll
         for (int m = 0; m < 16; m++) v[m] = mk<R>(bulk_f(v[m].x), bulk_f(v[m].y));
         dst = B.h[HF]; stride = N; off = i0;
@@ -809,6 +825,10 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_row_adv(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS
       }
     } else {
       const int q = it - Sc::PRE, h = q / Sc::PER, r = q % Sc::PER;
+      if constexpr (REC && MODEL == MODEL_BINARY) {  // (u, v), (wx, wy), (cx, cy) of x-row i0 + h
+        rec_row<N>(B.rec, 1 + 2 * r, i0 + h, v, false, live, t);
+        rec_row<N>(B.rec, 2 + 2 * r, i0 + h, v, true, live, t);
+      }
       if (r == 0) {
         // (u, v) of x-row i0 + h
 #pragma unroll
@@ -893,7 +913,7 @@ __device__ __forceinline__ RowSrc<R> force_src(const Bufs<R>& B, int it, int i0)
   return RowSrc<R>{B.g[slot], 2 * N, 2 * (i0 + h), 2 * slot};
 }
 
-template <int N, class R, int GPC, int MODEL, bool JT4 = false, bool GR = false>
+template <int N, class R, int GPC, int MODEL, bool JT4 = false, bool GR = false, bool REC = false>
 CHNS_STAGE_KERNEL(N, R, GPC) k_row_force(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CHNS_TMAG_PARAM T) {
   constexpr int NT = N / 16;
   constexpr int NIN = MODEL == MODEL_BINARY ? 3 : 6;      // steps with an input (binary: a last step only stores)
@@ -945,6 +965,10 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_row_force(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P, CH
       // (Fx at HFF, Fy behind it), so the group writes both halves of each 16-byte
       // pair of x-rows at once and P5 reads whole rows.
       if (it == 0) {
+        if constexpr (REC) {
+          rec_row<N>(B.rec, 7, i0, v, false, live, t);
+          rec_row<N>(B.rec, 7, i0 + 1, v, true, live, t);
+        }
 #pragma unroll
         for (int m = 0; m < 16; m++) a[m] = v[m];  // mu_t of x-rows i0, i1
       } else if (it == 1) {
@@ -1090,7 +1114,7 @@ __device__ __forceinline__ cxf split_k0(const double* st, cxf* lo) {
 // float with their low part left at zero.
 // FILT: the context's truncation is SMOOTH_FILTER's (P.filt), a variant of its own
 // so that the sharp cut's kernel carries none of the filter's registers
-template <int N, class R, int GPC, int MODEL, int STAGE, bool S64, bool FILT = false>
+template <int N, class R, int GPC, int MODEL, int STAGE, bool S64, bool FILT = false, bool REC = false>
 CHNS_STAGE_KERNEL(N, R, GPC) k_spec_fwd_c(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
   constexpr int NT = N / 16;
   constexpr int NR = N / 2 + 1;
@@ -1157,6 +1181,8 @@ CHNS_STAGE_KERNEL(N, R, GPC) k_spec_fwd_c(CHNS_BUFS_PARAM B, CHNS_PAR_PARAM P) {
       fft<N, -1>(f, sh, t, TW);
       load_row<N>(c, cst, row, live, t);
     }
+    if constexpr (REC && MODEL == MODEL_BINARY)  // F[f(c_t)] for the adjoint's record
+      store_row<N>(f, reinterpret_cast<cx<R>*>(B.rec + (size_t)8 * N * N), row, live, t);
     if (do_mu) {
       // binary: mu = T[1.5 sigma eps k^2 c + 24 (sigma/eps) F[f]]   (surface_tension.c:45-46)
       // ternary: mu_i = T[F[mu^F_i] + 0.75 gamma_i eps k^2 c_i]     (surface_tension.c:116-128)

@@ -71,8 +71,12 @@ static void launch_stage(const chns_ctx* c, K kern, dim3 grid, dim3 block, size_
 
 // the P3 variant of a context: double-float state (FP32 only) and SMOOTH_FILTER
 template <int N, class R, int GPC, int MODEL, int STAGE>
-static auto spec_fwd_c_kernel(bool s64, bool filt) {
+static auto spec_fwd_c_kernel(bool s64, bool filt, bool rec) {
   constexpr bool F32 = sizeof(R) == 4;
+  if constexpr (MODEL == MODEL_BINARY) {  // the adjoint's recording (sharp cut only)
+    if (rec) return s64 ? k_spec_fwd_c<N, R, GPC, MODEL, STAGE, F32, false, true>
+                        : k_spec_fwd_c<N, R, GPC, MODEL, STAGE, false, false, true>;
+  }
   return s64 ? (filt ? k_spec_fwd_c<N, R, GPC, MODEL, STAGE, F32, true> : k_spec_fwd_c<N, R, GPC, MODEL, STAGE, F32>)
              : (filt ? k_spec_fwd_c<N, R, GPC, MODEL, STAGE, false, true> : k_spec_fwd_c<N, R, GPC, MODEL, STAGE, false>);
 }
@@ -80,16 +84,26 @@ static auto spec_fwd_c_kernel(bool s64, bool filt) {
 // the row kernels of a context: the square-box cut's compile-time tile reads
 // (JT4) and grad c_i kept in real space from P2 for P4 (GR; pure Navier-Stokes has none)
 template <int N, class R, int GPC, int MODEL>
-static auto row_adv_kernel(bool jt4, bool gr) {
+static auto row_adv_kernel(bool jt4, bool gr, bool rec) {
   if constexpr (MODEL == MODEL_NS) {
     return jt4 ? k_row_adv<N, R, GPC, MODEL, true> : k_row_adv<N, R, GPC, MODEL, false>;
   } else {
+    if constexpr (MODEL == MODEL_BINARY) {  // the adjoint's recording
+      if (rec)
+        return jt4 ? (gr ? k_row_adv<N, R, GPC, MODEL, true, true, true> : k_row_adv<N, R, GPC, MODEL, true, false, true>)
+                   : (gr ? k_row_adv<N, R, GPC, MODEL, false, true, true> : k_row_adv<N, R, GPC, MODEL, false, false, true>);
+    }
     return jt4 ? (gr ? k_row_adv<N, R, GPC, MODEL, true, true> : k_row_adv<N, R, GPC, MODEL, true, false>)
                : (gr ? k_row_adv<N, R, GPC, MODEL, false, true> : k_row_adv<N, R, GPC, MODEL, false, false>);
   }
 }
 template <int N, class R, int GPC, int MODEL>
-static auto row_force_kernel(bool jt4, bool gr) {
+static auto row_force_kernel(bool jt4, bool gr, bool rec) {
+  if constexpr (MODEL == MODEL_BINARY) {  // the adjoint's recording
+    if (rec)
+      return jt4 ? (gr ? k_row_force<N, R, GPC, MODEL, true, true, true> : k_row_force<N, R, GPC, MODEL, true, false, true>)
+                 : (gr ? k_row_force<N, R, GPC, MODEL, false, true, true> : k_row_force<N, R, GPC, MODEL, false, false, true>);
+  }
   return jt4 ? (gr ? k_row_force<N, R, GPC, MODEL, true, true> : k_row_force<N, R, GPC, MODEL, true, false>)
              : (gr ? k_row_force<N, R, GPC, MODEL, false, true> : k_row_force<N, R, GPC, MODEL, false, false>);
 }
@@ -134,17 +148,17 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   // square box (jt = N/4) has row kernels whose tile reads are fixed at compile time.
   const bool jt4 = jt == N / 4;
   if (model == CHNS_MODEL_NS) {
-    auto k = row_adv_kernel<N, R, GPC, MODEL_NS>(jt4, c->p4_grad);
+    auto k = row_adv_kernel<N, R, GPC, MODEL_NS>(jt4, c->p4_grad, c->rec != nullptr);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_NS>());
     set_smem(k, sm);
     launch_stage(c, k, pairs, S::THREADS, sm, st, B, P, TG);
   } else if (model == CHNS_MODEL_BINARY) {
-    auto k = row_adv_kernel<N, R, GPC, MODEL_BINARY>(jt4, c->p4_grad);
+    auto k = row_adv_kernel<N, R, GPC, MODEL_BINARY>(jt4, c->p4_grad, c->rec != nullptr);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_BINARY>());
     set_smem(k, sm);
     launch_stage(c, k, pairs, S::THREADS, sm, st, B, P, TG);
   } else {
-    auto k = row_adv_kernel<N, R, GPC, MODEL_TERNARY>(jt4, c->p4_grad);
+    auto k = row_adv_kernel<N, R, GPC, MODEL_TERNARY>(jt4, c->p4_grad, c->rec != nullptr);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_adv_frags<MODEL_TERNARY>());
     set_smem(k, sm);
     launch_stage(c, k, pairs, S::THREADS, sm, st, B, P, TG);
@@ -171,10 +185,11 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
   {
     const bool bin = model == CHNS_MODEL_BINARY;
     const bool filt = c->filt != nullptr;
-    auto k = bin ? (stage == 1 ? spec_fwd_c_kernel<N, R, GPC, MODEL_BINARY, 1>(s64, filt)
-                               : spec_fwd_c_kernel<N, R, GPC, MODEL_BINARY, 2>(s64, filt))
-                 : (stage == 1 ? spec_fwd_c_kernel<N, R, GPC, MODEL_TERNARY, 1>(s64, filt)
-                               : spec_fwd_c_kernel<N, R, GPC, MODEL_TERNARY, 2>(s64, filt));
+    const bool rec = c->rec != nullptr;
+    auto k = bin ? (stage == 1 ? spec_fwd_c_kernel<N, R, GPC, MODEL_BINARY, 1>(s64, filt, rec)
+                               : spec_fwd_c_kernel<N, R, GPC, MODEL_BINARY, 2>(s64, filt, rec))
+                 : (stage == 1 ? spec_fwd_c_kernel<N, R, GPC, MODEL_TERNARY, 1>(s64, filt, rec)
+                               : spec_fwd_c_kernel<N, R, GPC, MODEL_TERNARY, 2>(s64, filt, rec));
     set_smem(k, spec_smem<N, R>(bin));
     launch_stage(c, k, rows_all, S::THREADS, spec_smem<N, R>(bin), st, B, P);
   }
@@ -183,12 +198,12 @@ template <int N, class R> int stage_impl(chns_ctx* c, int stage) {
 
   // P4: surface-tension force
   if (model == CHNS_MODEL_BINARY) {
-    auto k = row_force_kernel<N, R, GPC, MODEL_BINARY>(jt4, c->p4_grad);
+    auto k = row_force_kernel<N, R, GPC, MODEL_BINARY>(jt4, c->p4_grad, c->rec != nullptr);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_force_frags<MODEL_BINARY>());
     set_smem(k, sm);
     launch_stage(c, k, pairs, S::THREADS, sm, st, B, P, TG);
   } else {
-    auto k = row_force_kernel<N, R, GPC, MODEL_TERNARY>(jt4, c->p4_grad);
+    auto k = row_force_kernel<N, R, GPC, MODEL_TERNARY>(jt4, c->p4_grad, c->rec != nullptr);
     const size_t sm = S::TW + loaded_row_smem_bytes<N, R, GPC>(tma, jt, TG.boxr, TG.nbox, row_force_frags<MODEL_TERNARY>());
     set_smem(k, sm);
     launch_stage(c, k, pairs, S::THREADS, sm, st, B, P, TG);

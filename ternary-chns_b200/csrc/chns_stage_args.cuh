@@ -65,6 +65,7 @@ template <class R> Bufs<R> make_bufs(const chns_ctx* c) {
   B.nw = (cx<R>*)c->nw;
   for (int f = 0; f < 3; f++) B.lo[f] = c->st64 ? (cx<R>*)c->statelo[f] : nullptr;
   B.gr = (cx<R>*)c->gradr;
+  B.rec = (R*)c->rec;
   for (int k = 0; k < NG; k++) B.g[k] = (cx<R>*)c->g[k];
   for (int k = 0; k < NH; k++) B.h[k] = (cx<R>*)c->h[k];
   return B;
