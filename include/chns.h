@@ -251,8 +251,11 @@ int chns_read_phase(chns_ctx *ctx, const char *path1, const char *path2);
  * for pure Navier-Stokes); g_params = dJ/d(nu, lambda, sigma) (binary, 3 values;
  * pure Navier-Stokes: nu, 0, 0) or dJ/d(nu, lambda, sigma_12, sigma_13, sigma_23)
  * (ternary, 5 values).  The state is kept every `ckpt` steps and recomputed in
- * between; it is unchanged on return.  CHNS_FP32_STATE64 contexts return
- * CHNS_ERR_UNSUPPORTED. */
+ * between; it is unchanged on return.  The buffers stay in the context: 2 x ckpt
+ * segment slots (one set when two do not fit, else CHNS_ERR_NOMEM) of 26 (binary:
+ * the step's states and right-hand sides, and the forward fields its transpose
+ * reads), 12 (ternary) or 4 (pure Navier-Stokes) fields of n x n/2+1 complex or
+ * n x n real values.  CHNS_FP32_STATE64 contexts return CHNS_ERR_UNSUPPORTED. */
 int chns_adjoint(chns_ctx *ctx, int nsteps, int ckpt, const double *loss_w, double *J, double *g_w,
                  double *g_c, double *g_params, int where);
 
