@@ -109,7 +109,7 @@ constexpr int SSET = 9;                      // spectral fields per set
 enum { SB = 0, SXo = 7, SFFo = 8 };           // batch of 7, scratch, F[f]
 enum {
   SY = 2 * SSET,                             // scratch (f_bar spectrum)
-  SNBW, SNBC,                                // N*_bar
+  SNBW, SNBC,                                // N*_bar (its c part)
   SNBAW, SNBAC,                              // N(u_n)_bar
   SGW, SGC,                                  // running gradient (w_bar, c_bar)
   // current step, in the segment slot layout: u_n, u*, N(u_n), N(u*)
@@ -214,41 +214,42 @@ template <class R> struct Adj {
     c->stream = st;
   }
 
-  // (gw, gc) += J_N(state)^T (nbw, nbc) with the recorded forward fields a->rf[r]
-  // (c_hat of the state: cc); parameter partials into acc[4..6]
-  void transpose_rhs(int r, const cx<R>* cc, const cx<R>* nbw, const cx<R>* nbc, cx<R>* gw, cx<R>* gc) {
+  // the transposed right-hand side at a state from its tail batch (SS(kW, SB), four
+  // spectra of N_bar) to the batch of its seven transformed product adjoints in the
+  // same place, with the recorded forward fields a->rf[r] (c_hat of the state: cc,
+  // N_c_bar: nbc); gc += the mu term; parameter partials into acc[4..6]
+  void rhs_body(int r, const cx<R>* cc, const cx<R>* nbc, cx<R>* gc) {
     const RecFields<R>* rf = static_cast<const RecFields<R>*>(a->rf) + r;
     double* pacc = a->acc + 4;
-    // transposed spectral tail -> A_bar, B_bar, Fx_bar, Fy_bar
-    k_adj_tail4<R><<<blocks_s, 256, 0, st>>>(P, nbw, nbc, SS(kW, SB), ncx);
-    ifft(st, kW, SS(kW, SB), F(PAB), 4);
+    ifft(st, kW, SS(kW, SB), F(PAB), 4);  // A_bar, B_bar, Fx_bar, Fy_bar
     // mu_bar -> c_bar (s1 k^2), f_bar, lambda and sigma partials
     k_adj_mubar<R><<<blocks_p, 256, 0, st>>>(F(PFXB), F(PFYB), rf, F(PUB), nn);
     dfft(st, kW, F(PUB), SS(kW, SXo), 1);
     k_adj_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(kW, SXo), cc, rf, nbc, gc, S(SY), pacc);
     ifft(st, kW, S(SY), F(PFB), 1);
-    // products, then C^T of the seven forward fields
+    // products, then the forward transforms of their adjoints
     PhysAdj<R> pa{F(PAB), F(PBB), F(PFXB), F(PFYB), F(PFB), F(PUB), F(PVB), F(PWXB), F(PWYB), F(PCTB), F(PCXB),
                   F(PCYB)};
     k_adj_products<R><<<blocks_p, 256, 0, st>>>(rf, pa, nn);
     dfft(st, kW, F(PUB), SS(kW, SB), FOP_N);
-    k_adj_acc7<R><<<blocks_s, 256, 0, st>>>(P, SS(kW, SB), gw, gc, ncx);
   }
 
   // one reversed step from the current-step buffer (u_n, u*, N(u_n), N(u*)) with the
   // forward fields recorded for it (a->rf[0] at u*, a->rf[1] at u_n): the transposed
-  // stage 2, right-hand side at u*, stage 1 and right-hand side at u_n
+  // stage 2 with the tail at u*, the right-hand side at u*, its C^T with stage 1 and
+  // the tail at u_n, the right-hand side at u_n and its C^T
   void reverse_step(const R* coef, const double* dcoef, cudaStream_t, int) {
     double* pacc = a->acc + 4;
     cx<R>* gw = S(SGW);
     cx<R>* gc = S(SGC);
     cb = curbase(0);
-    k_adj_etd2<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(cb + 6), S(cb + 7), S(cb + 4), S(cb + 5),
-                                            S(SNBW), S(SNBC), S(SNBAW), S(SNBAC), pacc);
-    transpose_rhs(0, S(cb + 3), S(SNBW), S(SNBC), gw, gc);
-    k_adj_etd1<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(cb + 0), S(cb + 1), S(cb + 4), S(cb + 5),
-                                            S(SNBAW), S(SNBAC), pacc);
-    transpose_rhs(1, S(cb + 1), S(SNBAW), S(SNBAC), gw, gc);
+    k_adj_etd2_tail<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(cb + 6), S(cb + 7), S(cb + 4),
+                                                 S(cb + 5), S(SNBC), S(SNBAW), S(SNBAC), SS(kW, SB), ncx, pacc);
+    rhs_body(0, S(cb + 3), S(SNBC), gc);
+    k_adj_acc7_etd1_tail<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, SS(kW, SB), gw, gc, S(cb + 0), S(cb + 1),
+                                                      S(cb + 4), S(cb + 5), S(SNBAW), S(SNBAC), ncx, pacc);
+    rhs_body(1, S(cb + 1), S(SNBAC), gc);
+    k_adj_acc7<R><<<blocks_s, 256, 0, st>>>(P, SS(kW, SB), gw, gc, ncx);
   }
   void prime(cudaStream_t, int) {}  // the forward fields are recorded, not rebuilt
 };

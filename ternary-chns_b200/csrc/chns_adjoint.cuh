@@ -184,13 +184,9 @@ template <class R> __global__ void k_adj_bulk(const R* __restrict__ x, R* __rest
 // each scaled by n^2 / w_j (the inverse transform divides by n^2).
 // ---------------------------------------------------------------------------
 template <class R>
-__global__ void k_adj_tail4(const AdjPar<R> P, const cx<R>* __restrict__ nw, const cx<R>* __restrict__ nc,
-                            cx<R>* __restrict__ out, size_t ncx) {
-  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  ModeIdx<R> m;
-  if (!mode_of(P, idx, m)) return;
+__device__ __forceinline__ void tail4_at(const AdjPar<R>& P, const ModeIdx<R>& m, cx<R> a, cx<R> b, cx<R>* out,
+                                         size_t ncx, size_t idx) {
   const R sc = (R)((double)P.n * (double)P.n) / m.wj;
-  const cx<R> a = nw[idx], b = nc[idx];
   out[idx] = cscale(a, -sc);
   out[ncx + idx] = cscale(b, -sc);
   out[2 * ncx + idx] = cscale(mul_ik(a, m.ky), sc);   // conj(-i ky) = i ky
@@ -297,11 +293,8 @@ __global__ void k_adj_products(const RecFields<R>* rf, const PhysAdj<R> A, size_
 //   u = T[i ky psi], v = T[-i kx psi], psi = w / k^2; wx = T[i kx w], wy = T[i ky w];
 //   ct = T[c], cx = T[i kx c], cy = T[i ky c]
 template <class R>
-__global__ void k_adj_acc7(const AdjPar<R> P, const cx<R>* __restrict__ xb, cx<R>* __restrict__ gw,
-                           cx<R>* __restrict__ gc, size_t ncx) {
-  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  ModeIdx<R> m;
-  if (!mode_of(P, idx, m) || !m.in) return;
+__device__ __forceinline__ void acc7_at(const AdjPar<R>& P, const ModeIdx<R>& m, const cx<R>* xb, size_t ncx,
+                                        size_t idx, cx<R>& gw, cx<R>& gc) {
   const R sc = m.wj / (R)((double)P.n * (double)P.n);
   cx<R> x[FOP_N];
 #pragma unroll
@@ -314,9 +307,20 @@ __global__ void k_adj_acc7(const AdjPar<R> P, const cx<R>* __restrict__ xb, cx<R
   }
   const cx<R> ax = mul_mik(x[FOP_WX], m.kx), ay = mul_mik(x[FOP_WY], m.ky);
   const cx<R> bx = mul_mik(x[FOP_CX], m.kx), by = mul_mik(x[FOP_CY], m.ky);
-  const cx<R> ow = gw[idx], oc = gc[idx];
-  gw[idx] = mk<R>(ow.x + dw.x + ax.x + ay.x, ow.y + dw.y + ax.y + ay.y);
-  gc[idx] = mk<R>(oc.x + x[FOP_CT].x + bx.x + by.x, oc.y + x[FOP_CT].y + bx.y + by.y);
+  gw = mk<R>(gw.x + dw.x + ax.x + ay.x, gw.y + dw.y + ax.y + ay.y);
+  gc = mk<R>(gc.x + x[FOP_CT].x + bx.x + by.x, gc.y + x[FOP_CT].y + bx.y + by.y);
+}
+
+template <class R>
+__global__ void k_adj_acc7(const AdjPar<R> P, const cx<R>* __restrict__ xb, cx<R>* __restrict__ gw,
+                           cx<R>* __restrict__ gc, size_t ncx) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  ModeIdx<R> m;
+  if (!mode_of(P, idx, m) || !m.in) return;
+  cx<R> w = gw[idx], c = gc[idx];
+  acc7_at(P, m, xb, ncx, idx, w, c);
+  gw[idx] = w;
+  gc[idx] = c;
 }
 
 // ---------------------------------------------------------------------------
@@ -324,14 +328,15 @@ __global__ void k_adj_acc7(const AdjPar<R> P, const cx<R>* __restrict__ xb, cx<R
 // coef [6][nr][nr] (eta_w, z1_w, z2_w, beta_c, z1_c, z2_c); dcoef [9][nr][nr]:
 // d(eta_w, z1_w, z2_w)/d nu, d(beta_c, z1_c, z2_c)/d lambda, ... / d sigma.
 // ---------------------------------------------------------------------------
+// stage 2 (u1 = u* + z2 (N* - N)): N*_bar = z2 u1_bar (its c part kept in nbs_c, the
+// transposed tail of the right-hand side at u* into `out`), N_bar = -z2 u1_bar
 template <class R>
-__global__ void k_adj_etd2(const AdjPar<R> P, const R* __restrict__ coef, const double* __restrict__ dcoef,
-                           const cx<R>* __restrict__ gw, const cx<R>* __restrict__ gc,
-                           const cx<R>* __restrict__ nsw, const cx<R>* __restrict__ nsc,
-                           const cx<R>* __restrict__ nw, const cx<R>* __restrict__ nc,
-                           cx<R>* __restrict__ nbs_w, cx<R>* __restrict__ nbs_c,
-                           cx<R>* __restrict__ nba_w, cx<R>* __restrict__ nba_c, double* acc) {
-  // stage 2: u1 = u* + z2 (N* - N):  N*_bar = z2 u1_bar, N_bar (partial) = -z2 u1_bar
+__global__ void k_adj_etd2_tail(const AdjPar<R> P, const R* __restrict__ coef, const double* __restrict__ dcoef,
+                                const cx<R>* __restrict__ gw, const cx<R>* __restrict__ gc,
+                                const cx<R>* __restrict__ nsw, const cx<R>* __restrict__ nsc,
+                                const cx<R>* __restrict__ nw, const cx<R>* __restrict__ nc,
+                                cx<R>* __restrict__ nbs_c, cx<R>* __restrict__ nba_w, cx<R>* __restrict__ nba_c,
+                                cx<R>* __restrict__ out, size_t ncx, double* acc) {
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
   double dnu = 0.0, dl = 0.0, dsg = 0.0;
@@ -340,10 +345,11 @@ __global__ void k_adj_etd2(const AdjPar<R> P, const R* __restrict__ coef, const 
     const size_t t = (size_t)nr * nr, o = (size_t)m.row * nr + m.am;
     const R z2w = coef[2 * t + o], z2c = coef[5 * t + o];
     const cx<R> bw = gw[idx], bc = gc[idx];
-    nbs_w[idx] = cscale(bw, z2w);
-    nbs_c[idx] = cscale(bc, z2c);
+    const cx<R> sw = cscale(bw, z2w), sc = cscale(bc, z2c);
+    nbs_c[idx] = sc;
     nba_w[idx] = cscale(bw, -z2w);
     nba_c[idx] = cscale(bc, -z2c);
+    tail4_at(P, m, sw, sc, out, ncx, idx);
     const cx<R> dw = nsw[idx] - nw[idx], dc = nsc[idx] - nc[idx];
     dnu = dcoef[2 * t + o] * rdot(bw, dw);
     dl = dcoef[5 * t + o] * rdot(bc, dc);
@@ -352,12 +358,17 @@ __global__ void k_adj_etd2(const AdjPar<R> P, const R* __restrict__ coef, const 
   block_acc3(dnu, dl, dsg, acc);
 }
 
+// C^T of the right-hand side at u* (batch xb: its seven transformed product
+// adjoints) into u*_bar = (gw, gc); stage 1 (u* = e u + z1 N(u)): u_bar = e u*_bar,
+// N_bar += z1 u*_bar (its c part kept in nbc); the transposed tail of the right-hand
+// side at u_n into xb (each thread reads its seven entries before writing four)
 template <class R>
-__global__ void k_adj_etd1(const AdjPar<R> P, const R* __restrict__ coef, const double* __restrict__ dcoef,
-                           cx<R>* __restrict__ gw, cx<R>* __restrict__ gc, const cx<R>* __restrict__ uw,
-                           const cx<R>* __restrict__ uc, const cx<R>* __restrict__ nw, const cx<R>* __restrict__ nc,
-                           cx<R>* __restrict__ nbw, cx<R>* __restrict__ nbc, double* acc) {
-  // stage 1: u* = e u + z1 N(u):  u_bar = e u*_bar, N_bar += z1 u*_bar
+__global__ void k_adj_acc7_etd1_tail(const AdjPar<R> P, const R* __restrict__ coef,
+                                     const double* __restrict__ dcoef, cx<R>* xb, cx<R>* __restrict__ gw,
+                                     cx<R>* __restrict__ gc, const cx<R>* __restrict__ uw,
+                                     const cx<R>* __restrict__ uc, const cx<R>* __restrict__ nw,
+                                     const cx<R>* __restrict__ nc, const cx<R>* __restrict__ nbw,
+                                     cx<R>* __restrict__ nbc, size_t ncx, double* acc) {
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
   double dnu = 0.0, dl = 0.0, dsg = 0.0;
@@ -365,12 +376,14 @@ __global__ void k_adj_etd1(const AdjPar<R> P, const R* __restrict__ coef, const 
     const int nr = P.n / 2 + 1;
     const size_t t = (size_t)nr * nr, o = (size_t)m.row * nr + m.am;
     const R ew = coef[0 * t + o], z1w = coef[1 * t + o], ec = coef[3 * t + o], z1c = coef[4 * t + o];
-    const cx<R> bw = gw[idx], bc = gc[idx];
+    cx<R> bw = gw[idx], bc = gc[idx];
+    if (m.in) acc7_at(P, m, xb, ncx, idx, bw, bc);
     const cx<R> a = nbw[idx], b = nbc[idx];
-    nbw[idx] = mk<R>(a.x + z1w * bw.x, a.y + z1w * bw.y);
-    nbc[idx] = mk<R>(b.x + z1c * bc.x, b.y + z1c * bc.y);
+    const cx<R> na = mk<R>(a.x + z1w * bw.x, a.y + z1w * bw.y), nb = mk<R>(b.x + z1c * bc.x, b.y + z1c * bc.y);
+    nbc[idx] = nb;
     gw[idx] = cscale(bw, ew);
     gc[idx] = cscale(bc, ec);
+    tail4_at(P, m, na, nb, xb, ncx, idx);
     dnu = dcoef[0 * t + o] * rdot(bw, uw[idx]) + dcoef[1 * t + o] * rdot(bw, nw[idx]);
     dl = dcoef[3 * t + o] * rdot(bc, uc[idx]) + dcoef[4 * t + o] * rdot(bc, nc[idx]);
     dsg = dcoef[6 * t + o] * rdot(bc, uc[idx]) + dcoef[7 * t + o] * rdot(bc, nc[idx]);
