@@ -102,9 +102,9 @@ struct chns_adj {
 namespace {
 
 // Binary buffers: two field sets of a spectral batch, scratch and F[f] and of
-// physical fields (set 0: the loss; set 1: the transposes' work buffers; the
-// transposes read the forward fields the forward step recorded), the named
-// spectral fields and one current-step buffer.
+// physical fields (set 0: the loss; set 1: the transposes' work buffers) and the
+// named spectral fields; a reversed step reads its states and the forward fields
+// the forward step recorded in its segment slot, through the table RecStep.
 constexpr int SSET = 9;                      // spectral fields per set
 enum { SB = 0, SXo = 7, SFFo = 8 };           // batch of 7, scratch, F[f]
 enum {
@@ -112,8 +112,6 @@ enum {
   SNBW, SNBC,                                // N*_bar (its c part)
   SNBAW, SNBAC,                              // N(u_n)_bar
   SGW, SGC,                                  // running gradient (w_bar, c_bar)
-  // current step, in the segment slot layout: u_n, u*, N(u_n), N(u*)
-  CUW, CUC, CSW, CSC, CNW, CNC, CXW, CXC,
   NSPEC
 };
 constexpr int PSET = 9;                                    // physical fields per set
@@ -138,8 +136,6 @@ template <class R> struct Adj {
   size_t ncx, nn;
   int blocks_s, blocks_p;
 
-  int cb = CUW;  // current-step buffer of the step being reversed
-  int curbase(int) const { return CUW; }
   cx<R>* grad(int f) const { return S(SGW + f); }
   void setup() {
     const chns_params& p = c->p;
@@ -214,41 +210,40 @@ template <class R> struct Adj {
     c->stream = st;
   }
 
-  // the transposed right-hand side at a state from its tail batch (SS(kW, SB), four
-  // spectra of N_bar) to the batch of its seven transformed product adjoints in the
-  // same place, with the recorded forward fields a->rf[r] (c_hat of the state: cc,
-  // N_c_bar: nbc); gc += the mu term; parameter partials into acc[4..6]
-  void rhs_body(int r, const cx<R>* cc, const cx<R>* nbc, cx<R>* gc) {
-    const RecFields<R>* rf = static_cast<const RecFields<R>*>(a->rf) + r;
+  RecStep<R>* table() const { return static_cast<RecStep<R>*>(a->rf); }
+
+  // the transposed right-hand side r (0: at u*, 1: at u_n) from its tail batch
+  // (SS(kW, SB), four spectra of N_bar) to the batch of its seven transformed product
+  // adjoints in the same place, with the step's record (N_c_bar: nbc); gc += the mu
+  // term; parameter partials into acc[4..6]
+  void rhs_body(int r, const cx<R>* nbc, cx<R>* gc) {
+    const RecFields<R>* rf = &table()->rhs[r];
     double* pacc = a->acc + 4;
+    const void* in[5] = {F(PAB), F(PBB), F(PFXB), F(PFYB), F(PFB)};
     ifft(st, kW, SS(kW, SB), F(PAB), 4);  // A_bar, B_bar, Fx_bar, Fy_bar
-    // mu_bar -> c_bar (s1 k^2), f_bar, lambda and sigma partials
-    k_adj_mubar<R><<<blocks_p, 256, 0, st>>>(F(PFXB), F(PFYB), rf, F(PUB), nn);
-    dfft(st, kW, F(PUB), SS(kW, SXo), 1);
-    k_adj_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(kW, SXo), cc, rf, nbc, gc, S(SY), pacc);
+    // mu_bar (formed in the transform's first pass) -> c_bar (s1 k^2), f_bar, lambda
+    // and sigma partials
+    c->L->adjprod(c, rf, in, 7, 1, SS(kW, SXo), ncx, scratch(kW));
+    k_adj_mu<R><<<blocks_s, 256, 0, st>>>(P, SS(kW, SXo), rf, nbc, gc, S(SY), pacc);
     ifft(st, kW, S(SY), F(PFB), 1);
-    // products, then the forward transforms of their adjoints
-    PhysAdj<R> pa{F(PAB), F(PBB), F(PFXB), F(PFYB), F(PFB), F(PUB), F(PVB), F(PWXB), F(PWYB), F(PCTB), F(PCXB),
-                  F(PCYB)};
-    k_adj_products<R><<<blocks_p, 256, 0, st>>>(rf, pa, nn);
-    dfft(st, kW, F(PUB), SS(kW, SB), FOP_N);
+    // the seven product adjoints, formed in the first pass of their forward transforms
+    c->L->adjprod(c, rf, in, 0, FOP_N, SS(kW, SB), ncx, scratch(kW));
   }
 
-  // one reversed step from the current-step buffer (u_n, u*, N(u_n), N(u*)) with the
-  // forward fields recorded for it (a->rf[0] at u*, a->rf[1] at u_n): the transposed
-  // stage 2 with the tail at u*, the right-hand side at u*, its C^T with stage 1 and
-  // the tail at u_n, the right-hand side at u_n and its C^T
+  // one reversed step from the step's record (table(): its states u_n, u*, N(u_n),
+  // N(u*) and forward fields): the transposed stage 2 with the tail at u*, the
+  // right-hand side at u*, its C^T with stage 1 and the tail at u_n, the right-hand
+  // side at u_n and its C^T
   void reverse_step(const R* coef, const double* dcoef, cudaStream_t, int) {
     double* pacc = a->acc + 4;
     cx<R>* gw = S(SGW);
     cx<R>* gc = S(SGC);
-    cb = curbase(0);
-    k_adj_etd2_tail<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, S(cb + 6), S(cb + 7), S(cb + 4),
-                                                 S(cb + 5), S(SNBC), S(SNBAW), S(SNBAC), SS(kW, SB), ncx, pacc);
-    rhs_body(0, S(cb + 3), S(SNBC), gc);
-    k_adj_acc7_etd1_tail<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, SS(kW, SB), gw, gc, S(cb + 0), S(cb + 1),
-                                                      S(cb + 4), S(cb + 5), S(SNBAW), S(SNBAC), ncx, pacc);
-    rhs_body(1, S(cb + 1), S(SNBAC), gc);
+    k_adj_etd2_tail<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, gw, gc, table(), S(SNBC), S(SNBAW), S(SNBAC),
+                                                 SS(kW, SB), ncx, pacc);
+    rhs_body(0, S(SNBC), gc);
+    k_adj_acc7_etd1_tail<R><<<blocks_s, 256, 0, st>>>(P, coef, dcoef, SS(kW, SB), gw, gc, table(), S(SNBAW),
+                                                      S(SNBAC), ncx, pacc);
+    rhs_body(1, S(SNBAC), gc);
     k_adj_acc7<R><<<blocks_s, 256, 0, st>>>(P, SS(kW, SB), gw, gc, ncx);
   }
   void prime(cudaStream_t, int) {}  // the forward fields are recorded, not rebuilt
@@ -665,7 +660,7 @@ template <class A> int adj_alloc(chns_ctx* c, int seglen, int nckpt) {
     if (cudaMalloc(&a->phys, A::NPHYS_ALL * nn * c->rsz) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMalloc(&a->bscr, (size_t)A::NSCR * A::NBSCR * fbytes) != cudaSuccess) return CHNS_ERR_NOMEM;
     if (cudaMalloc((void**)&a->acc, (kAcc + 4 * kLossBlocks) * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
-    if (cudaMalloc(&a->rf, 2 * sizeof(RecFields<double>)) != cudaSuccess) return CHNS_ERR_NOMEM;
+    if (cudaMalloc(&a->rf, sizeof(RecStep<double>)) != cudaSuccess) return CHNS_ERR_NOMEM;
     std::vector<double> d;
     A::dcoef_tables(c, d);
     if (cudaMalloc(&a->dcoef, d.size() * sizeof(double)) != cudaSuccess) return CHNS_ERR_NOMEM;
@@ -802,19 +797,20 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
     ACK(cudaEventRecord(a->ev_ready[b], side));
     return CHNS_OK;
   };
-  // Steps alternate between two current-step buffers: while step k (buffer k & 1) is
-  // reversed, step k - 1 is already in the other buffer and its forward fields are
-  // built on the graph's parallel branch, so no reversed step waits for its own.
+  // Binary: the table is pointed at step k's slot and the one graph runs.  Ternary and
+  // pure Navier-Stokes: steps alternate between two current-step buffers; while step k
+  // (buffer k & 1) is reversed, step k - 1 is already in the other buffer and its
+  // forward fields are built on the graph's parallel branch, so no reversed step waits
+  // for its own.
   auto reverse = [&](int s) -> int {
     const int b = s % nbuf, len = (s * ckpt + ckpt <= nsteps) ? ckpt : nsteps - s * ckpt;
     if (s != nseg - 1) ACK(cudaStreamWaitEvent(st, a->ev_ready[b], 0));
     auto slot_of = [&](int k) { return segbase + ((size_t)b * ckpt + k) * slot; };
-    if (A::REC) {  // one current-step buffer; the step's forward fields were recorded with it
+    if constexpr (A::REC) {  // the reversed step reads the slot through the table
       for (int k = len - 1; k >= 0; k--) {
         char* sk = slot_of(k);
-        ACK(cudaMemcpyAsync(ad.S(ad.curbase(0)), sk, cur, cudaMemcpyDeviceToDevice, st));
-        k_adj_set_rec<R><<<1, 1, 0, st>>>(static_cast<RecFields<R>*>(a->rf), (const R*)(sk + cur + recb),
-                                          (const R*)(sk + cur), a->nn);
+        k_adj_set_rec<R><<<1, 1, 0, st>>>(static_cast<RecStep<R>*>(a->rf), (const cx<R>*)sk, ad.ncx,
+                                          (const R*)(sk + cur + recb), (const R*)(sk + cur), a->nn);
         if (a->rev[0]) {
           ACK(cudaGraphLaunch(a->rev[0], st));
         } else {
@@ -823,22 +819,23 @@ int adjoint_impl(chns_ctx* c, int nsteps, int ckpt, const double* lw, double* J,
       }
       ACK(cudaEventRecord(a->ev_free[b], st));
       return CHNS_OK;
-    }
-    const int p0 = (len - 1) & 1;
-    ACK(cudaMemcpyAsync(ad.S(ad.curbase(p0)), slot_of(len - 1), cur, cudaMemcpyDeviceToDevice, st));
-    ad.prime(st, p0);
-    for (int k = len - 1; k >= 0; k--) {
-      const int par = k & 1;
-      if (k > 0)
-        ACK(cudaMemcpyAsync(ad.S(ad.curbase(1 - par)), slot_of(k - 1), cur, cudaMemcpyDeviceToDevice, st));
-      if (a->rev[par]) {
-        ACK(cudaGraphLaunch(a->rev[par], st));
-      } else {
-        ad.reverse_step(coef, dcoef, nullptr, par);
+    } else {
+      const int p0 = (len - 1) & 1;
+      ACK(cudaMemcpyAsync(ad.S(ad.curbase(p0)), slot_of(len - 1), cur, cudaMemcpyDeviceToDevice, st));
+      ad.prime(st, p0);
+      for (int k = len - 1; k >= 0; k--) {
+        const int par = k & 1;
+        if (k > 0)
+          ACK(cudaMemcpyAsync(ad.S(ad.curbase(1 - par)), slot_of(k - 1), cur, cudaMemcpyDeviceToDevice, st));
+        if (a->rev[par]) {
+          ACK(cudaGraphLaunch(a->rev[par], st));
+        } else {
+          ad.reverse_step(coef, dcoef, nullptr, par);
+        }
       }
+      ACK(cudaEventRecord(a->ev_free[b], st));
+      return CHNS_OK;
     }
-    ACK(cudaEventRecord(a->ev_free[b], st));
-    return CHNS_OK;
   };
   for (int s = nseg - 1; s >= 0; s--) {
     if (nbuf == 2) {

@@ -14,6 +14,7 @@
 #pragma once
 
 #include "chns_kernels.cuh"
+#include "chns_adj_rows.cuh"
 
 namespace chns {
 
@@ -193,22 +194,15 @@ __device__ __forceinline__ void tail4_at(const AdjPar<R>& P, const ModeIdx<R>& m
   out[3 * ncx + idx] = cscale(mul_mik(a, m.kx), sc);  // conj(i kx) = -i kx
 }
 
-// The forward fields of one right-hand side that its transpose needs, as recorded by
-// the forward step's REC kernels (n x n real fields and F[f(c_t)] in the S layout).
-// Device-resident, so that a captured reversed step reads the record of whichever
-// step it reverses.
-template <class R> struct RecFields {
-  const R *u, *v, *wx, *wy, *ct, *gx, *gy, *mu;  // gx, gy: grad c
-  const cx<R>* ff;
-};
-
-// rf[0], rf[1] from two records laid out as the REC kernels write them: c_t, u, v,
-// wx, wy, cx, cy, mu (n x n each), then F[f(c_t)]
+// the record table of one step from its segment slot (8 S-layout state fields at
+// `state`, ncx complex each) and its two records, laid out as the REC kernels write
+// them: c_t, u, v, wx, wy, cx, cy, mu (n x n each), then F[f(c_t)]
 template <class R>
-__global__ void k_adj_set_rec(RecFields<R>* rf, const R* rec0, const R* rec1, size_t nn) {
+__global__ void k_adj_set_rec(RecStep<R>* t, const cx<R>* state, size_t ncx, const R* rec_us, const R* rec_un,
+                              size_t nn) {
   for (int s = 0; s < 2; s++) {
-    const R* b = s == 0 ? rec0 : rec1;
-    RecFields<R>& r = rf[s];
+    const R* b = s == 0 ? rec_us : rec_un;
+    RecFields<R>& r = t->rhs[s];
     r.ct = b;
     r.u = b + nn;
     r.v = b + 2 * nn;
@@ -218,7 +212,9 @@ __global__ void k_adj_set_rec(RecFields<R>* rf, const R* rec0, const R* rec1, si
     r.gy = b + 6 * nn;
     r.mu = b + 7 * nn;
     r.ff = reinterpret_cast<const cx<R>*>(b + 8 * nn);
+    r.cc = state + (s == 0 ? 3 : 1) * ncx;  // c_hat of u*, of u_n
   }
+  for (int f = 0; f < 8; f++) t->f[f] = state + f * ncx;
 }
 
 // mu_bar_hat = T[(w_j / n^2) dfft(mu_bar)]; c_bar += s1 k^2 mu_bar_hat; the
@@ -226,10 +222,11 @@ __global__ void k_adj_set_rec(RecFields<R>* rf, const R* rec0, const R* rec1, si
 // n^2 / w_j for F^T; lambda_bar and sigma_bar from the mu terms and from
 // N_c = -F[B] - lambda s2 k^2 F[f] (nonlin.c:240, 251).
 template <class R>
-__global__ void k_adj_mu(const AdjPar<R> P, const cx<R>* __restrict__ mub_hat_raw, const cx<R>* __restrict__ c,
-                         const RecFields<R>* rf, const cx<R>* __restrict__ nc, cx<R>* __restrict__ gc,
-                         cx<R>* __restrict__ fbar_spec, double* acc) {
+__global__ void k_adj_mu(const AdjPar<R> P, const cx<R>* __restrict__ mub_hat_raw, const RecFields<R>* rf,
+                         const cx<R>* __restrict__ nc, cx<R>* __restrict__ gc, cx<R>* __restrict__ fbar_spec,
+                         double* acc) {
   const cx<R>* __restrict__ Ff = rf->ff;
+  const cx<R>* __restrict__ c = rf->cc;
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
   double dl = 0.0, ds = 0.0;
@@ -251,40 +248,6 @@ __global__ void k_adj_mu(const AdjPar<R> P, const cx<R>* __restrict__ mub_hat_ra
     fbar_spec[idx] = cscale(fb, n2 / m.wj);
   }
   block_acc3(0.0, dl, ds, acc);
-}
-
-// physical adjoints of the products (nonlin.c:62, 207; surface_tension.c:87-88):
-// mu_bar = Fx_bar cx + Fy_bar cy
-template <class R>
-__global__ void k_adj_mubar(const R* __restrict__ fxb, const R* __restrict__ fyb, const RecFields<R>* rf,
-                            R* __restrict__ mub, size_t nn) {
-  const R* __restrict__ cxp = rf->gx;
-  const R* __restrict__ cyp = rf->gy;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x)
-    mub[k] = fxb[k] * cxp[k] + fyb[k] * cyp[k];
-}
-
-// (Ab, Bb, Fxb, Fyb, fb) -> (u_bar, v_bar, wx_bar, wy_bar, ct_bar, cx_bar, cy_bar)
-//   u_bar = Ab wx + Bb cx, v_bar = Ab wy + Bb cy, wx_bar = Ab u, wy_bar = Ab v,
-//   cx_bar = Bb u + Fxb mu, cy_bar = Bb v + Fyb mu, ct_bar = fb f'(ct)
-template <class R> struct PhysAdj {
-  R *ab, *bb, *fxb, *fyb, *fb;         // inputs
-  R *ub, *vb, *wxb, *wyb, *ctb, *cxb, *cyb;  // outputs
-};
-template <class R>
-__global__ void k_adj_products(const RecFields<R>* rf, const PhysAdj<R> A, size_t nn) {
-  const RecFields<R> F = *rf;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
-    const R ab = A.ab[k], bb = A.bb[k], fxb = A.fxb[k], fyb = A.fyb[k], fb = A.fb[k];
-    const R u = F.u[k], v = F.v[k], ct = F.ct[k], mu = F.mu[k];
-    A.ub[k] = ab * F.wx[k] + bb * F.gx[k];
-    A.vb[k] = ab * F.wy[k] + bb * F.gy[k];
-    A.wxb[k] = ab * u;
-    A.wyb[k] = ab * v;
-    A.cxb[k] = bb * u + fxb * mu;
-    A.cyb[k] = bb * v + fyb * mu;
-    A.ctb[k] = fb * ((R)1 - (R)6 * ct + (R)6 * ct * ct);
-  }
 }
 
 // accumulation of C^T(x_bar) = (w_j / n^2) dfft(x_bar) through the multipliers
@@ -333,10 +296,13 @@ __global__ void k_adj_acc7(const AdjPar<R> P, const cx<R>* __restrict__ xb, cx<R
 template <class R>
 __global__ void k_adj_etd2_tail(const AdjPar<R> P, const R* __restrict__ coef, const double* __restrict__ dcoef,
                                 const cx<R>* __restrict__ gw, const cx<R>* __restrict__ gc,
-                                const cx<R>* __restrict__ nsw, const cx<R>* __restrict__ nsc,
-                                const cx<R>* __restrict__ nw, const cx<R>* __restrict__ nc,
-                                cx<R>* __restrict__ nbs_c, cx<R>* __restrict__ nba_w, cx<R>* __restrict__ nba_c,
-                                cx<R>* __restrict__ out, size_t ncx, double* acc) {
+                                const RecStep<R>* __restrict__ rs, cx<R>* __restrict__ nbs_c,
+                                cx<R>* __restrict__ nba_w, cx<R>* __restrict__ nba_c, cx<R>* __restrict__ out,
+                                size_t ncx, double* acc) {
+  const cx<R>* __restrict__ nw = rs->f[4];
+  const cx<R>* __restrict__ nc = rs->f[5];
+  const cx<R>* __restrict__ nsw = rs->f[6];
+  const cx<R>* __restrict__ nsc = rs->f[7];
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
   double dnu = 0.0, dl = 0.0, dsg = 0.0;
@@ -365,10 +331,13 @@ __global__ void k_adj_etd2_tail(const AdjPar<R> P, const R* __restrict__ coef, c
 template <class R>
 __global__ void k_adj_acc7_etd1_tail(const AdjPar<R> P, const R* __restrict__ coef,
                                      const double* __restrict__ dcoef, cx<R>* xb, cx<R>* __restrict__ gw,
-                                     cx<R>* __restrict__ gc, const cx<R>* __restrict__ uw,
-                                     const cx<R>* __restrict__ uc, const cx<R>* __restrict__ nw,
-                                     const cx<R>* __restrict__ nc, const cx<R>* __restrict__ nbw,
-                                     cx<R>* __restrict__ nbc, size_t ncx, double* acc) {
+                                     cx<R>* __restrict__ gc, const RecStep<R>* __restrict__ rs,
+                                     const cx<R>* __restrict__ nbw, cx<R>* __restrict__ nbc, size_t ncx,
+                                     double* acc) {
+  const cx<R>* __restrict__ uw = rs->f[0];
+  const cx<R>* __restrict__ uc = rs->f[1];
+  const cx<R>* __restrict__ nw = rs->f[4];
+  const cx<R>* __restrict__ nc = rs->f[5];
   const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   ModeIdx<R> m;
   double dnu = 0.0, dl = 0.0, dsg = 0.0;

@@ -52,6 +52,11 @@ struct Launchers {
   // (complex elements); scratch holds nb n x (n/2+1) complex fields
   int (*dfftb)(chns_ctx* c, const void* real, size_t rs, void* s, size_t ss, int nb, void* scratch);
   int (*ifftb)(chns_ctx* c, const void* s, size_t ss, void* real, size_t rs, int nb, void* scratch);
+  // binary adjoint: product adjoints b0 .. b0 + nb - 1 (chns_adj_rows.cuh) formed from the
+  // device record table rf (RecFields) and the physical adjoints in[0..4] (Ab, Bb, Fxb,
+  // Fyb, fb) and transformed forward into s + b ss (S layout)
+  int (*adjprod)(chns_ctx* c, const void* rf, const void* const* in, int b0, int nb, void* s, size_t ss,
+                 void* scratch);
   // the largest dynamic shared memory a step kernel of the context needs (bytes)
   size_t (*step_smem)(const chns_ctx* c);
 };

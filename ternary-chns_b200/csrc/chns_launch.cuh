@@ -7,6 +7,7 @@
 #include "chns_tuned.h"
 #include "chns_diag.cuh"
 #include "chns_stage_args.cuh"
+#include "chns_adj_rows.cuh"
 
 namespace chns {
 
@@ -297,6 +298,22 @@ template <int N, class R> int ifftb_impl(chns_ctx* c, const void* s, size_t ss, 
   return 2;
 }
 
+template <int N, class R> int adjprod_impl(chns_ctx* c, const void* rf, const void* const* in, int b0, int nb,
+                                           void* s, size_t ss, void* scratch) {
+  using S = Sizes<N, R>;
+  constexpr size_t HS = (size_t)N * (N / 2 + 1);
+  const AdjIn<R> A{(const R*)in[0], (const R*)in[1], (const R*)in[2], (const R*)in[3], (const R*)in[4]};
+  auto k1 = k_adj_prod_r2c<N, R, S::GPC>;
+  set_smem(k1, S::FFT_SMEM);
+  k1<<<dim3(S::grid_rows(N / 2), nb), S::THREADS, S::FFT_SMEM, c->stream>>>((const RecFields<R>*)rf, A, b0,
+                                                                             (cx<R>*)scratch, (const cx<R>*)c->tw, HS);
+  auto k2 = k_col_plain<N, R, S::GPC, -1>;
+  set_smem(k2, S::FFT_SMEM);
+  k2<<<dim3(S::grid_rows(N / 2 + 1), nb), S::THREADS, S::FFT_SMEM, c->stream>>>(
+      (const cx<R>*)scratch, (cx<R>*)s, N / 2 + 1, (R)1, (const cx<R>*)c->tw, HS, ss);
+  return 2;
+}
+
 template <int N, class R> int dfft_impl(chns_ctx* c, const void* real, void* s) {
   return dfftb_impl<N, R>(c, real, 0, s, 0, 1, c->h[HAB]);
 }
@@ -357,7 +374,7 @@ template <int N, class R> const Launchers* make_launchers() {
   static const Launchers L = {stage_impl<N, R>,     truncate_impl<N, R>, dfft_impl<N, R>,
                               ifft_impl<N, R>,      from_fftw_impl<N, R>, to_fftw_impl<N, R>,
                               diag_impl<N, R>,      dfftb_impl<N, R>,     ifftb_impl<N, R>,
-                              step_smem_impl<N, R>};
+                              adjprod_impl<N, R>,   step_smem_impl<N, R>};
   return &L;
 }
 
