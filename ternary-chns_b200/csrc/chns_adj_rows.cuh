@@ -39,21 +39,31 @@ template <class R> struct AdjIn {
   const R *ab, *bb, *fxb, *fyb, *fb;
 };
 
-// product adjoint b (0..6: u, v, wx, wy, ct, cx, cy; 7: mu_bar) at point k
-template <class R>
-__device__ __forceinline__ R adj_product(int b, const RecFields<R>& F, const AdjIn<R>& A, size_t k) {
-  switch (b) {
-    case 0: return A.ab[k] * F.wx[k] + A.bb[k] * F.gx[k];
-    case 1: return A.ab[k] * F.wy[k] + A.bb[k] * F.gy[k];
-    case 2: return A.ab[k] * F.u[k];
-    case 3: return A.ab[k] * F.v[k];
-    case 4: {
-      const R ct = F.ct[k];
-      return A.fb[k] * ((R)1 - (R)6 * ct + (R)6 * ct * ct);
-    }
-    case 5: return A.bb[k] * F.u[k] + A.fxb[k] * F.mu[k];
-    case 6: return A.bb[k] * F.v[k] + A.fyb[k] * F.mu[k];
-    default: return A.fxb[k] * F.gx[k] + A.fyb[k] * F.gy[k];
+// product adjoint B (0..6: u, v, wx, wy, ct, cx, cy; 7: mu_bar) at point k
+template <int B, class R>
+__device__ __forceinline__ R adj_product(const RecFields<R>& F, const AdjIn<R>& A, size_t k) {
+  if constexpr (B == 0) return A.ab[k] * F.wx[k] + A.bb[k] * F.gx[k];
+  if constexpr (B == 1) return A.ab[k] * F.wy[k] + A.bb[k] * F.gy[k];
+  if constexpr (B == 2) return A.ab[k] * F.u[k];
+  if constexpr (B == 3) return A.ab[k] * F.v[k];
+  if constexpr (B == 4) {
+    const R ct = F.ct[k];
+    return A.fb[k] * ((R)1 - (R)6 * ct + (R)6 * ct * ct);
+  }
+  if constexpr (B == 5) return A.bb[k] * F.u[k] + A.fxb[k] * F.mu[k];
+  if constexpr (B == 6) return A.bb[k] * F.v[k] + A.fyb[k] * F.mu[k];
+  if constexpr (B == 7) return A.fxb[k] * F.gx[k] + A.fyb[k] * F.gy[k];
+}
+
+// x-rows i0, i0 + 1 of product adjoint B as the 16 complex values of thread t
+template <int N, int B, class R>
+__device__ __forceinline__ void adj_product_rows(cx<R>* v, const RecFields<R>& F, const AdjIn<R>& A, int i0,
+                                                 bool live, int t) {
+  constexpr int NT = N / 16;
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    const size_t k = (size_t)i0 * N + t + NT * m;
+    v[m] = live ? mk<R>(adj_product<B>(F, A, k), adj_product<B>(F, A, k + N)) : czero<R>();
   }
 }
 
@@ -76,10 +86,15 @@ __global__ void __launch_bounds__(GPC * (N / 16))
   const int i0 = 2 * pair;
   const RecFields<R> F = *rf;
   cx<R> v[16];
-#pragma unroll
-  for (int m = 0; m < 16; m++) {
-    const size_t k = (size_t)i0 * N + t + NT * m;
-    v[m] = live ? mk<R>(adj_product(b, F, A, k), adj_product(b, F, A, k + N)) : czero<R>();
+  switch (b) {  // uniform over the block
+    case 0: adj_product_rows<N, 0>(v, F, A, i0, live, t); break;
+    case 1: adj_product_rows<N, 1>(v, F, A, i0, live, t); break;
+    case 2: adj_product_rows<N, 2>(v, F, A, i0, live, t); break;
+    case 3: adj_product_rows<N, 3>(v, F, A, i0, live, t); break;
+    case 4: adj_product_rows<N, 4>(v, F, A, i0, live, t); break;
+    case 5: adj_product_rows<N, 5>(v, F, A, i0, live, t); break;
+    case 6: adj_product_rows<N, 6>(v, F, A, i0, live, t); break;
+    default: adj_product_rows<N, 7>(v, F, A, i0, live, t); break;
   }
   row_r2c_store<N>(v, H, N, i0, live, t, sh, TW);
 }
