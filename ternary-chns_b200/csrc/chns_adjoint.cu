@@ -94,29 +94,29 @@ struct chns_adj {
   void* phys;
   void* bscr;
   cudaGraphExec_t rev[2];  // one reverse step per current-step buffer (fixed buffers), or null
-  void* rf;                // RecFields of the step being reversed (binary: recorded forward fields)
+  void* rf;                // binary: RecStep, the record table of the step being reversed
   bool rev_tried;
   size_t ncx, nn;
 };
 
 namespace {
 
-// Binary buffers: two field sets of a spectral batch, scratch and F[f] and of
-// physical fields (set 0: the loss; set 1: the transposes' work buffers) and the
-// named spectral fields; a reversed step reads its states and the forward fields
-// the forward step recorded in its segment slot, through the table RecStep.
-constexpr int SSET = 9;                      // spectral fields per set
-enum { SB = 0, SXo = 7, SFFo = 8 };           // batch of 7, scratch, F[f]
+// Binary buffers: two spectral field sets of a batch and a scratch field (set 0: the
+// loss; set 1: the transposes' work buffers), the loss's physical fields and the named
+// ones; a reversed step reads its states and the forward fields the forward step
+// recorded in its segment slot, through the table RecStep.
+constexpr int SSET = 8;                      // spectral fields per set
+enum { SB = 0, SXo = 7 };                     // batch of 7, scratch
 enum {
   SY = 2 * SSET,                             // scratch (f_bar spectrum)
-  SNBW, SNBC,                                // N*_bar (its c part)
+  SNBC,                                      // N*_bar, its c part
   SNBAW, SNBAC,                              // N(u_n)_bar
   SGW, SGC,                                  // running gradient (w_bar, c_bar)
   NSPEC
 };
-constexpr int PSET = 9;                                    // physical fields per set
-enum { PU = 0, PV, PWX, PWY, PCT, PCX, PCY, PMU, PFT };     // forward fields, f(c_t)
-enum { PFB = 2 * PSET, PAB, PBB, PFXB, PFYB, PUB, PVB, PWXB, PWYB, PCTB, PCXB, PCYB, NPHYS };
+constexpr int PSET = 3;                                    // physical fields of the loss's set
+enum { PCT = 0, PCX, PCY };                                 // the loss's c, cx, cy
+enum { PFB = PSET, PAB, PBB, PFXB, PFYB, PUB, PVB, PWXB, PWYB, PCTB, PCXB, PCYB, NPHYS };
 constexpr int kLossBlocks = 1024;  // blocks of the loss reduction
 constexpr int kWork = 4;           // field-set index of the transposes' work buffers
 constexpr int kAcc = 32;           // accumulators; the loss reduction's per-block partials follow

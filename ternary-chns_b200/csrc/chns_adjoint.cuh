@@ -119,62 +119,10 @@ __device__ __forceinline__ void block_acc3(double a0, double a1, double a2, doub
   }
 }
 
-// ---------------------------------------------------------------------------
-// forward fields of the right-hand side at a state (nonlin.c:30-48, 177-198,
-// surface_tension.c:20-75).  The seven truncated spectra u, v, wx, wy, ct, cx, cy
-// are written as one batch (field k at out + k ncx) for one batched inverse
-// transform.
-// ---------------------------------------------------------------------------
+// The seven forward fields whose products the right-hand side forms (nonlin.c:30-48,
+// 177-198, surface_tension.c:20-75), in the order of a batch of their adjoints
+// (field k at xb + k ncx).
 enum { FOP_U = 0, FOP_V, FOP_WX, FOP_WY, FOP_CT, FOP_CX, FOP_CY, FOP_N };
-
-template <class R>
-__global__ void k_adj_fwd_prep7(const AdjPar<R> P, const cx<R>* __restrict__ w, const cx<R>* __restrict__ c,
-                                cx<R>* __restrict__ out, size_t ncx) {
-  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  ModeIdx<R> m;
-  if (!mode_of(P, idx, m)) return;
-  cx<R> r[FOP_N];
-#pragma unroll
-  for (int k = 0; k < FOP_N; k++) r[k] = czero<R>();
-  if (m.in) {
-    const cx<R> a = w[idx], b = c[idx];
-    cx<R> psi = czero<R>();
-    if (m.ks > (R)1e-12) psi = mk<R>(rdiv(a.x, m.ks), rdiv(a.y, m.ks));
-    r[FOP_U] = mul_ik(psi, m.ky);
-    r[FOP_V] = mul_ik(psi, -m.kx);
-    r[FOP_WX] = mul_ik(a, m.kx);
-    r[FOP_WY] = mul_ik(a, m.ky);
-    r[FOP_CT] = b;
-    r[FOP_CX] = mul_ik(b, m.kx);
-    r[FOP_CY] = mul_ik(b, m.ky);
-  }
-#pragma unroll
-  for (int k = 0; k < FOP_N; k++) out[k * ncx + idx] = r[k];
-}
-
-// mu_hat = T[1.5 sigma eps k^2 c + 24 (sigma/eps) F[f]]  (surface_tension.c:45-46)
-template <class R>
-__global__ void k_adj_mu_prep(const AdjPar<R> P, const cx<R>* __restrict__ c, const cx<R>* __restrict__ Ff,
-                              cx<R>* __restrict__ out) {
-  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  ModeIdx<R> m;
-  if (!mode_of(P, idx, m)) return;
-  cx<R> r = czero<R>();
-  if (m.in) {
-    const R q = rmul(P.s1, m.ks);
-    const cx<R> a = c[idx], f = Ff[idx];
-    r = mk<R>(radd(rmul(q, a.x), rmul(P.s2, f.x)), radd(rmul(q, a.y), rmul(P.s2, f.y)));
-  }
-  out[idx] = r;
-}
-
-// f(c) = c (1-c)(1-2c)
-template <class R> __global__ void k_adj_bulk(const R* __restrict__ x, R* __restrict__ y, size_t nn) {
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
-    const R a = x[k];
-    y[k] = rmul(rmul(a, rsub((R)1, a)), rsub((R)1, rmul((R)2, a)));
-  }
-}
 
 // ---------------------------------------------------------------------------
 // adjoint of the spectral tail of nonlin() (nonlin.c:74-101, 232-253,
