@@ -669,8 +669,9 @@ def run_gpu(args):
 def run_profile_case(args):
     """A small, fixed piece of work for an ncu capture: "step" = the workload's FP32
     context stepped --steps times ("step_state64": the CHNS_FP32_STATE64 context); "adjoint" = one adjoint of --steps steps (K = 20)
-    at 512^2 FP64 after a warm-up call; "ensemble" = --steps ensemble steps of the
-    64-member ternary ensemble."""
+    at 512^2 FP64 after a warm-up call; "adjoint_2048" = one binary adjoint of --steps
+    steps (K = 20) at 2048^2 FP32, whose fields are larger than L2; "ensemble" = --steps
+    ensemble steps of the 64-member ternary ensemble."""
     import torch
 
     import chns_b200 as C
@@ -683,6 +684,14 @@ def run_profile_case(args):
         with C.Context(p) as c:
             c.set_phase_real(c_real)
             c.adjoint(4, 20)
+            c.adjoint(args.steps, 20)
+        return
+    if args.profile_case == "adjoint_2048":
+        from chns_b200 import configs
+
+        p, c_real = configs.binary_adjoint(2048, C.FP32)
+        with C.Context(p) as c:
+            c.set_phase_real(c_real)
             c.adjoint(args.steps, 20)
         return
     if args.profile_case == "ensemble":
@@ -887,7 +896,7 @@ def main():
     ap.add_argument("--adjoint-big-steps", type=int, default=1000,
                     help="steps of the 4096^2 FP32 adjoint memory check (0: skip)")
     ap.add_argument("--profile-case", nargs="?", const="step", default=None,
-                    choices=["step", "step_state64", "adjoint", "ensemble"],
+                    choices=["step", "step_state64", "adjoint", "adjoint_2048", "ensemble"],
                     help="only run a small fixed case for ncu captures (step: --steps steps of the FP32 "
                          "workload; step_state64: the same with CHNS_FP32_STATE64; adjoint; ensemble); "
                          "prints nothing")
